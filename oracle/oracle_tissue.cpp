@@ -1,0 +1,622 @@
+// CPU oracle, tissue part -- test infrastructure only (see oracle.h).
+//
+// Restates, for one process, Chaste's monodomain step:
+//   MonodomainProblem -> AbstractDynamicLinearPdeSolver::Solve
+//     (pde/src/solver/AbstractDynamicLinearPdeSolver.hpp:328-497)
+//   a. MonodomainSolver::PrepareForSetupLinearSystem -> AbstractCardiacTissue::SolveCellSystems
+//      (heart/src/tissue/AbstractCardiacTissue.cpp:464-567, caches :730-734)
+//   b. MonodomainSolver::SetupLinearSystem (heart/src/solver/electrics/monodomain/MonodomainSolver.cpp:42-131)
+//      with A = Am*Cm/dt*M + K (MonodomainAssembler.cpp:43-66) assembled once
+//   c. LinearSystem::Solve (linalg/src/LinearSystem.cpp:674-1215) = PETSc KSPCG with
+//      jacobi / bjacobi(ILU(0)) and the default convergence test.
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <set>
+#include <thread>
+#include <vector>
+
+#include "oracle.h"
+#include "oracle_internal.h"
+
+namespace orc {
+
+// ------------------------------------------------------------ thread pool --
+class Pool {
+  public:
+    explicit Pool(int n) { resize(n); }
+    ~Pool() { stop(); }
+    int size() const { return (int)workers_.size() + 1; }
+    void resize(int n) {
+        stop();
+        if (n < 1) n = 1;
+        quit_ = false;
+        for (int i = 1; i < n; ++i) workers_.emplace_back([this, i] { loop(i); });
+    }
+    // fn(thread_index, n_threads)
+    void run(const std::function<void(int, int)>& fn) {
+        const int nt = size();
+        if (nt == 1) {
+            fn(0, 1);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            job_ = &fn;
+            pending_ = nt - 1;
+            gen_++;
+        }
+        cv_.notify_all();
+        fn(0, nt);
+        std::unique_lock<std::mutex> lk(m_);
+        done_cv_.wait(lk, [this] { return pending_ == 0; });
+        job_ = nullptr;
+    }
+
+  private:
+    void loop(int idx) {
+        unsigned long seen = 0;
+        for (;;) {
+            const std::function<void(int, int)>* job;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return quit_ || gen_ != seen; });
+                if (quit_) return;
+                seen = gen_;
+                job = job_;
+            }
+            (*job)(idx, size());
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                if (--pending_ == 0) done_cv_.notify_one();
+            }
+        }
+    }
+    void stop() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            quit_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+        workers_.clear();
+    }
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int, int)>* job_ = nullptr;
+    int pending_ = 0;
+    unsigned long gen_ = 0;
+    bool quit_ = false;
+};
+
+static Pool& pool() {
+    static Pool p(1);
+    return p;
+}
+
+template <class F>
+static void parallel_for(int n, F f) {
+    Pool& P = pool();
+    P.run([&](int ti, int nt) {
+        const int b = (int)((long long)n * ti / nt), e = (int)((long long)n * (ti + 1) / nt);
+        f(b, e);
+    });
+}
+
+// Deterministic sum over [0,n): per-thread partials added in thread order.
+template <class F>
+static double parallel_sum(int n, F f) {
+    Pool& P = pool();
+    std::vector<double> part(P.size(), 0.0);
+    P.run([&](int ti, int nt) {
+        const int b = (int)((long long)n * ti / nt), e = (int)((long long)n * (ti + 1) / nt);
+        double s = 0.0;
+        for (int i = b; i < e; ++i) s += f(i);
+        part[ti] = s;
+    });
+    double s = 0.0;
+    for (double x : part) s += x;
+    return s;
+}
+
+// ------------------------------------------------------------------- CSR --
+struct Csr {
+    int n = 0;
+    std::vector<int> rp, ci;
+    std::vector<double> v;
+    void matvec(const double* x, double* y) const {
+        parallel_for(n, [&](int b, int e) {
+            for (int i = b; i < e; ++i) {
+                double s = 0.0;
+                for (int k = rp[i]; k < rp[i + 1]; ++k) s += v[k] * x[ci[k]];
+                y[i] = s;
+            }
+        });
+    }
+    int find(int i, int j) const {
+        int lo = rp[i], hi = rp[i + 1] - 1;
+        while (lo <= hi) {
+            const int mid = (lo + hi) / 2;
+            if (ci[mid] == j) return mid;
+            if (ci[mid] < j) lo = mid + 1;
+            else hi = mid - 1;
+        }
+        return -1;
+    }
+};
+
+// ---------------------------------------------------- element matrices --
+// P1 simplex in dim dimensions.  The reference integrates with the order-2
+// Gauss rule (AbstractFeVolumeIntegralAssembler.hpp:253, GaussianQuadratureRule.cpp),
+// which is exact for these integrands, so the closed forms are used:
+//   M_e = |J| * vol_ref * (1 + delta_ij) / ((d+1)(d+2))   (MassMatrixAssembler.hpp:76-104)
+//   K_e = |J| * vol_ref * gradphi^T sigma gradphi        (MonodomainStiffnessMatrixAssembler.hpp:68-84)
+static bool element_matrices(int dim, const double* X /*(dim+1)x3*/, const double* sigma,
+                             bool lump, double* Me, double* Ke) {
+    const int nb = dim + 1;
+    double J[3][3] = {{0}}, Ji[3][3] = {{0}};
+    for (int c = 0; c < dim; ++c)
+        for (int r = 0; r < dim; ++r) J[r][c] = X[(c + 1) * 3 + r] - X[r];
+    double det;
+    if (dim == 1) {
+        det = J[0][0];
+        Ji[0][0] = 1.0 / det;
+    } else if (dim == 2) {
+        det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        Ji[0][0] = J[1][1] / det;
+        Ji[0][1] = -J[0][1] / det;
+        Ji[1][0] = -J[1][0] / det;
+        Ji[1][1] = J[0][0] / det;
+    } else {
+        det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+              J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+              J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+        Ji[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+        Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+        Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+        Ji[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+        Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+        Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+        Ji[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+        Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+        Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    }
+    if (det == 0.0) return false;
+    const double adet = std::fabs(det);
+    const double vol_ref = dim == 1 ? 1.0 : (dim == 2 ? 0.5 : 1.0 / 6.0);
+    // reference gradients: phi_0 = 1 - sum xi, phi_k = xi_k
+    double G[3][4] = {{0}};   // G[s][b] = d phi_b / d x_s
+    for (int b = 0; b < nb; ++b) {
+        double g_ref[3] = {0, 0, 0};
+        if (b == 0)
+            for (int s = 0; s < dim; ++s) g_ref[s] = -1.0;
+        else
+            g_ref[b - 1] = 1.0;
+        for (int s = 0; s < dim; ++s) {
+            double acc = 0.0;
+            for (int r = 0; r < dim; ++r) acc += Ji[r][s] * g_ref[r];   // (J^{-T} g)_s
+            G[s][b] = acc;
+        }
+    }
+    const double w = adet * vol_ref;
+    for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) {
+            double k = 0.0;
+            for (int s = 0; s < dim; ++s) k += G[s][i] * sigma[s] * G[s][j];
+            Ke[i * nb + j] = w * k;
+            Me[i * nb + j] = w * (i == j ? 2.0 : 1.0) / ((dim + 1) * (dim + 2));
+        }
+    if (lump) {
+        for (int i = 0; i < nb; ++i) {
+            double s = 0.0;
+            for (int j = 0; j < nb; ++j) s += Me[i * nb + j];
+            for (int j = 0; j < nb; ++j) Me[i * nb + j] = (i == j) ? s : 0.0;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------- tissue --
+struct Tissue {
+    orc_config cfg;
+    int dim, n, ns, np;
+    std::vector<double> V, states /* node-major */, iion, istim;
+    std::vector<int> stim_id, param_id;
+    std::vector<orc_stimulus> stims;
+    std::vector<double> param_table;
+    Csr A, M;
+    std::vector<double> dinv;                 // Jacobi
+    std::vector<double> ilu;                  // ILU(0) factors in A's pattern
+    std::vector<int> ilu_diag;
+    std::vector<double> b, z, r, p, w, x;
+    double t = 0.0;
+    long long steps = 0;
+};
+
+static void ilu0_factor(const Csr& A, std::vector<double>& lu, std::vector<int>& diag) {
+    // ILU(0) with natural ordering, no pivoting: PETSc bjacobi on one process
+    // applies ILU(0) to the single diagonal block (the whole matrix).
+    const int n = A.n;
+    lu = A.v;
+    diag.assign(n, -1);
+    for (int i = 0; i < n; ++i) diag[i] = A.find(i, i);
+    for (int i = 1; i < n; ++i) {
+        for (int kk = A.rp[i]; kk < A.rp[i + 1] && A.ci[kk] < i; ++kk) {
+            const int k = A.ci[kk];
+            lu[kk] /= lu[diag[k]];
+            const double lik = lu[kk];
+            // row i -= lik * row k (only on the pattern of row i, columns > k)
+            int jj = kk + 1;
+            for (int kj = diag[k] + 1; kj < A.rp[k + 1]; ++kj) {
+                const int j = A.ci[kj];
+                while (jj < A.rp[i + 1] && A.ci[jj] < j) ++jj;
+                if (jj < A.rp[i + 1] && A.ci[jj] == j) lu[jj] -= lik * lu[kj];
+            }
+        }
+    }
+}
+
+static void ilu0_apply(const Csr& A, const std::vector<double>& lu, const std::vector<int>& diag,
+                       const double* rin, double* zout) {
+    const int n = A.n;
+    for (int i = 0; i < n; ++i) {
+        double s = rin[i];
+        for (int k = A.rp[i]; k < diag[i]; ++k) s -= lu[k] * zout[A.ci[k]];
+        zout[i] = s;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = zout[i];
+        for (int k = diag[i] + 1; k < A.rp[i + 1]; ++k) s -= lu[k] * zout[A.ci[k]];
+        zout[i] = s / lu[diag[i]];
+    }
+}
+
+static void pc_apply(Tissue& T, const double* rin, double* zout) {
+    const int n = T.n;
+    if (T.cfg.pc == ORC_PC_JACOBI) {
+        const double* d = T.dinv.data();
+        parallel_for(n, [&](int b, int e) {
+            for (int i = b; i < e; ++i) zout[i] = rin[i] * d[i];
+        });
+    } else if (T.cfg.pc == ORC_PC_BJACOBI) {
+        ilu0_apply(T.A, T.ilu, T.ilu_diag, rin, zout);
+    } else {
+        std::memcpy(zout, rin, sizeof(double) * n);
+    }
+}
+
+static double dot(int n, const double* a, const double* b) {
+    return parallel_sum(n, [&](int i) { return a[i] * b[i]; });
+}
+
+// PETSc KSPSolve_CG (src/ksp/ksp/impls/cg/cg.c, standard variant, left
+// preconditioning, KSP_NORM_PRECONDITIONED) with KSPConvergedDefault: with a
+// nonzero initial guess rnorm0 = ||B b||, ttol = max(rtol*rnorm0, abstol);
+// converged when ||B r_k|| <= ttol (checked from iteration 0), diverged when
+// ||B r_k|| >= dtol*rnorm0 (dtol 1e5) or the iteration count reaches max_it.
+static int cg_solve(Tissue& T, double* xv, const double* bv, int* iters) {
+    const int n = T.n;
+    double* R = T.r.data();
+    double* Z = T.z.data();
+    double* P = T.p.data();
+    const double rtol = T.cfg.use_abs_tol ? DBL_EPSILON : T.cfg.tol;
+    const double abstol = T.cfg.use_abs_tol ? T.cfg.tol : 1e-50;
+    const double dtol = 1e5;
+    const int maxit = T.cfg.max_iterations > 0 ? T.cfg.max_iterations : 10000;
+    // LinearSystem::Solve: small nonzero RHS -> zero guess (LinearSystem.cpp:984-994)
+    double rhs1 = parallel_sum(n, [&](int i) { return std::fabs(bv[i]); });
+    bool guess_zero = false;
+    if (rhs1 < 1e-15 && rhs1 > 0.0) {
+        std::fill(xv, xv + n, 0.0);
+        guess_zero = true;
+    }
+    // r = b - A x
+    T.A.matvec(xv, R);
+    parallel_for(n, [&](int b, int e) {
+        for (int i = b; i < e; ++i) R[i] = bv[i] - R[i];
+    });
+    pc_apply(T, R, Z);
+    double dp = std::sqrt(dot(n, Z, Z));
+    double rnorm0;
+    if (!guess_zero) {
+        pc_apply(T, bv, T.w.data());
+        double snorm = std::sqrt(dot(n, T.w.data(), T.w.data()));
+        rnorm0 = snorm != 0.0 ? snorm : dp;
+    } else {
+        rnorm0 = dp;
+    }
+    const double ttol = std::max(rtol * rnorm0, abstol);
+    *iters = 0;
+    if (std::isnan(dp) || std::isinf(dp)) return -3;
+    if (dp <= ttol) return 0;
+    if (dp >= dtol * rnorm0) return -2;
+    double beta = dot(n, Z, R), betaold = 0.0;
+    int i = 0;
+    do {
+        *iters = i + 1;
+        if (beta == 0.0) return 0;
+        if (i == 0) {
+            std::memcpy(P, Z, sizeof(double) * n);
+        } else {
+            const double bb = beta / betaold;
+            parallel_for(n, [&](int b, int e) {
+                for (int k = b; k < e; ++k) P[k] = Z[k] + bb * P[k];
+            });
+        }
+        T.A.matvec(P, Z);                       // Z = A p
+        const double dpi = dot(n, P, Z);
+        if (dpi <= 0.0) return -2;              // indefinite matrix
+        const double a = beta / dpi;
+        parallel_for(n, [&](int b, int e) {
+            for (int k = b; k < e; ++k) {
+                xv[k] += a * P[k];
+                R[k] -= a * Z[k];
+            }
+        });
+        pc_apply(T, R, Z);
+        dp = std::sqrt(dot(n, Z, Z));
+        if (std::isnan(dp) || std::isinf(dp)) return -3;
+        if (dp <= ttol) return 0;
+        if (dp >= dtol * rnorm0) return -2;
+        betaold = beta;
+        beta = dot(n, Z, R);
+        i++;
+    } while (i < maxit);
+    return -1;
+}
+
+template <class Mdl>
+static void solve_cells(Tissue& T, double t0, double t1) {
+    const int ns = Mdl::kNumStates;
+    const int np = Mdl::kNumParams;
+    parallel_for(T.n, [&](int b, int e) {
+        double y[Mdl::kNumStates];
+        double pdef[16];
+        for (int k = 0; k < np; ++k) pdef[k] = 1.0;
+        for (int i = b; i < e; ++i) {
+            double* s = &T.states[(size_t)i * ns];
+            for (int k = 0; k < ns; ++k) y[k] = s[k];
+            y[0] = T.V[i];                                   // SetVoltage
+            const double* p = pdef;
+            if (!T.param_id.empty() && T.param_id[i] >= 0)
+                p = &T.param_table[(size_t)T.param_id[i] * np];
+            const orc_stimulus* st = (!T.stim_id.empty() && T.stim_id[i] >= 0) ? &T.stims[T.stim_id[i]] : nullptr;
+            except_voltage<Mdl>(T.cfg.ode_method, y, p, st, T.cfg.am, T.cfg.cm, t0, t1, T.cfg.dt_ode);
+            y[0] = T.V[i];                                   // restore V (AbstractCardiacCell.cpp:98)
+            for (int k = 0; k < ns; ++k) s[k] = y[k];
+            T.iion[i] = Mdl::template iionic<double>(y, T.cfg.cm, p);     // UpdateCaches
+            T.istim[i] = stimulus_value(st, t1);
+        }
+    });
+}
+
+static int step_once(Tissue& T, int* iters) {
+    const double t0 = T.t;
+    const double t1 = (double)(T.steps + 1) * T.cfg.dt_pde;
+    if (T.cfg.model == ORC_TT06) solve_cells<chb::TenTusscher2006Epi>(T, t0, t1);
+    else solve_cells<chb::LuoRudy1991>(T, t0, t1);
+    // z = Am*Cm*V/dt - Am*Iion - Istim ; b = M z  (MonodomainSolver.cpp:92-107)
+    const double am = T.cfg.am, cm = T.cfg.cm;
+    const double dtinv = 1.0 / T.cfg.dt_pde;
+    double* zz = T.w.data();
+    parallel_for(T.n, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            const double F = -am * T.iion[i] - T.istim[i];
+            zz[i] = am * cm * T.V[i] * dtinv + F;
+        }
+    });
+    T.M.matvec(zz, T.b.data());
+    T.x = T.V;
+    const int rc = cg_solve(T, T.x.data(), T.b.data(), iters);
+    if (rc != 0) return rc;
+    T.V = T.x;
+    T.steps++;
+    T.t = t1;
+    return 0;
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+struct orc_tissue {
+    Tissue T;
+};
+
+extern "C" {
+
+void orc_set_threads(int n) { pool().resize(n); }
+
+int orc_slab_mesh(int dim, double h, double width, double height, double depth, int* n_nodes,
+                  int* n_elems, int* grid, double* xyz, int* conn) {
+    // ConstructRegularSlabMesh (AbstractTetrahedralMesh.cpp:569-614)
+    const unsigned nx = (unsigned)((width + 0.5 * h) / h);
+    const unsigned ny = dim > 1 ? (unsigned)((height + 0.5 * h) / h) : 0;
+    const unsigned nz = dim > 2 ? (unsigned)((depth + 0.5 * h) / h) : 0;
+    if (std::fabs(nx * h - width) > DBL_EPSILON * width ||
+        (dim > 1 && height != 0.0 && std::fabs(ny * h - height) > DBL_EPSILON * height) ||
+        (dim > 2 && depth != 0.0 && std::fabs(nz * h - depth) > DBL_EPSILON * depth))
+        return -1;
+    const int NX = nx + 1, NY = dim > 1 ? ny + 1 : 1, NZ = dim > 2 ? nz + 1 : 1;
+    *n_nodes = NX * NY * NZ;
+    *n_elems = dim == 1 ? nx : (dim == 2 ? 2 * nx * ny : 6 * nx * ny * nz);
+    if (grid) {
+        grid[0] = nx;
+        grid[1] = ny;
+        grid[2] = nz;
+    }
+    if (!xyz || !conn) return 0;
+    // node index (k*(ny+1)+j)*(nx+1)+i; coordinates scaled by h (Scale, :613)
+    for (int k = 0; k < NZ; ++k)
+        for (int j = 0; j < NY; ++j)
+            for (int i = 0; i < NX; ++i) {
+                const long idx = ((long)k * NY + j) * NX + i;
+                xyz[idx * 3 + 0] = i * h;
+                xyz[idx * 3 + 1] = j * h;
+                xyz[idx * 3 + 2] = k * h;
+            }
+    if (dim == 1) {
+        // ConstructLinearMesh (:244-275)
+        for (unsigned e = 0; e < nx; ++e) {
+            conn[e * 2] = e;
+            conn[e * 2 + 1] = e + 1;
+        }
+    } else if (dim == 2) {
+        // ConstructRectangularMesh with stagger (:336-376)
+        long el = 0;
+        for (unsigned j = 0; j < ny; ++j)
+            for (unsigned i = 0; i < nx; ++i) {
+                const unsigned parity = (i + (ny - j)) % 2;
+                const int nw = (j + 1) * (nx + 1) + i;
+                const int sw = j * (nx + 1) + i;
+                conn[el * 3 + 0] = nw;
+                conn[el * 3 + 1] = nw + 1;
+                conn[el * 3 + 2] = parity == 1 ? sw + 1 : sw;
+                el++;
+                conn[el * 3 + 0] = sw + 1;
+                conn[el * 3 + 1] = sw;
+                conn[el * 3 + 2] = parity == 1 ? nw : nw + 1;
+                el++;
+            }
+    } else {
+        // ConstructCuboid: 6 tetrahedra per cube sharing the diagonal 0-7 (:420-422)
+        static const int en[6][4] = {{0, 1, 5, 7}, {0, 1, 3, 7}, {0, 2, 3, 7},
+                                     {0, 2, 6, 7}, {0, 4, 6, 7}, {0, 4, 5, 7}};
+        long el = 0;
+        for (unsigned k = 0; k < nz; ++k)
+            for (unsigned j = 0; j < ny; ++j)
+                for (unsigned i = 0; i < nx; ++i) {
+                    int g[8], l = 0;
+                    for (int z = 0; z < 2; ++z)
+                        for (int y = 0; y < 2; ++y)
+                            for (int x = 0; x < 2; ++x)
+                                g[l++] = i + x + (nx + 1) * (j + y + (ny + 1) * (k + z));
+                    for (int m = 0; m < 6; ++m) {
+                        for (int q = 0; q < 4; ++q) conn[el * 4 + q] = g[en[m][q]];
+                        el++;
+                    }
+                }
+    }
+    return 0;
+}
+
+orc_tissue* orc_tissue_create(const orc_config* cfg, int dim, int n_nodes, const double* xyz,
+                              int n_elems, const int* conn, const double* sigma, const int* stim_id,
+                              const orc_stimulus* stims, int n_stims, const int* param_id,
+                              const double* param_table, int n_param_sets, const double* init_states) {
+    orc_tissue* h = new orc_tissue();
+    Tissue& T = h->T;
+    T.cfg = *cfg;
+    T.dim = dim;
+    T.n = n_nodes;
+    T.ns = orc_num_states(cfg->model);
+    T.np = orc_num_params(cfg->model);
+    T.states.resize((size_t)T.n * T.ns);
+    std::vector<double> y0(T.ns);
+    orc_initial_states(cfg->model, y0.data());
+    for (int i = 0; i < T.n; ++i)
+        for (int k = 0; k < T.ns; ++k)
+            T.states[(size_t)i * T.ns + k] = init_states ? init_states[(size_t)i * T.ns + k] : y0[k];
+    // initial condition: each cell's voltage (AbstractCardiacProblem.cpp:265-292)
+    T.V.resize(T.n);
+    for (int i = 0; i < T.n; ++i) T.V[i] = T.states[(size_t)i * T.ns];
+    T.iion.assign(T.n, 0.0);
+    T.istim.assign(T.n, 0.0);
+    if (stim_id) T.stim_id.assign(stim_id, stim_id + T.n);
+    if (stims) T.stims.assign(stims, stims + n_stims);
+    if (param_id) T.param_id.assign(param_id, param_id + T.n);
+    if (param_table) T.param_table.assign(param_table, param_table + (size_t)n_param_sets * T.np);
+    // sparsity: node adjacency through elements
+    const int nb = dim + 1;
+    std::vector<std::vector<int>> adj(T.n);
+    for (int e = 0; e < n_elems; ++e)
+        for (int a = 0; a < nb; ++a)
+            for (int c = 0; c < nb; ++c) adj[conn[e * nb + a]].push_back(conn[e * nb + c]);
+    for (Csr* C : {&T.A, &T.M}) {
+        C->n = T.n;
+        C->rp.assign(T.n + 1, 0);
+    }
+    for (int i = 0; i < T.n; ++i) {
+        std::sort(adj[i].begin(), adj[i].end());
+        adj[i].erase(std::unique(adj[i].begin(), adj[i].end()), adj[i].end());
+        T.A.rp[i + 1] = T.A.rp[i] + (int)adj[i].size();
+    }
+    T.A.ci.resize(T.A.rp[T.n]);
+    for (int i = 0; i < T.n; ++i) std::copy(adj[i].begin(), adj[i].end(), T.A.ci.begin() + T.A.rp[i]);
+    T.A.v.assign(T.A.ci.size(), 0.0);
+    T.M.rp = T.A.rp;
+    T.M.ci = T.A.ci;
+    T.M.v.assign(T.A.ci.size(), 0.0);
+    // assemble (AbstractFeVolumeIntegralAssembler::DoAssemble, element loop)
+    const double mass_scale = cfg->am * cfg->cm / cfg->dt_pde;
+    for (int e = 0; e < n_elems; ++e) {
+        double X[4 * 3];
+        for (int a = 0; a < nb; ++a)
+            for (int s = 0; s < 3; ++s) X[a * 3 + s] = xyz[(size_t)conn[e * nb + a] * 3 + s];
+        double Me[16], Ke[16];
+        if (!element_matrices(dim, X, sigma + (size_t)e * dim, cfg->mass_lumping != 0, Me, Ke)) {
+            delete h;
+            return nullptr;
+        }
+        for (int a = 0; a < nb; ++a)
+            for (int c = 0; c < nb; ++c) {
+                const int k = T.A.find(conn[e * nb + a], conn[e * nb + c]);
+                T.A.v[k] += mass_scale * Me[a * nb + c] + Ke[a * nb + c];
+                T.M.v[k] += Me[a * nb + c];
+            }
+    }
+    T.dinv.resize(T.n);
+    for (int i = 0; i < T.n; ++i) T.dinv[i] = 1.0 / T.A.v[T.A.find(i, i)];
+    if (cfg->pc == ORC_PC_BJACOBI) ilu0_factor(T.A, T.ilu, T.ilu_diag);
+    T.b.assign(T.n, 0.0);
+    T.z.assign(T.n, 0.0);
+    T.r.assign(T.n, 0.0);
+    T.p.assign(T.n, 0.0);
+    T.w.assign(T.n, 0.0);
+    T.x.assign(T.n, 0.0);
+    return h;
+}
+
+void orc_tissue_destroy(orc_tissue* t) { delete t; }
+
+int orc_tissue_step(orc_tissue* h, int n, int* cg_iters) {
+    for (int s = 0; s < n; ++s) {
+        int it = 0;
+        const int rc = step_once(h->T, &it);
+        if (cg_iters) cg_iters[s] = it;
+        if (rc != 0) return rc;
+    }
+    return 0;
+}
+
+double orc_tissue_time(const orc_tissue* h) { return h->T.t; }
+
+void orc_tissue_get_voltage(const orc_tissue* h, double* v) {
+    std::memcpy(v, h->T.V.data(), sizeof(double) * h->T.n);
+}
+
+void orc_tissue_get_states(const orc_tissue* h, double* s) {
+    std::memcpy(s, h->T.states.data(), sizeof(double) * h->T.states.size());
+    for (int i = 0; i < h->T.n; ++i) s[(size_t)i * h->T.ns] = h->T.V[i];
+}
+
+void orc_tissue_get_caches(const orc_tissue* h, double* iion, double* istim) {
+    std::memcpy(iion, h->T.iion.data(), sizeof(double) * h->T.n);
+    std::memcpy(istim, h->T.istim.data(), sizeof(double) * h->T.n);
+}
+
+int orc_tissue_matrix(const orc_tissue* h, int which, int* rowptr, int* cols, double* vals) {
+    const Csr& C = which == 0 ? h->T.A : h->T.M;
+    if (rowptr) std::memcpy(rowptr, C.rp.data(), sizeof(int) * (C.n + 1));
+    if (cols) std::memcpy(cols, C.ci.data(), sizeof(int) * C.ci.size());
+    if (vals) std::memcpy(vals, C.v.data(), sizeof(double) * C.v.size());
+    return (int)C.ci.size();
+}
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+"""Extract Chaste's own golden vectors for the monodomain path into chaste_kats.json.
+
+Run in a container where the reference tree is mounted (default
+/root/reference); the GPU tests and the benchmark only read the JSON.
+Sources:
+  heart/test/data/ionicmodels/Lr91DelayedStimValidData.dat   (TestIonicModels.hpp:406-467)
+  heart/test/data/ionicmodels/Lr91RegularStimValidData.dat   (TestIonicModels.hpp:469-500)
+  heart/test/data/ionicmodels/TenTusscherValidData.dat       (TestIonicModels.hpp:793-835)
+  hard-coded values of heart/test/monodomain/TestMonodomainProblem.hpp
+  (:166-218, :226-297, :303-340, :784-974) and TestIonicModels.hpp GetIIonic checks.
+"""
+import json
+import os
+import sys
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+
+
+def read_dat(rel):
+    with open(os.path.join(REF, rel)) as f:
+        header = f.readline().split()
+        rows = [[float(x) for x in line.split()] for line in f if line.strip()]
+    names = [h.split("(")[0] for h in header]
+    return {n: [r[i] for r in rows] for i, n in enumerate(names)}
+
+
+out = {
+    "source": "Chaste heart/test (see make_golden.py docstring)",
+    "lr91_delayed_stim": {
+        "stimulus": {"kind": "simple", "magnitude": -25.5, "duration": 2.0, "start": 50.0},
+        "dt": 0.01, "end": 1000.0, "sample_every_steps": 100, "tolerance": 1e-3,
+        "V": read_dat("heart/test/data/ionicmodels/Lr91DelayedStimValidData.dat")["V"],
+        "iionic_after_1000_plus_60ms": 1.9411, "iionic_tolerance": 1e-3,
+    },
+    "lr91_regular_stim": {
+        "stimulus": {"kind": "regular", "magnitude": -25.5, "duration": 2.0, "period": 500.0,
+                     "start": 50.0},
+        "dt": 0.01, "end": 1000.0, "sample_every_steps": 100, "tolerance": 1e-3,
+        "states": read_dat("heart/test/data/ionicmodels/Lr91RegularStimValidData.dat"),
+    },
+    "tt06_simple_stim": {
+        "stimulus": {"kind": "simple", "magnitude": -38.0, "duration": 1.0, "start": 5.0},
+        "dt": 0.001, "end": 40.0, "sample_every_steps": 1000, "tolerance": 1e-3,
+        "states": read_dat("heart/test/data/ionicmodels/TenTusscherValidData.dat"),
+        "iionic_at_end": -0.1843, "iionic_initial": 0.0012, "iionic_tolerance": 1e-3,
+    },
+    "tissue": [
+        {"name": "TestMonodomainProblem1D", "dim": 1, "h": 0.01, "size": [0.1, 0, 0],
+         "sigma": 0.0005, "am": 1.0, "cm": 1.0, "stim": -600.0, "stim_duration": 0.5,
+         "end": 2.0, "abs_tol": 2e-4, "nodes": [1, 3, 5, 7, 9, 10],
+         "V": [20.7710232, 21.5319692, 22.9280817, 24.0611303, -0.770330519, -19.2234919],
+         "tolerance": 5e-3},
+        {"name": "TestMonodomainProblem1DWithRelativeTolerance", "dim": 1, "h": 0.01,
+         "size": [0.1, 0, 0], "sigma": 0.0005, "am": 1.0, "cm": 1.0, "stim": -600.0,
+         "stim_duration": 0.5, "end": 2.0, "rel_tol": 1e-9, "nodes": [1, 3, 5, 7, 9, 10],
+         "V": [20.7710232, 21.5319692, 22.9280817, 24.0611303, -0.770330519, -19.2234919],
+         "tolerance": 2e-5},
+        {"name": "TestMonodomainProblemSimplestMesh1D", "dim": 1, "h": 1.0, "size": [1.0, 0, 0],
+         "sigma": 0.0005, "am": 1.0, "cm": 10.0, "stim": -600.0, "stim_duration": 0.5,
+         "end": 2.0, "abs_tol": 2e-4, "nodes": [0, 1], "V": [-52.1698, -83.8381],
+         "tolerance": 5e-3},
+        {"name": "TestMonodomainProblemCreates1DGeometry", "dim": 1, "h": 0.01,
+         "size": [1.0, 0, 0], "sigma": 1.75, "am": 1400.0, "cm": 1.0, "stim": -3.0e6,
+         "stim_duration": 0.5, "end": 5.0, "abs_tol": 2e-4, "nodes": [1, 3, 5, 7],
+         "V": [13.9682, 13.9149, 13.8216, 13.7275], "tolerance": 5e-3},
+        {"name": "TestMonodomainProblemCreates2DGeometry", "dim": 2, "h": 0.01,
+         "size": [0.3, 0.3, 0], "sigma": 1.75, "am": 1400.0, "cm": 1.0, "stim": -3.0e6,
+         "stim_duration": 0.5, "end": 4.0, "abs_tol": 2e-4, "nodes": [1, 3, 5, 7],
+         "V": [17.5728, 17.4562, 17.2559, 17.0440], "tolerance": 5e-3},
+        {"name": "TestMonodomainProblemCreates3DGeometry", "dim": 3, "h": 0.01,
+         "size": [0.1, 0.1, 0.1], "sigma": 1.75, "am": 1400.0, "cm": 1.0, "stim": -3.0e6,
+         "stim_duration": 0.5, "end": 2.0, "abs_tol": 2e-4, "nodes": [1, 3, 5, 7, 0, 665, 1330],
+         "V": [31.8958, 32.1109, 32.7315, 33.7011, 31.8730, 32.6531, 34.5152],
+         "tolerance": 5e-3,
+         "midway": {"end": 1.0, "nodes": [0, 665, 1330], "V": [48.0637, 26.5404, -55.3058],
+                    "tolerance": 1e-3}},
+    ],
+}
+here = os.path.dirname(os.path.abspath(__file__))
+with open(os.path.join(here, "chaste_kats.json"), "w") as f:
+    json.dump(out, f, indent=1)
+print("wrote chaste_kats.json")
