@@ -463,6 +463,9 @@ class ModelEmitter:
         rl_flags = ", ".join("true" if s in self.rl else "false" for s in self.states)
         A(f"    // 1 where the state is advanced by Rush-Larsen (ODE affine in itself)")
         A(f"    static constexpr bool kRushLarsen[{n}] = {{{rl_flags}}};")
+        rl_idx = [str(i) for i, st in enumerate(self.states) if st in self.rl]
+        cond = " || ".join(f"i == {k}" for k in rl_idx) or "false"
+        A(f"    CHB_HD static constexpr bool rush_larsen(int i) {{ return {cond}; }}")
         # verify ranges: dimensionless RL states with initial value in [0,1] are gates
         kinds = []
         for s in self.states:
@@ -478,13 +481,18 @@ class ModelEmitter:
                 kinds.append("0")
         A(f"    // range class per state: 1 gate in [0,1], 2 concentration > 0, 0 unchecked")
         A(f"    static constexpr int kRangeClass[{n}] = {{{', '.join(kinds)}}};")
+        g = [str(i) for i, k in enumerate(kinds) if k == "1"]
+        cc = [str(i) for i, k in enumerate(kinds) if k == "2"]
+        gc = " || ".join(f"i == {k}" for k in g) or "false"
+        ccc = " || ".join(f"i == {k}" for k in cc) or "false"
+        A(f"    CHB_HD static constexpr int range_class(int i) {{ return ({gc}) ? 1 : (({ccc}) ? 2 : 0); }}")
         A("")
         # ---- rhs (forward Euler derivatives, all states, dV included)
         dy_exprs = [self.odes[s] for s in self.states]
         A("    // dy/dt for every state at (y, stim) where stim is the Chaste area stimulus")
         A("    // in uA/cm^2 and cm the Chaste capacitance in uF/cm^2.  y[0] is the voltage.")
         A("    template <typename T>")
-        A("    CHB_HD static inline void rhs(const T* __restrict__ y, T stim, T cm,")
+        A("    CHB_HD static void rhs(const T* __restrict__ y, T stim, T cm,")
         A("                                  const T* __restrict__ p, T* __restrict__ dy) {")
         A("        (void)stim; (void)cm; (void)p;")
         lines.extend(self._body(dy_exprs, pr))
@@ -497,7 +505,7 @@ class ModelEmitter:
         A("    // the (negative) affine coefficient h so y' = inf + (y - inf)*exp(h*dt);")
         A("    // for the other states rate[i] holds dy/dt.  rate[0] is dV/dt.")
         A("    template <typename T>")
-        A("    CHB_HD static inline void rl_terms(const T* __restrict__ y, T stim, T cm,")
+        A("    CHB_HD static void rl_terms(const T* __restrict__ y, T stim, T cm,")
         A("                                       const T* __restrict__ p, T* __restrict__ rate,")
         A("                                       T* __restrict__ inf) {")
         A("        (void)stim; (void)cm; (void)p; (void)inf;")
@@ -528,7 +536,7 @@ class ModelEmitter:
         A("    // Total ionic current in uA/cm^2 (GetIIonic): the dV/dt currents without")
         A("    // the stimulus" + (", times the capacitance cm." if self.current_per_cap else "."))
         A("    template <typename T>")
-        A("    CHB_HD static inline T iionic(const T* __restrict__ y, T cm, const T* __restrict__ p) {")
+        A("    CHB_HD static T iionic(const T* __restrict__ y, T cm, const T* __restrict__ p) {")
         A("        (void)cm; (void)p;")
         A("        const T stim = T(0.0); (void)stim;")
         lines.extend(self._body([tot], pr))

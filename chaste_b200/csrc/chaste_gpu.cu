@@ -1,0 +1,947 @@
+// libchastegpu: the C-ABI of include/chaste_gpu.h.  Owns device memory,
+// launches the ODE and CG kernels and captures one PDE step as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/chaste_gpu.h"
+#include "host/assemble.h"
+#include "kernels/cg.cuh"
+#include "kernels/cg_mixed.cuh"
+#include "kernels/ode.cuh"
+
+using namespace chb;
+
+namespace {
+
+constexpr int kRing = 4096;   // iteration-count history per context
+
+struct DeviceBuffers {
+    std::vector<void*> owned;
+    ~DeviceBuffers() { release(); }
+    void release() {
+        for (void* p : owned) cudaFree(p);
+        owned.clear();
+    }
+};
+
+}  // namespace
+
+struct cg_ctx {
+    cg_config cfg{};
+    int n_states = 0, n_params = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool graph_dirty = true;
+    DeviceBuffers mem;
+    // mesh / operator
+    int n = 0, dim = 0;
+    bool have_mesh = false, have_cells = false;
+    bool slab = false;
+    SlabGrid grid;
+    SlabStencil stencil;
+    HostCsr csr;
+    // device arrays
+    double* d_V = nullptr;
+    void* d_states = nullptr;     // (S-1) x n of T
+    void* d_iion = nullptr;
+    void* d_z = nullptr;
+    double* d_act = nullptr;
+    uint8_t* d_stim_id = nullptr;
+    DevStimulus* d_stims = nullptr;
+    uint8_t* d_pset = nullptr;
+    void* d_params = nullptr;
+    uint8_t* d_cls8 = nullptr;
+    double *d_r = nullptr, *d_p0 = nullptr, *d_p1 = nullptr, *d_q = nullptr;
+    float *d_r32 = nullptr, *d_p32a = nullptr, *d_p32b = nullptr, *d_e32 = nullptr, *d_q32 = nullptr;
+    double* d_partials = nullptr;
+    GridSync* d_gs = nullptr;
+    int* d_status = nullptr;
+    long long* d_step = nullptr;
+    int* d_ring = nullptr;
+    int* d_refine = nullptr;
+    double *d_atab = nullptr, *d_mtab = nullptr;
+    float *d_atab32 = nullptr, *d_mtab32 = nullptr;
+    int *d_rowptr = nullptr, *d_cols = nullptr;
+    double *d_aval = nullptr, *d_mval = nullptr, *d_dinv = nullptr;
+    float *d_aval32 = nullptr, *d_dinv32 = nullptr;
+    // host mirrors
+    std::vector<int> stim_id_host;
+    std::vector<cg_stimulus> stims_host;
+    // launch shapes
+    int ode_blocks = 0;
+    int cg_blocks = 0;
+    int diag_slot = 0;
+    // stats
+    long long steps = 0;
+    long long total_iters = 0;
+    int max_iters = 0;
+    double ms_last = 0.0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    bool mixed() const { return cfg.precision == CG_PRECISION_MIXED; }
+    size_t real_size() const { return mixed() ? sizeof(float) : sizeof(double); }
+};
+
+namespace {
+
+#define CG_CUDA(call)                                 \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) {                      \
+            cudaGetLastError();                       \
+            return CG_ERR_CUDA;                       \
+        }                                             \
+    } while (0)
+
+#define CG_TRY(x)                     \
+    do {                              \
+        int rc_ = (x);                \
+        if (rc_ != CG_OK) return rc_; \
+    } while (0)
+
+template <typename P>
+int dalloc(cg_ctx* c, P** p, size_t bytes) {
+    void* q = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&q, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return CG_ERR_NOMEM;
+    }
+    c->mem.owned.push_back(q);
+    *p = reinterpret_cast<P*>(q);
+    return CG_OK;
+}
+
+int states_of(int model) { return model == CG_MODEL_TT06 ? TenTusscher2006Epi::kNumStates : LuoRudy1991::kNumStates; }
+int params_of(int model) { return model == CG_MODEL_TT06 ? TenTusscher2006Epi::kNumParams : LuoRudy1991::kNumParams; }
+const double* init_of(int model) {
+    return model == CG_MODEL_TT06 ? TenTusscher2006Epi::kInitialStates : LuoRudy1991::kInitialStates;
+}
+
+int status_from_bits(int bits) {
+    if (bits & kStatusBarrierTimeout) return CG_ERR_TIMEOUT;
+    if (bits & kStatusNaN) return CG_ERR_NAN;
+    if (bits & kStatusCgDiverged) return CG_ERR_CG_DIVERGED;
+    if (bits & kStatusCgMaxIt) return CG_ERR_CG_MAXIT;
+    if (bits & kStatusStateRange) return CG_ERR_STATE_RANGE;
+    return CG_OK;
+}
+
+DevStimulus to_dev(const cg_stimulus& s) {
+    // duration padding exactly as the reference constructors do
+    DevStimulus d{};
+    d.kind = s.kind;
+    d.magnitude = s.magnitude;
+    d.start = s.start;
+    d.period = s.period;
+    d.stop = s.stop;
+    if (s.kind == CG_STIM_SIMPLE) d.duration = s.duration + (s.duration + s.start) * DBL_EPSILON;
+    else if (s.kind == CG_STIM_REGULAR) d.duration = s.duration + s.period * DBL_EPSILON;
+    else d.duration = 0.0;
+    return d;
+}
+
+double host_stim(const cg_stimulus& s, double t) {
+    const DevStimulus d = to_dev(s);
+    if (d.kind == 1) return (d.start <= t && t <= d.duration + d.start) ? d.magnitude : 0.0;
+    if (d.kind == 2) {
+        if (t < d.start) return 0.0;
+        const double beat = std::fmod(t - d.start, d.period);
+        return (beat >= 0 && beat <= d.duration && t <= d.stop) ? d.magnitude : 0.0;
+    }
+    return 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cg_default_config(cg_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->model = CG_MODEL_LR91;
+    c->ode_method = CG_ODE_FORWARD_EULER;
+    c->ode_time_step = 0.01;
+    c->pde_time_step = 0.01;
+    c->surface_area_to_volume_ratio = 1400.0;
+    c->capacitance = 1.0;
+    c->ksp_preconditioner = CG_PC_JACOBI;
+    c->use_absolute_tolerance = 1;
+    c->ksp_tolerance = 2e-4;
+    c->use_mass_lumping = 0;
+    c->max_iterations = 10000;
+    c->precision = CG_PRECISION_FP64;
+    c->device = 0;
+    c->check_state_ranges = 0;
+    c->activation_threshold = -40.0;
+}
+
+const char* cg_status_string(int s) {
+    switch (s) {
+        case CG_OK: return "ok";
+        case CG_ERR_ARG: return "invalid argument";
+        case CG_ERR_CUDA: return "CUDA runtime error or no CUDA device";
+        case CG_ERR_CG_MAXIT: return "CG reached the maximum number of iterations (KSP_DIVERGED_ITS)";
+        case CG_ERR_CG_DIVERGED: return "CG diverged (KSP_DIVERGED_DTOL or indefinite matrix)";
+        case CG_ERR_NAN: return "NaN or Inf in the linear solve (KSP_DIVERGED_NANORINF)";
+        case CG_ERR_STATE_RANGE: return "a cell state variable left its valid range";
+        case CG_ERR_ORDER: return "calls made in the wrong order";
+        case CG_ERR_TIMEOUT: return "a device-side barrier timed out";
+        case CG_ERR_NOMEM: return "device allocation failed";
+        case CG_ERR_UNSUPPORTED: return "unsupported configuration";
+        default: return "unknown status";
+    }
+}
+
+int cg_num_states(int model, int* n) {
+    if (!n || (model != CG_MODEL_LR91 && model != CG_MODEL_TT06)) return CG_ERR_ARG;
+    *n = states_of(model);
+    return CG_OK;
+}
+
+int cg_num_params(int model, int* n) {
+    if (!n || (model != CG_MODEL_LR91 && model != CG_MODEL_TT06)) return CG_ERR_ARG;
+    *n = params_of(model);
+    return CG_OK;
+}
+
+int cg_create(const cg_config* cfg, cg_ctx** out) {
+    if (!cfg || !out) return CG_ERR_ARG;
+    *out = nullptr;
+    if (cfg->model != CG_MODEL_LR91 && cfg->model != CG_MODEL_TT06) return CG_ERR_ARG;
+    if (cfg->ode_method != CG_ODE_FORWARD_EULER && cfg->ode_method != CG_ODE_RUSH_LARSEN) return CG_ERR_ARG;
+    if (!(cfg->ode_time_step > 0) || !(cfg->pde_time_step > 0)) return CG_ERR_ARG;
+    if (!(cfg->surface_area_to_volume_ratio > 0) || !(cfg->capacitance > 0)) return CG_ERR_ARG;
+    if (!(cfg->ksp_tolerance > 0)) return CG_ERR_ARG;
+    if (cfg->ksp_preconditioner == CG_PC_BJACOBI) return CG_ERR_UNSUPPORTED;
+    if (cfg->ksp_preconditioner != CG_PC_NONE && cfg->ksp_preconditioner != CG_PC_JACOBI) return CG_ERR_ARG;
+    if (cfg->precision != CG_PRECISION_FP64 && cfg->precision != CG_PRECISION_MIXED) return CG_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return CG_ERR_CUDA;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) return CG_ERR_ARG;
+    cg_ctx* c = new (std::nothrow) cg_ctx();
+    if (!c) return CG_ERR_NOMEM;
+    c->cfg = *cfg;
+    if (c->cfg.max_iterations <= 0) c->cfg.max_iterations = 10000;
+    c->n_states = states_of(cfg->model);
+    c->n_params = params_of(cfg->model);
+    c->device = cfg->device;
+    if (cudaSetDevice(c->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return CG_ERR_CUDA;
+    }
+    *out = c;
+    return CG_OK;
+}
+
+int cg_destroy(cg_ctx* c) {
+    if (!c) return CG_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    c->mem.release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- mesh --
+namespace {
+
+int alloc_vectors(cg_ctx* c) {
+    const size_t n = (size_t)c->n;
+    CG_TRY(dalloc(c, &c->d_V, n * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_r, n * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_p0, n * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_p1, n * sizeof(double)));
+    if (!c->slab) CG_TRY(dalloc(c, &c->d_q, n * sizeof(double)));
+    if (c->mixed()) {
+        CG_TRY(dalloc(c, &c->d_r32, n * sizeof(float)));
+        CG_TRY(dalloc(c, &c->d_p32a, n * sizeof(float)));
+        CG_TRY(dalloc(c, &c->d_p32b, n * sizeof(float)));
+        CG_TRY(dalloc(c, &c->d_e32, n * sizeof(float)));
+        if (!c->slab) CG_TRY(dalloc(c, &c->d_q32, n * sizeof(float)));
+    }
+    CG_TRY(dalloc(c, &c->d_act, n * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_gs, sizeof(GridSync)));
+    CG_TRY(dalloc(c, &c->d_status, sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_step, sizeof(long long)));
+    CG_TRY(dalloc(c, &c->d_ring, kRing * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_refine, sizeof(int)));
+    cudaStream_t s = c->stream;
+    CG_CUDA(cudaMemsetAsync(c->d_gs, 0, sizeof(GridSync), s));
+    CG_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+    CG_CUDA(cudaMemsetAsync(c->d_step, 0, sizeof(long long), s));
+    CG_CUDA(cudaMemsetAsync(c->d_ring, 0, kRing * sizeof(int), s));
+    CG_CUDA(cudaMemsetAsync(c->d_refine, 0, sizeof(int), s));
+    CG_CUDA(cudaMemsetAsync(c->d_V, 0, n * sizeof(double), s));
+    CG_CUDA(cudaMemsetAsync(c->d_r, 0, n * sizeof(double), s));
+    CG_CUDA(cudaMemsetAsync(c->d_p0, 0, n * sizeof(double), s));
+    CG_CUDA(cudaMemsetAsync(c->d_p1, 0, n * sizeof(double), s));
+    // launch shapes: the CG kernel is cooperative, so its grid must be co-resident
+    int sms = 0;
+    CG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    int per_sm = 0;
+    if (c->mixed()) {
+        if (c->slab) CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_mixed_kernel<true>, 512, 0));
+        else CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_mixed_kernel<false>, 512, 0));
+    } else {
+        if (c->slab) CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fp64_kernel<true>, 512, 0));
+        else CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fp64_kernel<false>, 512, 0));
+    }
+    if (per_sm < 1) return CG_ERR_UNSUPPORTED;
+    const long long want = ((long long)n + 511) / 512;
+    c->cg_blocks = (int)std::max(1LL, std::min(want, (long long)per_sm * sms));
+    CG_TRY(dalloc(c, &c->d_partials, (size_t)c->cg_blocks * 4 * sizeof(double)));
+    c->ode_blocks = (int)std::max(1LL, std::min(((long long)n + 255) / 256, (long long)sms * 16));
+    CG_CUDA(cudaStreamSynchronize(s));
+    return CG_OK;
+}
+
+int upload_operator(cg_ctx* c) {
+    cudaStream_t s = c->stream;
+    if (c->slab) {
+        const SlabStencil& st = c->stencil;
+        const size_t tab = (size_t)st.n_classes * st.n_offsets;
+        CG_TRY(dalloc(c, &c->d_atab, tab * sizeof(double)));
+        CG_TRY(dalloc(c, &c->d_mtab, tab * sizeof(double)));
+        CG_TRY(dalloc(c, &c->d_atab32, tab * sizeof(float)));
+        CG_TRY(dalloc(c, &c->d_mtab32, tab * sizeof(float)));
+        std::vector<float> a32(st.a.begin(), st.a.end()), m32(st.m.begin(), st.m.end());
+        CG_CUDA(cudaMemcpyAsync(c->d_atab, st.a.data(), tab * sizeof(double), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_mtab, st.m.data(), tab * sizeof(double), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_atab32, a32.data(), tab * sizeof(float), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_mtab32, m32.data(), tab * sizeof(float), cudaMemcpyHostToDevice, s));
+        std::vector<uint8_t> cls((size_t)c->n);
+        const int NX = c->grid.NX(), NY = c->grid.NY(), NZ = c->grid.NZ();
+        for (int k = 0; k < NZ; ++k)
+            for (int j = 0; j < NY; ++j)
+                for (int i = 0; i < NX; ++i) cls[((size_t)k * NY + j) * NX + i] = (uint8_t)slab_class(c->grid, i, j, k);
+        CG_TRY(dalloc(c, &c->d_cls8, cls.size()));
+        CG_CUDA(cudaMemcpyAsync(c->d_cls8, cls.data(), cls.size(), cudaMemcpyHostToDevice, s));
+        c->diag_slot = -1;
+        for (int o = 0; o < st.n_offsets; ++o)
+            if (st.offsets[o] == 0) c->diag_slot = o;
+        if (c->diag_slot < 0) return CG_ERR_ARG;
+        CG_CUDA(cudaStreamSynchronize(s));
+    } else {
+        const HostCsr& m = c->csr;
+        const size_t nnz = m.cols.size();
+        CG_TRY(dalloc(c, &c->d_rowptr, (m.n + 1) * sizeof(int)));
+        CG_TRY(dalloc(c, &c->d_cols, nnz * sizeof(int)));
+        CG_TRY(dalloc(c, &c->d_aval, nnz * sizeof(double)));
+        CG_TRY(dalloc(c, &c->d_mval, nnz * sizeof(double)));
+        CG_TRY(dalloc(c, &c->d_dinv, m.n * sizeof(double)));
+        std::vector<double> dinv(m.n);
+        for (int i = 0; i < m.n; ++i) {
+            const int k = m.find(i, i);
+            if (k < 0 || m.a[k] == 0.0) return CG_ERR_ARG;
+            dinv[i] = 1.0 / m.a[k];
+        }
+        CG_CUDA(cudaMemcpyAsync(c->d_rowptr, m.rowptr.data(), (m.n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_cols, m.cols.data(), nnz * sizeof(int), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_aval, m.a.data(), nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_mval, m.m.data(), nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_dinv, dinv.data(), m.n * sizeof(double), cudaMemcpyHostToDevice, s));
+        std::vector<float> a32, d32;
+        if (c->mixed()) {
+            a32.assign(m.a.begin(), m.a.end());
+            d32.assign(dinv.begin(), dinv.end());
+            CG_TRY(dalloc(c, &c->d_aval32, nnz * sizeof(float)));
+            CG_TRY(dalloc(c, &c->d_dinv32, m.n * sizeof(float)));
+            CG_CUDA(cudaMemcpyAsync(c->d_aval32, a32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, s));
+            CG_CUDA(cudaMemcpyAsync(c->d_dinv32, d32.data(), m.n * sizeof(float), cudaMemcpyHostToDevice, s));
+        }
+        CG_CUDA(cudaStreamSynchronize(s));
+    }
+    return alloc_vectors(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cg_set_mesh(cg_ctx* c, int n_nodes, int dim, const double* xyz, int n_elems, const int* conn,
+                const double* sigma) {
+    if (!c || !xyz || !conn || !sigma || n_nodes <= 0 || n_elems <= 0 || dim < 1 || dim > 3) return CG_ERR_ARG;
+    if (c->have_mesh) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    c->n = n_nodes;
+    c->dim = dim;
+    c->slab = false;
+    const double mass_scale = c->cfg.surface_area_to_volume_ratio * c->cfg.capacitance / c->cfg.pde_time_step;
+    if (!assemble(dim, n_nodes, xyz, n_elems, conn, sigma, mass_scale, c->cfg.use_mass_lumping != 0, c->csr))
+        return CG_ERR_ARG;
+    CG_TRY(upload_operator(c));
+    c->have_mesh = true;
+    return CG_OK;
+}
+
+int cg_set_slab_mesh(cg_ctx* c, int dim, double h, double width, double height, double depth,
+                     const double* sigma, int* n_nodes_out) {
+    if (!c || !sigma) return CG_ERR_ARG;
+    if (c->have_mesh) return CG_ERR_ORDER;
+    SlabGrid g;
+    if (!slab_grid(dim, h, width, height, depth, g)) return CG_ERR_ARG;
+    if (g.nodes() > (1LL << 31) - 1) return CG_ERR_ARG;
+    CG_CUDA(cudaSetDevice(c->device));
+    std::vector<double> xyz;
+    std::vector<int> conn;
+    slab_mesh(g, xyz, conn);
+    const int n_elems = (int)(conn.size() / (dim + 1));
+    std::vector<double> sig((size_t)n_elems * dim);
+    for (int e = 0; e < n_elems; ++e)
+        for (int s = 0; s < dim; ++s) sig[(size_t)e * dim + s] = sigma[s];
+    c->n = (int)g.nodes();
+    c->dim = dim;
+    c->grid = g;
+    const double mass_scale = c->cfg.surface_area_to_volume_ratio * c->cfg.capacitance / c->cfg.pde_time_step;
+    if (!assemble(dim, c->n, xyz.data(), n_elems, conn.data(), sig.data(), mass_scale,
+                  c->cfg.use_mass_lumping != 0, c->csr))
+        return CG_ERR_ARG;
+    c->slab = build_slab_stencil(g, c->csr, c->stencil);
+    if (c->slab) {
+        HostCsr empty;
+        std::swap(c->csr, empty);
+    }
+    CG_TRY(upload_operator(c));
+    c->have_mesh = true;
+    if (n_nodes_out) *n_nodes_out = c->n;
+    return CG_OK;
+}
+
+int cg_num_nodes(cg_ctx* c, int* n) {
+    if (!c || !n) return CG_ERR_ARG;
+    if (!c->have_mesh) return CG_ERR_ORDER;
+    *n = c->n;
+    return CG_OK;
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------------- cells --
+namespace {
+
+int ensure_stimulus_buffers(cg_ctx* c) {
+    if (c->d_stim_id) return CG_OK;
+    CG_TRY(dalloc(c, &c->d_stim_id, (size_t)c->n));
+    CG_TRY(dalloc(c, &c->d_stims, 256 * sizeof(DevStimulus)));
+    CG_CUDA(cudaMemsetAsync(c->d_stim_id, 0xFF, (size_t)c->n, c->stream));
+    CG_CUDA(cudaMemsetAsync(c->d_stims, 0, 256 * sizeof(DevStimulus), c->stream));
+    c->stim_id_host.assign(c->n, -1);
+    return CG_OK;
+}
+
+template <typename T>
+int upload_cells_t(cg_ctx* c, const double* init, const int* pset, const double* ptab, int nsets) {
+    const size_t n = (size_t)c->n;
+    const int S = c->n_states, P = c->n_params;
+    if (!c->d_states) {
+        T* p = nullptr;
+        CG_TRY(dalloc(c, &p, (size_t)(S - 1) * n * sizeof(T)));
+        c->d_states = p;
+        CG_TRY(dalloc(c, &p, n * sizeof(T)));
+        c->d_iion = p;
+        CG_TRY(dalloc(c, &p, n * sizeof(T)));
+        c->d_z = p;
+    }
+    CG_TRY(ensure_stimulus_buffers(c));
+    std::vector<T> soa((size_t)(S - 1) * n);
+    std::vector<double> v(n);
+    const double* y0 = init_of(c->cfg.model);
+    for (size_t i = 0; i < n; ++i) {
+        const double* y = init ? init + i * S : y0;
+        v[i] = y[0];
+        for (int k = 1; k < S; ++k) soa[(size_t)(k - 1) * n + i] = (T)y[k];
+    }
+    cudaStream_t s = c->stream;
+    CG_CUDA(cudaMemcpyAsync(c->d_states, soa.data(), soa.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(c->d_V, v.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemsetAsync(c->d_iion, 0, n * sizeof(T), s));
+    CG_CUDA(cudaMemsetAsync(c->d_z, 0, n * sizeof(T), s));
+    std::vector<uint8_t> ps;
+    std::vector<T> tab;
+    if (pset && ptab && nsets > 0) {
+        if (nsets > 255) return CG_ERR_ARG;
+        ps.resize(n);
+        for (size_t i = 0; i < n; ++i) {
+            if (pset[i] < 0 || pset[i] >= nsets) return CG_ERR_ARG;
+            ps[i] = (uint8_t)pset[i];
+        }
+        tab.resize((size_t)nsets * P);
+        for (size_t k = 0; k < tab.size(); ++k) tab[k] = (T)ptab[k];
+        if (!c->d_pset) CG_TRY(dalloc(c, &c->d_pset, n));
+        T* dp = nullptr;
+        CG_TRY(dalloc(c, &dp, tab.size() * sizeof(T)));
+        c->d_params = dp;
+        CG_CUDA(cudaMemcpyAsync(c->d_pset, ps.data(), n, cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(c->d_params, tab.data(), tab.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    } else {
+        c->d_pset = nullptr;
+        c->d_params = nullptr;
+    }
+    std::vector<double> neg(n, -1.0);
+    CG_CUDA(cudaMemcpyAsync(c->d_act, neg.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemsetAsync(c->d_step, 0, sizeof(long long), s));
+    CG_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(int), s));
+    CG_CUDA(cudaStreamSynchronize(s));
+    c->steps = 0;
+    c->total_iters = 0;
+    c->max_iters = 0;
+    return CG_OK;
+}
+
+template <class M, typename T>
+void launch_ode(cg_ctx* c) {
+    OdeArgs<T> a;
+    a.n = c->n;
+    a.V = c->d_V;
+    a.states = (T*)c->d_states;
+    a.iion = (T*)c->d_iion;
+    a.zrhs = (T*)c->d_z;
+    a.stim_id = c->d_stim_id;
+    a.stims = c->d_stims;
+    a.pset = c->d_pset;
+    a.params = (const T*)c->d_params;
+    a.step = c->d_step;
+    a.status = c->d_status;
+    a.dt_ode = c->cfg.ode_time_step;
+    a.dt_pde = c->cfg.pde_time_step;
+    a.am = c->cfg.surface_area_to_volume_ratio;
+    a.cm = c->cfg.capacitance;
+    a.check_range = c->cfg.check_state_ranges;
+    a.act = c->d_act;
+    a.act_threshold = c->cfg.activation_threshold;
+    if (c->cfg.ode_method == CG_ODE_RUSH_LARSEN)
+        ode_kernel<M, T, 1><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+    else
+        ode_kernel<M, T, 0><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+}
+
+CgArgs make_cg_args(cg_ctx* c) {
+    CgArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = c->n;
+    if (c->slab) {
+        const SlabStencil& st = c->stencil;
+        a.slab.n_off = st.n_offsets;
+        a.slab.n_cls = st.n_classes;
+        for (int o = 0; o < st.n_offsets; ++o) a.slab.off[o] = st.offsets[o];
+        a.slab.a_tab = c->d_atab;
+        a.slab.m_tab = c->d_mtab;
+        a.slab.a_tab32 = c->d_atab32;
+        a.slab.m_tab32 = c->d_mtab32;
+    } else {
+        a.csr.rowptr = c->d_rowptr;
+        a.csr.cols = c->d_cols;
+        a.csr.a = c->d_aval;
+        a.csr.m = c->d_mval;
+        a.csr.dinv = c->d_dinv;
+        a.csr.a32 = c->d_aval32;
+        a.csr.dinv32 = c->d_dinv32;
+    }
+    a.x = c->d_V;
+    a.zrhs = c->mixed() ? nullptr : (const double*)c->d_z;
+    a.zrhs32 = c->mixed() ? (const float*)c->d_z : nullptr;
+    a.cls8 = c->d_cls8;
+    a.r = c->d_r;
+    a.p0 = c->d_p0;
+    a.p1 = c->d_p1;
+    a.q = c->d_q;
+    a.r32 = c->d_r32;
+    a.p32a = c->d_p32a;
+    a.p32b = c->d_p32b;
+    a.e32 = c->d_e32;
+    a.q32 = c->d_q32;
+    a.partials = c->d_partials;
+    a.gs = c->d_gs;
+    a.status = c->d_status;
+    a.step = c->d_step;
+    a.iters_ring = c->d_ring;
+    a.ring = kRing;
+    a.refine_out = c->d_refine;
+    // KSPSetTolerances as LinearSystem sets them (LinearSystem.cpp:584-602, 755-762)
+    a.rtol = c->cfg.use_absolute_tolerance ? DBL_EPSILON : c->cfg.ksp_tolerance;
+    a.abstol = c->cfg.use_absolute_tolerance ? c->cfg.ksp_tolerance : 1e-50;
+    a.dtol = 1e5;
+    a.maxit = c->cfg.max_iterations;
+    a.pc = c->cfg.ksp_preconditioner == CG_PC_JACOBI ? 1 : 0;
+    a.diag_slot = c->diag_slot;
+    a.max_refine = 20;
+    return a;
+}
+
+cudaError_t launch_cg(cg_ctx* c) {
+    CgArgs a = make_cg_args(c);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c->cg_blocks);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (c->mixed()) {
+        if (c->slab) return cudaLaunchKernelEx(&cfg, cg_mixed_kernel<true>, a);
+        return cudaLaunchKernelEx(&cfg, cg_mixed_kernel<false>, a);
+    }
+    if (c->slab) return cudaLaunchKernelEx(&cfg, cg_fp64_kernel<true>, a);
+    return cudaLaunchKernelEx(&cfg, cg_fp64_kernel<false>, a);
+}
+
+cudaError_t launch_step(cg_ctx* c) {
+    const bool tt = c->cfg.model == CG_MODEL_TT06;
+    if (c->mixed()) {
+        if (tt) launch_ode<TenTusscher2006Epi, float>(c);
+        else launch_ode<LuoRudy1991, float>(c);
+    } else {
+        if (tt) launch_ode<TenTusscher2006Epi, double>(c);
+        else launch_ode<LuoRudy1991, double>(c);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_cg(c);
+}
+
+int build_graph(cg_ctx* c) {
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return CG_ERR_CUDA;
+    }
+    cudaError_t le = launch_step(c);
+    cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        return CG_ERR_CUDA;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        cudaGetLastError();
+        c->graph = nullptr;
+        return CG_ERR_CUDA;
+    }
+    return CG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cg_set_cells(cg_ctx* c, const double* init_states, const int* param_set, const double* param_table,
+                 int n_param_sets) {
+    if (!c) return CG_ERR_ARG;
+    if (!c->have_mesh) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    const int rc = c->mixed() ? upload_cells_t<float>(c, init_states, param_set, param_table, n_param_sets)
+                              : upload_cells_t<double>(c, init_states, param_set, param_table, n_param_sets);
+    if (rc != CG_OK) return rc;
+    c->have_cells = true;
+    c->graph_dirty = true;
+    return CG_OK;
+}
+
+int cg_set_stimulus(cg_ctx* c, const int* stim_id, const cg_stimulus* stims, int n_stims) {
+    if (!c || n_stims < 0 || n_stims > 255 || (n_stims > 0 && (!stims || !stim_id))) return CG_ERR_ARG;
+    if (!c->have_mesh) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->n;
+    std::vector<uint8_t> ids(n, 0xFF);
+    std::vector<int> host_ids(n, -1);
+    if (stim_id)
+        for (size_t i = 0; i < n; ++i) {
+            if (stim_id[i] >= n_stims) return CG_ERR_ARG;
+            if (stim_id[i] >= 0) {
+                ids[i] = (uint8_t)stim_id[i];
+                host_ids[i] = stim_id[i];
+            }
+        }
+    std::vector<DevStimulus> d(std::max(1, n_stims));
+    for (int k = 0; k < n_stims; ++k) {
+        if (stims[k].kind == CG_STIM_REGULAR && !(stims[k].period > 0)) return CG_ERR_ARG;
+        if (stims[k].kind < CG_STIM_NONE || stims[k].kind > CG_STIM_REGULAR) return CG_ERR_ARG;
+        d[k] = to_dev(stims[k]);
+    }
+    CG_TRY(ensure_stimulus_buffers(c));
+    c->stim_id_host = host_ids;
+    c->stims_host.assign(stims, stims + n_stims);
+    CG_CUDA(cudaMemcpyAsync(c->d_stim_id, ids.data(), n, cudaMemcpyHostToDevice, c->stream));
+    CG_CUDA(cudaMemcpyAsync(c->d_stims, d.data(), d.size() * sizeof(DevStimulus), cudaMemcpyHostToDevice, c->stream));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    c->graph_dirty = true;
+    return CG_OK;
+}
+
+int cg_step(cg_ctx* c, int n_steps) {
+    if (!c || n_steps < 0) return CG_ERR_ARG;
+    if (!c->have_mesh || !c->have_cells) return CG_ERR_ORDER;
+    if (n_steps == 0) return CG_OK;
+    CG_CUDA(cudaSetDevice(c->device));
+    if (c->graph_dirty) {
+        if (build_graph(c) != CG_OK) c->graph = nullptr;   // plain launches instead
+        c->graph_dirty = false;
+    }
+    CG_CUDA(cudaEventRecord(c->ev0, c->stream));
+    for (int k = 0; k < n_steps; ++k) {
+        const cudaError_t e = c->graph ? cudaGraphLaunch(c->graph, c->stream) : launch_step(c);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return CG_ERR_CUDA;
+        }
+    }
+    CG_CUDA(cudaEventRecord(c->ev1, c->stream));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->ms_last = ms;
+    int bits = 0;
+    long long dstep = 0;
+    CG_CUDA(cudaMemcpy(&bits, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    CG_CUDA(cudaMemcpy(&dstep, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost));
+    const long long from = std::max(c->steps, dstep - kRing);
+    if (dstep > from) {
+        std::vector<int> ring(kRing);
+        CG_CUDA(cudaMemcpy(ring.data(), c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost));
+        for (long long s = from; s < dstep; ++s) {
+            const int it = ring[s % kRing];
+            c->total_iters += it;
+            c->max_iters = std::max(c->max_iters, it);
+        }
+    }
+    c->steps = dstep;
+    return status_from_bits(bits);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- getters --
+namespace {
+
+template <typename T>
+int read_states_t(cg_ctx* c, double* out, int node) {
+    const size_t n = (size_t)c->n;
+    const int S = c->n_states;
+    if (node >= 0) {
+        CG_CUDA(cudaMemcpy(out, c->d_V + node, sizeof(double), cudaMemcpyDeviceToHost));
+        for (int k = 1; k < S; ++k) {
+            T x;
+            CG_CUDA(cudaMemcpy(&x, (T*)c->d_states + (size_t)(k - 1) * n + node, sizeof(T), cudaMemcpyDeviceToHost));
+            out[k] = (double)x;
+        }
+        return CG_OK;
+    }
+    std::vector<double> v(n);
+    CG_CUDA(cudaMemcpy(v.data(), c->d_V, n * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<T> soa((size_t)(S - 1) * n);
+    CG_CUDA(cudaMemcpy(soa.data(), c->d_states, soa.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) {
+        out[i * S] = v[i];
+        for (int k = 1; k < S; ++k) out[i * S + k] = (double)soa[(size_t)(k - 1) * n + i];
+    }
+    return CG_OK;
+}
+
+template <typename T>
+int read_vec_t(const void* d, size_t n, double* out) {
+    std::vector<T> h(n);
+    CG_CUDA(cudaMemcpy(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) out[i] = (double)h[i];
+    return CG_OK;
+}
+
+struct SnapshotHeader {
+    char magic[8];
+    int n, n_states, model, precision;
+    long long step;
+    long long bytes;
+};
+
+}  // namespace
+
+extern "C" {
+
+int cg_get_voltage(cg_ctx* c, double* v) {
+    if (!c || !v) return CG_ERR_ARG;
+    if (!c->have_cells) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaMemcpy(v, c->d_V, (size_t)c->n * sizeof(double), cudaMemcpyDeviceToHost));
+    return CG_OK;
+}
+
+int cg_set_voltage(cg_ctx* c, const double* v) {
+    if (!c || !v) return CG_ERR_ARG;
+    if (!c->have_cells) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaMemcpy(c->d_V, v, (size_t)c->n * sizeof(double), cudaMemcpyHostToDevice));
+    return CG_OK;
+}
+
+int cg_get_states(cg_ctx* c, double* states) {
+    if (!c || !states) return CG_ERR_ARG;
+    if (!c->have_cells) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    return c->mixed() ? read_states_t<float>(c, states, -1) : read_states_t<double>(c, states, -1);
+}
+
+int cg_get_cell_state(cg_ctx* c, int node, double* state) {
+    if (!c || !state) return CG_ERR_ARG;
+    if (!c->have_cells) return CG_ERR_ORDER;
+    if (node < 0 || node >= c->n) return CG_ERR_ARG;
+    CG_CUDA(cudaSetDevice(c->device));
+    return c->mixed() ? read_states_t<float>(c, state, node) : read_states_t<double>(c, state, node);
+}
+
+int cg_get_caches(cg_ctx* c, double* iion, double* istim) {
+    if (!c) return CG_ERR_ARG;
+    if (!c->have_cells) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    if (iion) CG_TRY(c->mixed() ? read_vec_t<float>(c->d_iion, c->n, iion) : read_vec_t<double>(c->d_iion, c->n, iion));
+    if (istim) {
+        // the cache holds GetIntracellularStimulus(t_{n+1}) of the last step
+        const double t = (double)c->steps * c->cfg.pde_time_step;
+        for (int i = 0; i < c->n; ++i) {
+            const int s = c->stim_id_host.empty() ? -1 : c->stim_id_host[i];
+            istim[i] = (s >= 0 && c->steps > 0) ? host_stim(c->stims_host[s], t) : 0.0;
+        }
+    }
+    return CG_OK;
+}
+
+int cg_get_activation_times(cg_ctx* c, double* t) {
+    if (!c || !t) return CG_ERR_ARG;
+    if (!c->have_cells) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    const double now = (double)c->steps * c->cfg.pde_time_step;
+    activation_kernel<<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, c->d_act, c->cfg.activation_threshold, now);
+    CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    CG_CUDA(cudaMemcpy(t, c->d_act, (size_t)c->n * sizeof(double), cudaMemcpyDeviceToHost));
+    return CG_OK;
+}
+
+int cg_get_stats(cg_ctx* c, cg_stats* s) {
+    if (!c || !s) return CG_ERR_ARG;
+    std::memset(s, 0, sizeof(*s));
+    s->steps = c->steps;
+    s->time = (double)c->steps * c->cfg.pde_time_step;
+    s->total_cg_iterations = c->total_iters;
+    s->max_cg_iterations = c->max_iters;
+    s->operator_kind = c->slab ? 1 : 0;
+    s->ms_last_call = c->ms_last;
+    if (c->have_cells && c->steps > 0) {
+        CG_CUDA(cudaSetDevice(c->device));
+        CG_CUDA(cudaMemcpy(&s->last_cg_iterations, c->d_ring + ((c->steps - 1) % kRing), sizeof(int),
+                           cudaMemcpyDeviceToHost));
+        CG_CUDA(cudaMemcpy(&s->refinement_sweeps, c->d_refine, sizeof(int), cudaMemcpyDeviceToHost));
+        CG_CUDA(cudaMemcpy(&s->status_bits, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    return CG_OK;
+}
+
+int cg_get_iteration_history(cg_ctx* c, int n, int* it) {
+    if (!c || !it || n < 0) return CG_ERR_ARG;
+    const long long avail = std::min<long long>(c->steps, kRing);
+    const long long m = std::min<long long>(n, avail);
+    if (m > 0) {
+        CG_CUDA(cudaSetDevice(c->device));
+        std::vector<int> ring(kRing);
+        CG_CUDA(cudaMemcpy(ring.data(), c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost));
+        for (long long k = 0; k < m; ++k) it[k] = ring[(c->steps - m + k) % kRing];
+    }
+    for (long long k = m; k < n; ++k) it[k] = 0;
+    return CG_OK;
+}
+
+int cg_snapshot_size(cg_ctx* c, size_t* bytes) {
+    if (!c || !bytes) return CG_ERR_ARG;
+    if (!c->have_cells) return CG_ERR_ORDER;
+    const size_t n = (size_t)c->n, w = c->real_size();
+    *bytes = sizeof(SnapshotHeader) + n * sizeof(double) * 2 + (size_t)(c->n_states - 1) * n * w + 2 * n * w;
+    return CG_OK;
+}
+
+int cg_snapshot(cg_ctx* c, void* buf, size_t bytes) {
+    size_t need = 0;
+    CG_TRY(cg_snapshot_size(c, &need));
+    if (!buf || bytes < need) return CG_ERR_ARG;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)c->n, w = c->real_size();
+    SnapshotHeader h{};
+    std::memcpy(h.magic, "CHBSNAP1", 8);
+    h.n = c->n;
+    h.n_states = c->n_states;
+    h.model = c->cfg.model;
+    h.precision = c->cfg.precision;
+    h.step = c->steps;
+    h.bytes = (long long)need;
+    char* p = (char*)buf;
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    CG_CUDA(cudaMemcpy(p, c->d_V, n * sizeof(double), cudaMemcpyDeviceToHost));
+    p += n * sizeof(double);
+    CG_CUDA(cudaMemcpy(p, c->d_act, n * sizeof(double), cudaMemcpyDeviceToHost));
+    p += n * sizeof(double);
+    CG_CUDA(cudaMemcpy(p, c->d_states, (size_t)(c->n_states - 1) * n * w, cudaMemcpyDeviceToHost));
+    p += (size_t)(c->n_states - 1) * n * w;
+    CG_CUDA(cudaMemcpy(p, c->d_iion, n * w, cudaMemcpyDeviceToHost));
+    p += n * w;
+    CG_CUDA(cudaMemcpy(p, c->d_z, n * w, cudaMemcpyDeviceToHost));
+    return CG_OK;
+}
+
+int cg_restore(cg_ctx* c, const void* buf, size_t bytes) {
+    size_t need = 0;
+    CG_TRY(cg_snapshot_size(c, &need));
+    if (!buf || bytes < need) return CG_ERR_ARG;
+    SnapshotHeader h;
+    std::memcpy(&h, buf, sizeof(h));
+    if (std::memcmp(h.magic, "CHBSNAP1", 8) != 0 || h.n != c->n || h.n_states != c->n_states ||
+        h.model != c->cfg.model || h.precision != c->cfg.precision || h.bytes != (long long)need)
+        return CG_ERR_ARG;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)c->n, w = c->real_size();
+    const char* p = (const char*)buf + sizeof(h);
+    CG_CUDA(cudaMemcpy(c->d_V, p, n * sizeof(double), cudaMemcpyHostToDevice));
+    p += n * sizeof(double);
+    CG_CUDA(cudaMemcpy(c->d_act, p, n * sizeof(double), cudaMemcpyHostToDevice));
+    p += n * sizeof(double);
+    CG_CUDA(cudaMemcpy(c->d_states, p, (size_t)(c->n_states - 1) * n * w, cudaMemcpyHostToDevice));
+    p += (size_t)(c->n_states - 1) * n * w;
+    CG_CUDA(cudaMemcpy(c->d_iion, p, n * w, cudaMemcpyHostToDevice));
+    p += n * w;
+    CG_CUDA(cudaMemcpy(c->d_z, p, n * w, cudaMemcpyHostToDevice));
+    CG_CUDA(cudaMemcpy(c->d_step, &h.step, sizeof(long long), cudaMemcpyHostToDevice));
+    CG_CUDA(cudaMemset(c->d_status, 0, sizeof(int)));
+    c->steps = h.step;
+    return CG_OK;
+}
+
+}  // extern "C"

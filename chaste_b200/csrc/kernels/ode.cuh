@@ -1,0 +1,97 @@
+// Ionic ODE update of every tissue node with the voltage clamped
+// (AbstractCardiacTissue::SolveCellSystems, heart/src/tissue/AbstractCardiacTissue.cpp:464-567),
+// fused with the Iion cache (UpdateCaches, :730-734) and the per-node RHS term
+// z = Am*Cm*V/dt - Am*Iion - Istim(t+dt) (MonodomainSolver.cpp:92-101).
+//
+// Layout: states are structure-of-arrays, row k-1 holds state k (k >= 1) of
+// every node, so a warp reads 32 consecutive values of one state (coalesced).
+// V is FP64 (it is the CG solution); the states, Iion and z use T.
+#pragma once
+
+#include "../models/lr91.h"
+#include "../models/tt06.h"
+#include "common.cuh"
+
+namespace chb {
+
+template <typename T>
+struct OdeArgs {
+    int n;
+    const double* __restrict__ V;
+    T* __restrict__ states;             // (S-1) x n
+    T* __restrict__ iion;               // n
+    T* __restrict__ zrhs;               // n
+    const uint8_t* __restrict__ stim_id;  // n, 0xFF = none
+    const DevStimulus* __restrict__ stims;
+    const uint8_t* __restrict__ pset;   // n (may be null)
+    const T* __restrict__ params;       // nsets x P
+    const long long* __restrict__ step; // device step counter
+    int* status;
+    double dt_ode, dt_pde, am, cm;
+    int check_range;
+    double* act;                        // first activation time per node (-1: none yet)
+    double act_threshold;
+};
+
+// First step with V above the threshold (ActivationOutputModifier::ProcessSolutionAtTimeStep,
+// heart/src/problem/ActivationOutputModifier.cpp:91-101), checked once per PDE step.
+__global__ void activation_kernel(int n, const double* __restrict__ V, double* __restrict__ act,
+                                  double threshold, double t) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (V[i] > threshold && act[i] < 0.0) act[i] = t;
+}
+
+template <class M, typename T, int METHOD>
+__global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
+    constexpr int S = M::kNumStates;
+    constexpr int P = M::kNumParams;
+    if (*(volatile int*)a.status & ~kStatusStateRange) return;   // a failed step stops the run
+    const long long step = *a.step;
+    const double t0 = (double)step * a.dt_pde;
+    const double t1 = (double)(step + 1) * a.dt_pde;
+    const double dtinv = 1.0 / a.dt_pde;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        T y[S];
+        const double v = a.V[i];
+        // activation bookkeeping of the previous step's solution (time t0)
+        if (v > a.act_threshold && a.act[i] < 0.0) a.act[i] = t0;
+        y[0] = (T)v;
+#pragma unroll
+        for (int k = 1; k < S; ++k) y[k] = a.states[(size_t)(k - 1) * a.n + i];
+        T p[P > 0 ? P : 1];
+        if (a.pset) {
+            const T* pp = a.params + (size_t)a.pset[i] * P;
+#pragma unroll
+            for (int k = 0; k < P; ++k) p[k] = pp[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < P; ++k) p[k] = T(1);
+        }
+        const int sid = a.stim_id[i];
+        DevStimulus st{0, 0, 0, 0, 0, 0};
+        if (sid != 0xFF) st = a.stims[sid];
+        const T cm = (T)a.cm;
+        DevTimeStepper ts(t0, t1, a.dt_ode);
+        while (!ts.at_end()) {
+            // cell stimulus in uA/cm^2 = tissue stimulus / Am (GetIntracellularAreaStimulus)
+            const T s = (T)(stimulus_value(st, ts.time) / a.am);
+            if (METHOD == 1) {
+                rl_step_except_voltage<M, T>(y, s, cm, p, (T)a.dt_ode);
+            } else {
+                fe_step_except_voltage<M, T>(y, s, cm, p, (T)(ts.next - ts.time));
+            }
+            ts.advance();
+        }
+#pragma unroll
+        for (int k = 1; k < S; ++k) a.states[(size_t)(k - 1) * a.n + i] = y[k];
+        y[0] = (T)v;
+        const T ii = M::template iionic<T>(y, cm, p);
+        a.iion[i] = ii;
+        const double istim = stimulus_value(st, t1);
+        const double F = -a.am * (double)ii - istim;
+        a.zrhs[i] = (T)(a.am * a.cm * v * dtinv + F);
+        if (a.check_range && !states_in_range<M, T>(y)) atomicOr(a.status, kStatusStateRange);
+    }
+}
+
+}  // namespace chb

@@ -1,0 +1,92 @@
+// Sparse operators of the diffusion solve: the assembled CSR (any mesh) and the
+// matrix-free slab stencil (ConstructRegularSlabMesh meshes with uniform sigma).
+#pragma once
+
+#include "common.cuh"
+
+namespace chb {
+
+constexpr int kMaxOffsets = 27;
+constexpr int kMaxClasses = 27;
+
+// Matrix-free operator of a regular slab: the row of node i is the row of its
+// boundary class (3 per axis; x2 for the stagger parity in 2D) in a small
+// coefficient table, so a product streams only the vector and a 1-byte class
+// per node.  Offsets are in ascending column order, the order a sorted CSR row
+// sums in.
+struct SlabOp {
+    int n_off, n_cls;
+    int off[kMaxOffsets];
+    const double* a_tab;   // [cls][off]
+    const double* m_tab;
+    const float* a_tab32;
+    const float* m_tab32;
+};
+
+// Shared-memory copy of the slab tables, filled at kernel start.
+template <typename T>
+struct SlabShared {
+    T a[kMaxClasses * kMaxOffsets];
+    T m[kMaxClasses * kMaxOffsets];
+    T dinv[kMaxClasses];
+    int off[kMaxOffsets];
+};
+
+template <typename T>
+__device__ void slab_load_shared(const SlabOp& op, SlabShared<T>& sh, int diag_slot) {
+    const T* at;
+    const T* mt;
+    if constexpr (sizeof(T) == 8) {
+        at = reinterpret_cast<const T*>(op.a_tab);
+        mt = reinterpret_cast<const T*>(op.m_tab);
+    } else {
+        at = reinterpret_cast<const T*>(op.a_tab32);
+        mt = reinterpret_cast<const T*>(op.m_tab32);
+    }
+    const int tot = op.n_cls * op.n_off;
+    for (int k = threadIdx.x; k < tot; k += blockDim.x) {
+        sh.a[k] = at[k];
+        sh.m[k] = mt[k];
+    }
+    for (int k = threadIdx.x; k < op.n_off; k += blockDim.x) sh.off[k] = op.off[k];
+    __syncthreads();
+    for (int c = threadIdx.x; c < op.n_cls; c += blockDim.x) {
+        const T d = sh.a[c * op.n_off + diag_slot];
+        sh.dinv[c] = d != T(0) ? T(1) / d : T(0);
+    }
+    __syncthreads();
+}
+
+// sum_o coef[o] * ld(i + off[o]) over the nonzero coefficients (a zero marks a
+// neighbour outside the slab, whose index is never formed into a load)
+template <typename T, typename Acc, class Load>
+__device__ __forceinline__ Acc slab_row(const T* coef, const int* off, int n_off, int i, Load ld) {
+    Acc acc = Acc(0);
+    for (int o = 0; o < n_off; ++o) {
+        const T c = coef[o];
+        if (c != T(0)) acc += (Acc)c * (Acc)ld(i + off[o]);
+    }
+    return acc;
+}
+
+// Assembled operator: A and M share one sorted CSR pattern.
+struct CsrOp {
+    const int* __restrict__ rowptr;
+    const int* __restrict__ cols;
+    const double* __restrict__ a;
+    const double* __restrict__ m;
+    const double* __restrict__ dinv;     // 1 / diag(A)
+    const float* __restrict__ a32;
+    const float* __restrict__ dinv32;
+};
+
+template <typename T, typename Acc, class Load>
+__device__ __forceinline__ Acc csr_row(const int* __restrict__ rp, const int* __restrict__ ci,
+                                       const T* __restrict__ v, int i, Load ld) {
+    Acc acc = Acc(0);
+    const int e = rp[i + 1];
+    for (int k = rp[i]; k < e; ++k) acc += (Acc)v[k] * (Acc)ld(ci[k]);
+    return acc;
+}
+
+}  // namespace chb

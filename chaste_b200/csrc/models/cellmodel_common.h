@@ -47,7 +47,7 @@ CHB_HD void rl_step_except_voltage(T* y, T stim, T cm, const T* p, T dt) {
     Model::template rl_terms<T>(y, stim, cm, p, rate, inf);
 CHB_UNROLL
     for (int i = 1; i < Model::kNumStates; ++i) {
-        if (Model::kRushLarsen[i]) {
+        if (Model::rush_larsen(i)) {
             y[i] = inf[i] + (y[i] - inf[i]) * exp(rate[i] * dt);
         } else {
             y[i] += dt * rate[i];
@@ -75,7 +75,7 @@ CHB_HD void rl_step(T* y, T stim, T cm, const T* p, T dt) {
     y[0] += dt * rate[0];
 CHB_UNROLL
     for (int i = 1; i < Model::kNumStates; ++i) {
-        if (Model::kRushLarsen[i]) {
+        if (Model::rush_larsen(i)) {
             y[i] = inf[i] + (y[i] - inf[i]) * exp(rate[i] * dt);
         } else {
             y[i] += dt * rate[i];
@@ -91,8 +91,8 @@ CHB_HD bool states_in_range(const T* y) {
 CHB_UNROLL
     for (int i = 0; i < Model::kNumStates; ++i) {
         const T v = y[i];
-        if (Model::kRangeClass[i] == 1) ok = ok && (v >= T(0) && v <= T(1));
-        else if (Model::kRangeClass[i] == 2) ok = ok && (v > T(0));
+        if (Model::range_class(i) == 1) ok = ok && (v >= T(0) && v <= T(1));
+        else if (Model::range_class(i) == 2) ok = ok && (v > T(0));
         else ok = ok && (v == v);
     }
     return ok;

@@ -15,13 +15,15 @@ struct LuoRudy1991 {
     static constexpr const char* kParamNames[6] = {"g_Na", "g_si", "g_K", "g_K1", "g_Kp", "g_b"};
     // 1 where the state is advanced by Rush-Larsen (ODE affine in itself)
     static constexpr bool kRushLarsen[8] = {false, true, true, true, true, true, true, false};
+    CHB_HD static constexpr bool rush_larsen(int i) { return i == 1 || i == 2 || i == 3 || i == 4 || i == 5 || i == 6; }
     // range class per state: 1 gate in [0,1], 2 concentration > 0, 0 unchecked
     static constexpr int kRangeClass[8] = {0, 1, 1, 1, 1, 1, 1, 2};
+    CHB_HD static constexpr int range_class(int i) { return (i == 1 || i == 2 || i == 3 || i == 4 || i == 5 || i == 6) ? 1 : ((i == 7) ? 2 : 0); }
 
     // dy/dt for every state at (y, stim) where stim is the Chaste area stimulus
     // in uA/cm^2 and cm the Chaste capacitance in uF/cm^2.  y[0] is the voltage.
     template <typename T>
-    CHB_HD static inline void rhs(const T* __restrict__ y, T stim, T cm,
+    CHB_HD static void rhs(const T* __restrict__ y, T stim, T cm,
                                   const T* __restrict__ p, T* __restrict__ dy) {
         (void)stim; (void)cm; (void)p;
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
@@ -65,7 +67,7 @@ struct LuoRudy1991 {
     // the (negative) affine coefficient h so y' = inf + (y - inf)*exp(h*dt);
     // for the other states rate[i] holds dy/dt.  rate[0] is dV/dt.
     template <typename T>
-    CHB_HD static inline void rl_terms(const T* __restrict__ y, T stim, T cm,
+    CHB_HD static void rl_terms(const T* __restrict__ y, T stim, T cm,
                                        const T* __restrict__ p, T* __restrict__ rate,
                                        T* __restrict__ inf) {
         (void)stim; (void)cm; (void)p; (void)inf;
@@ -115,7 +117,7 @@ struct LuoRudy1991 {
     // Total ionic current in uA/cm^2 (GetIIonic): the dV/dt currents without
     // the stimulus.
     template <typename T>
-    CHB_HD static inline T iionic(const T* __restrict__ y, T cm, const T* __restrict__ p) {
+    CHB_HD static T iionic(const T* __restrict__ y, T cm, const T* __restrict__ p) {
         (void)cm; (void)p;
         const T stim = T(0.0); (void)stim;
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));

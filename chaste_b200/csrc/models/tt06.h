@@ -15,13 +15,15 @@ struct TenTusscher2006Epi {
     static constexpr const char* kParamNames[9] = {"g_Na", "g_CaL", "g_Kr", "g_Ks", "g_K1", "g_to", "ScaleFactorGks", "ScaleFactorGkr", "ScaleFactorIto"};
     // 1 where the state is advanced by Rush-Larsen (ODE affine in itself)
     static constexpr bool kRushLarsen[19] = {false, true, true, true, true, true, true, true, true, true, true, true, true, true, false, false, false, false, false};
+    CHB_HD static constexpr bool rush_larsen(int i) { return i == 1 || i == 2 || i == 3 || i == 4 || i == 5 || i == 6 || i == 7 || i == 8 || i == 9 || i == 10 || i == 11 || i == 12 || i == 13; }
     // range class per state: 1 gate in [0,1], 2 concentration > 0, 0 unchecked
     static constexpr int kRangeClass[19] = {0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2};
+    CHB_HD static constexpr int range_class(int i) { return (i == 1 || i == 2 || i == 3 || i == 4 || i == 5 || i == 6 || i == 7 || i == 8 || i == 9 || i == 10 || i == 11 || i == 12 || i == 13) ? 1 : ((i == 14 || i == 15 || i == 16 || i == 17 || i == 18) ? 2 : 0); }
 
     // dy/dt for every state at (y, stim) where stim is the Chaste area stimulus
     // in uA/cm^2 and cm the Chaste capacitance in uF/cm^2.  y[0] is the voltage.
     template <typename T>
-    CHB_HD static inline void rhs(const T* __restrict__ y, T stim, T cm,
+    CHB_HD static void rhs(const T* __restrict__ y, T stim, T cm,
                                   const T* __restrict__ p, T* __restrict__ dy) {
         (void)stim; (void)cm; (void)p;
         const T v_L_type_Ca_current__i_CaL = (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0)));
@@ -119,7 +121,7 @@ struct TenTusscher2006Epi {
     // the (negative) affine coefficient h so y' = inf + (y - inf)*exp(h*dt);
     // for the other states rate[i] holds dy/dt.  rate[0] is dV/dt.
     template <typename T>
-    CHB_HD static inline void rl_terms(const T* __restrict__ y, T stim, T cm,
+    CHB_HD static void rl_terms(const T* __restrict__ y, T stim, T cm,
                                        const T* __restrict__ p, T* __restrict__ rate,
                                        T* __restrict__ inf) {
         (void)stim; (void)cm; (void)p; (void)inf;
@@ -230,7 +232,7 @@ struct TenTusscher2006Epi {
     // Total ionic current in uA/cm^2 (GetIIonic): the dV/dt currents without
     // the stimulus, times the capacitance cm.
     template <typename T>
-    CHB_HD static inline T iionic(const T* __restrict__ y, T cm, const T* __restrict__ p) {
+    CHB_HD static T iionic(const T* __restrict__ y, T cm, const T* __restrict__ p) {
         (void)cm; (void)p;
         const T stim = T(0.0); (void)stim;
         const T v_L_type_Ca_current__i_CaL = (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0)));

@@ -1,0 +1,160 @@
+/*
+ * libchastegpu -- B200 monodomain tissue behind a plain C ABI.
+ *
+ * One context holds one monodomain tissue resident on one GPU: the mesh
+ * operators (A = Am*Cm/dt*M + K and M), the cell states in
+ * structure-of-arrays layout, the voltage, the Iion/Istim caches and the CG
+ * workspace.  A PDE step is the operator-split step Chaste takes in
+ * AbstractDynamicLinearPdeSolver::Solve (pde/src/solver/AbstractDynamicLinearPdeSolver.hpp:372-469):
+ *   1. the ionic ODEs of every node with V clamped
+ *      (AbstractCardiacTissue::SolveCellSystems, heart/src/tissue/AbstractCardiacTissue.cpp:464-567),
+ *   2. b = M (Am*Cm*V/dt - Am*Iion - Istim)
+ *      (MonodomainSolver::SetupLinearSystem, heart/src/solver/electrics/monodomain/MonodomainSolver.cpp:42-131),
+ *   3. CG on A V' = b from the guess V (LinearSystem::Solve, linalg/src/LinearSystem.cpp:674-1215),
+ * all on the device; host memory is touched only by the set/get calls.
+ *
+ * Every call returns a cg_status (0 = CG_OK).  No C++ exception crosses the
+ * ABI.  A context is bound to one CUDA device and one stream; calls on the
+ * same context must not run concurrently.
+ */
+#ifndef CHASTE_GPU_H
+#define CHASTE_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cg_ctx cg_ctx;
+
+/* Status codes.  CG_ERR_CG_MAXIT / CG_ERR_CG_DIVERGED are the KSP failures
+ * Chaste turns into an exception (KSPEXCEPT, linalg/src/LinearSystem.cpp:1119-1129);
+ * CG_ERR_STATE_RANGE mirrors VerifyStateVariables. */
+typedef enum {
+    CG_OK = 0,
+    CG_ERR_ARG = 1,           /* invalid argument */
+    CG_ERR_CUDA = 2,          /* CUDA runtime error (or no device) */
+    CG_ERR_CG_MAXIT = 3,      /* KSP_DIVERGED_ITS */
+    CG_ERR_CG_DIVERGED = 4,   /* KSP_DIVERGED_DTOL / indefinite matrix */
+    CG_ERR_NAN = 5,           /* KSP_DIVERGED_NANORINF */
+    CG_ERR_STATE_RANGE = 6,   /* a gate left [0,1] or a concentration became <= 0 */
+    CG_ERR_ORDER = 7,         /* calls made in the wrong order */
+    CG_ERR_TIMEOUT = 8,       /* a device-side grid barrier gave up (bounded wait) */
+    CG_ERR_NOMEM = 9,         /* device allocation failed */
+    CG_ERR_UNSUPPORTED = 10
+} cg_status;
+
+enum { CG_MODEL_LR91 = 0, CG_MODEL_TT06 = 1 };
+enum { CG_ODE_FORWARD_EULER = 0, CG_ODE_RUSH_LARSEN = 1 };
+enum { CG_PC_NONE = 0, CG_PC_JACOBI = 1, CG_PC_BJACOBI = 2 };
+enum { CG_PRECISION_FP64 = 0, CG_PRECISION_MIXED = 1 };
+enum { CG_STIM_NONE = 0, CG_STIM_SIMPLE = 1, CG_STIM_REGULAR = 2 };
+
+/* HeartConfig fields used by the path (heart/src/problem/HeartConfig.cpp:1581-1650,
+ * 2337-2412; defaults heart/src/problem/HeartConfigDefaults.hpp:53-91). */
+typedef struct {
+    int model;                 /* CG_MODEL_* */
+    int ode_method;            /* CG_ODE_* */
+    double ode_time_step;      /* ms */
+    double pde_time_step;      /* ms */
+    double surface_area_to_volume_ratio;  /* Am, 1/cm (default 1400) */
+    double capacitance;        /* Cm, uF/cm^2 (default 1) */
+    int ksp_preconditioner;    /* CG_PC_*; bjacobi is rejected (CG_ERR_UNSUPPORTED) */
+    int use_absolute_tolerance;/* 1: KSPSetTolerances(DBL_EPSILON, tol); 0: (tol, default) */
+    double ksp_tolerance;
+    int use_mass_lumping;
+    int max_iterations;        /* 0 -> PETSc default 10000 */
+    int precision;             /* CG_PRECISION_* */
+    int device;                /* CUDA device ordinal */
+    int check_state_ranges;    /* 1: device-side VerifyStateVariables analogue */
+    double activation_threshold; /* mV; activation time = first step with V above it */
+} cg_config;
+
+/* SimpleStimulus (heart/src/stimulus/SimpleStimulus.cpp:44-76) / RegularStimulus
+ * (heart/src/stimulus/RegularStimulus.cpp:43-81), magnitude in uA/cm^3. */
+typedef struct {
+    int kind;
+    double magnitude;
+    double duration;
+    double start;
+    double period;
+    double stop;
+} cg_stimulus;
+
+typedef struct {
+    long long steps;               /* PDE steps taken */
+    double time;                   /* current simulation time, ms */
+    int last_cg_iterations;
+    int max_cg_iterations;
+    long long total_cg_iterations;
+    int refinement_sweeps;         /* mixed precision: FP64 outer corrections, last step */
+    int operator_kind;             /* 0 CSR, 1 structured slab stencil */
+    int status_bits;
+    double ms_last_call;           /* device time of the last cg_step call */
+} cg_stats;
+
+/* Fill cfg with Chaste's defaults (LR91, FE, dt 0.01, Am 1400, Cm 1, Jacobi, atol 2e-4). */
+void cg_default_config(cg_config* cfg);
+
+/* Replaces MonodomainProblem construction + HeartConfig reads
+ * (heart/src/problem/MonodomainProblem.cpp:45-77). */
+int cg_create(const cg_config* cfg, cg_ctx** out);
+
+/* Mesh + conductivities; assembles A and M on the host once and uploads them
+ * (MonodomainSolver::SetupLinearSystem with computeMatrix, MonodomainSolver.cpp:51-76).
+ * conn: n_elems x (dim+1) node indices; sigma: n_elems x dim diagonal
+ * intracellular conductivities (AbstractCardiacTissue::CreateIntracellularConductivityTensor,
+ * heart/src/tissue/AbstractCardiacTissue.cpp:240-349, axis-aligned fibres). */
+int cg_set_mesh(cg_ctx* ctx, int n_nodes, int dim, const double* xyz, int n_elems,
+                const int* conn, const double* sigma);
+
+/* Regular slab mesh (AbstractTetrahedralMesh::ConstructRegularSlabMesh,
+ * mesh/src/common/AbstractTetrahedralMesh.cpp:569-614) with uniform diagonal
+ * sigma (dim values); lets the library use the matrix-free slab stencil. */
+int cg_set_slab_mesh(cg_ctx* ctx, int dim, double h, double width, double height,
+                     double depth, const double* sigma, int* n_nodes_out);
+
+/* Cells: what AbstractCardiacCellFactory::CreateCardiacCellForTissueNode decides per node
+ * (heart/src/problem/cell_factories/AbstractCardiacCellFactory.cpp:42-67).
+ * init_states: n_nodes x n_states node-major (AoS as Chaste cells hold them) or NULL
+ * for the model defaults; param_set: per-node index into param_table
+ * (n_param_sets x n_params scale factors, n_param_sets <= 255) or NULL for all-ones. */
+int cg_set_cells(cg_ctx* ctx, const double* init_states, const int* param_set,
+                 const double* param_table, int n_param_sets);
+
+/* Stimulus per node: stim_id[i] = -1 (ZeroStimulus) or an index into stims (< 255). */
+int cg_set_stimulus(cg_ctx* ctx, const int* stim_id, const cg_stimulus* stims, int n_stims);
+
+/* Advance n PDE steps (ODE -> RHS -> CG each), launched as a CUDA graph. */
+int cg_step(cg_ctx* ctx, int n_steps);
+
+int cg_get_voltage(cg_ctx* ctx, double* v);
+int cg_set_voltage(cg_ctx* ctx, const double* v);
+int cg_get_states(cg_ctx* ctx, double* states /* n_nodes x n_states, node-major */);
+int cg_get_cell_state(cg_ctx* ctx, int node, double* state /* n_states */);
+/* rGetIionicCacheReplicated / rGetIntracellularStimulusCacheReplicated
+ * (heart/src/tissue/AbstractCardiacTissue.hpp:457-460). */
+int cg_get_caches(cg_ctx* ctx, double* iionic, double* istim);
+int cg_get_activation_times(cg_ctx* ctx, double* t /* -1 where not activated */);
+int cg_get_stats(cg_ctx* ctx, cg_stats* stats);
+/* Iteration count of each of the last min(n, steps) solves, oldest first. */
+int cg_get_iteration_history(cg_ctx* ctx, int n, int* iterations);
+
+int cg_num_nodes(cg_ctx* ctx, int* n);
+int cg_num_states(int model, int* n);
+int cg_num_params(int model, int* n);
+
+/* Device-resident state snapshot: step, V, states, caches, activation times
+ * (stands in for CardiacSimulationArchiver, heart/src/problem/CardiacSimulationArchiver.cpp:55-110). */
+int cg_snapshot_size(cg_ctx* ctx, size_t* bytes);
+int cg_snapshot(cg_ctx* ctx, void* host_buffer, size_t bytes);
+int cg_restore(cg_ctx* ctx, const void* host_buffer, size_t bytes);
+
+int cg_destroy(cg_ctx* ctx);
+const char* cg_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHASTE_GPU_H */
