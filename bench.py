@@ -1,0 +1,347 @@
+"""Benchmark of the monodomain operator-split step on B200.
+
+Workload (default): the 3D ten Tusscher 2006 epicardial slab, 2 x 0.7 x 0.3 cm
+at h = 0.01 cm (201 x 71 x 31 = 442,371 nodes, 2.52M tetrahedra), Rush-Larsen
+dt_ode = 0.02 ms, PDE dt = 0.1 ms, sigma = (1.75, 0.19, 0.19) mS/cm, corner
+stimulus -5e5 uA/cm^3 for 1 ms in a 0.1 cm cube, CG + Jacobi at rtol 1e-8.
+A step is one PDE step of every node (ODE -> RHS -> CG).  Metric: node-steps/s.
+
+The mixed-precision path (FP32 states, FP32 inner CG, FP64 residual
+refinement) is the headline when its Vm stays within 0.5 mV of the FP64 path
+run over the same steps in the same process; both are reported.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # BASELINE config 2 (3D TT06 slab) -- the metric's configuration
+    "tt06_slab_3d": dict(model=1, method=1, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01,
+                         size=(2.0, 0.7, 0.3), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
+                         box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8,
+                         name="3D TT06-epi Rush-Larsen slab 2x0.7x0.3 cm h=0.01 (442,371 nodes)"),
+    # BASELINE config 5 (2.1M nodes), used for profiling at a size beyond L2
+    "tt06_slab_3d_large": dict(model=1, method=1, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.0125,
+                               size=(2.0, 2.0, 1.0), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
+                               box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8,
+                               name="3D TT06-epi Rush-Larsen slab 2x2x1 cm h=0.0125 (2,099,601 nodes)"),
+    # BASELINE config 1 (2D LR91 forward Euler)
+    "lr91_sheet_2d": dict(model=0, method=0, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, size=(1.0, 1.0, 0.0),
+                          sigma=(1.75, 1.75, 1.75), stim=(-5e5, 0.5, 0.0), box_hi=(0.0199, 1e9),
+                          rel_tol=1e-8, name="2D LR91 forward-Euler sheet 1x1 cm h=0.01 (10,201 nodes)"),
+}
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ode_bytes_per_node(model, w):
+    s = 19 if model == 1 else 8
+    # read+write S-1 states, read V (8) and the stimulus id (1), write Iion and z
+    return 2 * (s - 1) * w + 8 + 1 + 2 * w
+
+
+def cg_bytes(mixed, its, sweeps):
+    """Algorithmic bytes per node of one diffusion solve on the slab operator."""
+    if not mixed:
+        # phase 0: V, z, class in; r out.  per iteration: (r, p_old, cls) -> p_new ; (x, p_new, r, cls) -> (x, r)
+        return (8 + 8 + 1 + 8) + its * ((8 + 8 + 1 + 8) + (8 + 8 + 8 + 1 + 16))
+    per_sweep = (8 + 4 + 1 + 4 + 4) + (4 + 8 + 8)       # residual pass + x update
+    per_it = (4 + 4 + 1 + 4) + (4 + 4 + 4 + 1 + 8)      # FP32 inner phases A and B
+    return (8 + 4 + 1 + 4 + 4) + sweeps * per_sweep + its * per_it
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_tissue(N, wl, precision, device):
+    cfg = N.default_config()
+    cfg.model, cfg.ode_method = wl["model"], wl["method"]
+    cfg.ode_time_step, cfg.pde_time_step = wl["dt_ode"], wl["dt_pde"]
+    cfg.ksp_preconditioner = N.PC_JACOBI
+    cfg.use_absolute_tolerance, cfg.ksp_tolerance = 0, wl["rel_tol"]
+    cfg.precision = precision
+    cfg.device = device
+    t = N.Tissue(cfg)
+    t.set_slab_mesh(wl["dim"], wl["h"], *wl["size"], sigma=wl["sigma"])
+    t.set_cells()
+    from chaste_b200.heart import slab_coordinates
+
+    xyz = slab_coordinates(wl["dim"], wl["h"], *wl["size"])
+    inside = np.ones(t.n, bool)
+    for d, hi in enumerate(wl["box_hi"][: wl["dim"]]):
+        inside &= xyz[:, d] <= hi + 1e-12
+    t.set_stimulus(np.where(inside, 0, -1).astype(np.int32), [N.stimulus(N.STIM_SIMPLE, *wl["stim"])])
+    return t
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def run_ours(args, rank, world, device):
+    import torch
+
+    from chaste_b200 import _native as N
+    from chaste_b200.build import build_native
+
+    build_native()
+    torch.cuda.set_device(device)
+    wl = WORKLOADS[args.workload]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")  # 256 MB > L2
+    results = {}
+    for prec, label in ((0, "fp64"), (1, "mixed")):
+        t = build_tissue(N, wl, prec, device)
+        t.step(args.warmup)
+        ms_total, ms_ode, ms_cg, its = 0.0, 0.0, 0.0, 0
+        sweeps = 0
+        with ClockSampler(device) as clk:
+            for _ in range(args.steps):
+                flush_l2(flush)
+                torch.cuda.synchronize()
+                t.step(1)
+                st = t.stats()
+                ms_total += st.ms_last_call
+                its += st.last_cg_iterations
+                sweeps += st.refinement_sweeps
+        # per-phase device times on the same workload (kernel by kernel, no graph)
+        k_prof = min(args.steps, 20)
+        for _ in range(k_prof):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            a, b = t.step_profiled(1)
+            ms_ode += a
+            ms_cg += b
+        results[label] = dict(tissue=t, ms_total=ms_total, its=its, sweeps=sweeps, ms_ode=ms_ode / k_prof,
+                              ms_cg=ms_cg / k_prof, clocks=clk.summary(), steps_done=t.stats().steps)
+    n = results["fp64"]["tissue"].n
+    # accuracy of the mixed path against FP64 at the same simulated time
+    v64 = results["fp64"]["tissue"].voltage()
+    v32 = results["mixed"]["tissue"].voltage()
+    vm_err = float(np.abs(v64 - v32).max())
+    # end-to-end through the C-ABI with host buffers: V in, step, V out every step
+    head = "mixed" if vm_err <= 0.5 else "fp64"
+    te = results[head]["tissue"]
+    vh = te.voltage()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        te.set_voltage(vh)
+        te.step(1)
+        vh = te.voltage()
+    e2e_s = time.perf_counter() - t0
+    out = {}
+    for label, r in results.items():
+        sec = r["ms_total"] / 1e3
+        out[label] = dict(node_steps_per_s=n * args.steps / sec, ms_per_step=r["ms_total"] / args.steps,
+                          mean_cg_iterations=r["its"] / args.steps, ms_ode=r["ms_ode"], ms_cg=r["ms_cg"],
+                          sweeps=r["sweeps"] / args.steps, clocks=r["clocks"])
+    return dict(n=n, out=out, vm_err=vm_err, head=head, e2e_s=e2e_s, wl=wl)
+
+
+def roofline(res, args):
+    peak, kind = hbm_peak()
+    head = res["head"]
+    o = res["out"][head]
+    n = res["n"]
+    mixed = head == "mixed"
+    w = 4 if mixed else 8
+    b_ode = ode_bytes_per_node(res["wl"]["model"], w) * n
+    b_cg = cg_bytes(mixed, o["mean_cg_iterations"], o["sweeps"] if mixed else 0) * n
+    ach_ode = b_ode / (o["ms_ode"] / 1e3) / 1e9
+    ach_cg = b_cg / (o["ms_cg"] / 1e3) / 1e9
+    dom = "ode" if o["ms_ode"] >= o["ms_cg"] else "cg"
+    ach = ach_ode if dom == "ode" else ach_cg
+    return {"bound": "hbm", "kernel": "ode_kernel" if dom == "ode" else "cg_kernel", "achieved": round(ach, 1),
+            "peak": peak, "peak_kind": kind, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+            "per_kernel": {"ode_kernel": {"ms": round(o["ms_ode"], 4), "algorithmic_bytes": b_ode,
+                                          "achieved_gbs": round(ach_ode, 1)},
+                           "cg_kernel": {"ms": round(o["ms_cg"], 4), "algorithmic_bytes": int(b_cg),
+                                         "achieved_gbs": round(ach_cg, 1)}}}
+
+
+def cpu_baseline(wl, seconds=15.0, threads=None):
+    """The CPU oracle (a C++ restatement of Chaste's step) on the host cores, bounded sample."""
+    from oracle import pyoracle as O
+
+    threads = threads or os.cpu_count() or 1
+    O.lib().orc_set_threads(threads)
+    xyz, conn, _ = O.slab_mesh(wl["dim"], wl["h"], *wl["size"])
+    cfg = O.Config(wl["model"], wl["method"], wl["dt_ode"], wl["dt_pde"], 1400.0, 1.0, O.PC_JACOBI, 0,
+                   wl["rel_tol"], 0, 10000)
+    sig = np.tile(np.asarray(wl["sigma"][: wl["dim"]]), (conn.shape[0], 1))
+    inside = np.ones(xyz.shape[0], bool)
+    for d, hi in enumerate(wl["box_hi"][: wl["dim"]]):
+        inside &= xyz[:, d] <= hi + 1e-12
+    t = O.Tissue(cfg, wl["dim"], xyz, conn, sig, np.where(inside, 0, -1).astype(np.int32),
+                 [O.simple(*wl["stim"])])
+    t.step(1)
+    k, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds and k < 200:
+        t.step(1)
+        k += 1
+    dt = time.perf_counter() - t0
+    return {"value": xyz.shape[0] * k / dt, "unit": "node-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{k} PDE steps of the full {xyz.shape[0]}-node workload after 1 warm-up step, "
+                      f"{dt:.1f} s, FP64, {threads} threads"}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, world, local, pg
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tt06_slab_3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, world, local, dist = dist_setup(args)
+    wl = WORKLOADS[args.workload]
+    metric = "monodomain node-steps/s on 1 B200, mixed vs FP64 at <=0.5 mV Vm error"
+
+    if args.impl == "reference":
+        # Chaste's own CPU path (PETSc/MPI) cannot be built here; its restatement
+        # (the oracle port) is timed on every host core, rank 0 only.
+        if rank == 0:
+            cb = cpu_baseline(wl, seconds=max(5.0, args.cpu_seconds))
+            v = cb["value"]
+            line = {"impl": "reference", "metric": metric, "value": v, "unit": "node-steps/s",
+                    "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                    "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                    "config": {"workload": wl["name"]}, "cpu_baseline": cb,
+                    "e2e": {"value": v, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import torch
+
+    if dist:
+        dist.barrier()
+    res = run_ours(args, rank, world, local)
+    head = res["head"]
+    o = res["out"][head]
+    ms_step = o["ms_per_step"]
+    e2e_rate = res["n"] * args.steps / res["e2e_s"]
+    if dist:
+        tt = torch.tensor([ms_step, res["e2e_s"]], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms_step, e2e_s = tt.tolist()
+        e2e_rate = world * res["n"] * args.steps / e2e_s
+    value = world * res["n"] / (ms_step / 1e3)
+    if rank == 0:
+        line = {
+            "metric": metric, "value": value, "unit": "node-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 states+inner CG, f64 residual refinement" if head == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "dt_ode_ms": wl["dt_ode"], "dt_pde_ms": wl["dt_pde"],
+                       "solver": "CG+Jacobi rtol 1e-8 (PETSc convergence test)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "headline_precision": head},
+            "fp64": res["out"]["fp64"], "mixed": res["out"]["mixed"],
+            "mixed_vs_fp64": {"max_abs_vm_mv": res["vm_err"],
+                              "speedup": res["out"]["fp64"]["ms_per_step"] / res["out"]["mixed"]["ms_per_step"]},
+            "e2e": {"value": e2e_rate, "unit": "node-steps/s", "h2d_bytes_per_step": 8 * res["n"],
+                    "d2h_bytes_per_step": 8 * res["n"]},
+            "gpu_launches": 2 * args.steps,
+            "roofline": roofline(res, args),
+            "clocks": o["clocks"],
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(wl, seconds=args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

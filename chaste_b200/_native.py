@@ -1,0 +1,262 @@
+"""ctypes binding of libchastegpu.so (include/chaste_gpu.h).
+
+The library is the only compute path: there is no CPU fallback.  Importing
+works without a GPU (so the ABI can be inspected), but creating a tissue
+raises :class:`ChasteGpuError` when the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libchastegpu.so")
+
+CG_OK = 0
+STATUS_NAMES = {
+    0: "CG_OK", 1: "CG_ERR_ARG", 2: "CG_ERR_CUDA", 3: "CG_ERR_CG_MAXIT", 4: "CG_ERR_CG_DIVERGED",
+    5: "CG_ERR_NAN", 6: "CG_ERR_STATE_RANGE", 7: "CG_ERR_ORDER", 8: "CG_ERR_TIMEOUT",
+    9: "CG_ERR_NOMEM", 10: "CG_ERR_UNSUPPORTED",
+}
+MODEL_LR91, MODEL_TT06 = 0, 1
+ODE_FORWARD_EULER, ODE_RUSH_LARSEN = 0, 1
+PC_NONE, PC_JACOBI, PC_BJACOBI = 0, 1, 2
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+STIM_NONE, STIM_SIMPLE, STIM_REGULAR = 0, 1, 2
+
+
+class ChasteGpuError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = status
+        name = STATUS_NAMES.get(status, str(status))
+        msg = f"{where}: {name}"
+        try:
+            msg += f" ({lib().cg_status_string(status).decode()})"
+        except Exception:  # noqa: BLE001 - message decoration only
+            pass
+        super().__init__(msg)
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("model", C.c_int), ("ode_method", C.c_int), ("ode_time_step", C.c_double),
+        ("pde_time_step", C.c_double), ("surface_area_to_volume_ratio", C.c_double),
+        ("capacitance", C.c_double), ("ksp_preconditioner", C.c_int),
+        ("use_absolute_tolerance", C.c_int), ("ksp_tolerance", C.c_double),
+        ("use_mass_lumping", C.c_int), ("max_iterations", C.c_int), ("precision", C.c_int),
+        ("device", C.c_int), ("check_state_ranges", C.c_int), ("activation_threshold", C.c_double),
+    ]
+
+
+class Stimulus(C.Structure):
+    _fields_ = [("kind", C.c_int), ("magnitude", C.c_double), ("duration", C.c_double),
+                ("start", C.c_double), ("period", C.c_double), ("stop", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_longlong), ("time", C.c_double), ("last_cg_iterations", C.c_int),
+        ("max_cg_iterations", C.c_int), ("total_cg_iterations", C.c_longlong),
+        ("refinement_sweeps", C.c_int), ("operator_kind", C.c_int), ("status_bits", C.c_int),
+        ("ms_last_call", C.c_double),
+    ]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+# exported symbol -> (restype, argtypes); every name declared in include/chaste_gpu.h
+SIGNATURES = {
+    "cg_default_config": (None, [C.POINTER(Config)]),
+    "cg_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "cg_set_mesh": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_int, _ip, _dp]),
+    "cg_set_slab_mesh": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _ip]),
+    "cg_set_cells": (C.c_int, [_vp, _dp, _ip, _dp, C.c_int]),
+    "cg_set_stimulus": (C.c_int, [_vp, _ip, C.POINTER(Stimulus), C.c_int]),
+    "cg_step": (C.c_int, [_vp, C.c_int]),
+    "cg_step_profiled": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+    "cg_get_voltage": (C.c_int, [_vp, _dp]),
+    "cg_set_voltage": (C.c_int, [_vp, _dp]),
+    "cg_get_states": (C.c_int, [_vp, _dp]),
+    "cg_get_cell_state": (C.c_int, [_vp, C.c_int, _dp]),
+    "cg_get_caches": (C.c_int, [_vp, _dp, _dp]),
+    "cg_get_activation_times": (C.c_int, [_vp, _dp]),
+    "cg_get_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "cg_get_iteration_history": (C.c_int, [_vp, C.c_int, _ip]),
+    "cg_num_nodes": (C.c_int, [_vp, _ip]),
+    "cg_num_states": (C.c_int, [C.c_int, _ip]),
+    "cg_num_params": (C.c_int, [C.c_int, _ip]),
+    "cg_snapshot_size": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
+    "cg_snapshot": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "cg_restore": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "cg_destroy": (C.c_int, [_vp]),
+    "cg_status_string": (C.c_char_p, [C.c_int]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libchastegpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ChasteGpuError(2, f"{LIB_PATH} not built (run chaste_b200.build.build_native())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, where):
+    if status != CG_OK:
+        raise ChasteGpuError(status, where)
+
+
+def dptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def iptr(a):
+    return None if a is None else a.ctypes.data_as(_ip)
+
+
+def default_config() -> Config:
+    c = Config()
+    lib().cg_default_config(C.byref(c))
+    return c
+
+
+def num_states(model):
+    n = C.c_int()
+    check(lib().cg_num_states(model, C.byref(n)), "cg_num_states")
+    return n.value
+
+
+def num_params(model):
+    n = C.c_int()
+    check(lib().cg_num_params(model, C.byref(n)), "cg_num_params")
+    return n.value
+
+
+def stimulus(kind, magnitude=0.0, duration=0.0, start=0.0, period=0.0, stop=1.7976931348623157e308):
+    return Stimulus(kind, magnitude, duration, start, period, stop)
+
+
+class Tissue:
+    """One device-resident monodomain tissue (a cg_ctx)."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(lib().cg_create(C.byref(cfg), C.byref(h)), "cg_create")
+        self.h = h
+        self.n = 0
+        self.n_states = num_states(cfg.model)
+
+    # -- set-up
+    def set_mesh(self, xyz, conn, sigma):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        conn = np.ascontiguousarray(conn, dtype=np.int32)
+        dim = conn.shape[1] - 1
+        sigma = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma, dtype=np.float64),
+                                                     (conn.shape[0], dim)))
+        check(lib().cg_set_mesh(self.h, xyz.shape[0], dim, dptr(xyz), conn.shape[0], iptr(conn), dptr(sigma)),
+              "cg_set_mesh")
+        self.n = xyz.shape[0]
+
+    def set_slab_mesh(self, dim, h, width, height=0.0, depth=0.0, sigma=(1.75, 1.75, 1.75)):
+        sig = np.ascontiguousarray(np.asarray(sigma, dtype=np.float64)[:dim])
+        n = C.c_int()
+        check(lib().cg_set_slab_mesh(self.h, dim, h, width, height, depth, dptr(sig), C.byref(n)),
+              "cg_set_slab_mesh")
+        self.n = n.value
+
+    def set_cells(self, init_states=None, param_set=None, param_table=None):
+        ini = None if init_states is None else np.ascontiguousarray(init_states, dtype=np.float64)
+        ps = None if param_set is None else np.ascontiguousarray(param_set, dtype=np.int32)
+        pt = None if param_table is None else np.ascontiguousarray(param_table, dtype=np.float64)
+        check(lib().cg_set_cells(self.h, dptr(ini), iptr(ps), dptr(pt), 0 if pt is None else pt.shape[0]),
+              "cg_set_cells")
+
+    def set_stimulus(self, stim_id, stims):
+        sid = np.ascontiguousarray(stim_id, dtype=np.int32)
+        arr = (Stimulus * max(1, len(stims)))(*stims)
+        check(lib().cg_set_stimulus(self.h, iptr(sid), arr, len(stims)), "cg_set_stimulus")
+
+    # -- stepping
+    def step(self, n=1):
+        check(lib().cg_step(self.h, int(n)), "cg_step")
+
+    def step_profiled(self, n=1):
+        """Returns (ms in the ODE kernel, ms in the RHS+CG kernel) over n steps."""
+        a, b = C.c_double(), C.c_double()
+        check(lib().cg_step_profiled(self.h, int(n), C.byref(a), C.byref(b)), "cg_step_profiled")
+        return a.value, b.value
+
+    # -- views
+    def voltage(self):
+        v = np.empty(self.n)
+        check(lib().cg_get_voltage(self.h, dptr(v)), "cg_get_voltage")
+        return v
+
+    def set_voltage(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        check(lib().cg_set_voltage(self.h, dptr(v)), "cg_set_voltage")
+
+    def states(self):
+        s = np.empty((self.n, self.n_states))
+        check(lib().cg_get_states(self.h, dptr(s)), "cg_get_states")
+        return s
+
+    def cell_state(self, node):
+        s = np.empty(self.n_states)
+        check(lib().cg_get_cell_state(self.h, int(node), dptr(s)), "cg_get_cell_state")
+        return s
+
+    def caches(self):
+        a, b = np.empty(self.n), np.empty(self.n)
+        check(lib().cg_get_caches(self.h, dptr(a), dptr(b)), "cg_get_caches")
+        return a, b
+
+    def activation_times(self):
+        t = np.empty(self.n)
+        check(lib().cg_get_activation_times(self.h, dptr(t)), "cg_get_activation_times")
+        return t
+
+    def stats(self) -> Stats:
+        s = Stats()
+        check(lib().cg_get_stats(self.h, C.byref(s)), "cg_get_stats")
+        return s
+
+    def iteration_history(self, n):
+        it = np.zeros(n, dtype=np.int32)
+        check(lib().cg_get_iteration_history(self.h, n, iptr(it)), "cg_get_iteration_history")
+        return it
+
+    def snapshot(self) -> bytes:
+        sz = C.c_size_t()
+        check(lib().cg_snapshot_size(self.h, C.byref(sz)), "cg_snapshot_size")
+        buf = C.create_string_buffer(sz.value)
+        check(lib().cg_snapshot(self.h, buf, sz.value), "cg_snapshot")
+        return buf.raw
+
+    def restore(self, blob: bytes):
+        buf = C.create_string_buffer(blob, len(blob))
+        check(lib().cg_restore(self.h, buf, len(blob)), "cg_restore")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

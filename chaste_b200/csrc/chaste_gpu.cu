@@ -945,3 +945,55 @@ int cg_restore(cg_ctx* c, const void* buf, size_t bytes) {
 }
 
 }  // extern "C"
+
+extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double* ms_linear) {
+    if (!c || n_steps < 0) return CG_ERR_ARG;
+    if (!c->have_mesh || !c->have_cells) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    cudaEvent_t e[3];
+    for (auto& x : e)
+        if (cudaEventCreate(&x) != cudaSuccess) {
+            cudaGetLastError();
+            return CG_ERR_CUDA;
+        }
+    double t_ode = 0.0, t_cg = 0.0;
+    int rc = CG_OK;
+    const bool tt = c->cfg.model == CG_MODEL_TT06;
+    for (int k = 0; k < n_steps && rc == CG_OK; ++k) {
+        cudaEventRecord(e[0], c->stream);
+        if (c->mixed()) {
+            if (tt) launch_ode<TenTusscher2006Epi, float>(c);
+            else launch_ode<LuoRudy1991, float>(c);
+        } else {
+            if (tt) launch_ode<TenTusscher2006Epi, double>(c);
+            else launch_ode<LuoRudy1991, double>(c);
+        }
+        cudaEventRecord(e[1], c->stream);
+        if (cudaGetLastError() != cudaSuccess || launch_cg(c) != cudaSuccess) rc = CG_ERR_CUDA;
+        cudaEventRecord(e[2], c->stream);
+        if (cudaEventSynchronize(e[2]) != cudaSuccess) rc = CG_ERR_CUDA;
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, e[0], e[1]);
+        cudaEventElapsedTime(&b, e[1], e[2]);
+        t_ode += a;
+        t_cg += b;
+    }
+    for (auto& x : e) cudaEventDestroy(x);
+    cudaGetLastError();
+    if (ms_odes) *ms_odes = t_ode;
+    if (ms_linear) *ms_linear = t_cg;
+    if (rc != CG_OK) return rc;
+    int bits = 0;
+    long long dstep = 0;
+    CG_CUDA(cudaMemcpy(&bits, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    CG_CUDA(cudaMemcpy(&dstep, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost));
+    std::vector<int> ring(kRing);
+    CG_CUDA(cudaMemcpy(ring.data(), c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost));
+    for (long long s = std::max(c->steps, dstep - kRing); s < dstep; ++s) {
+        c->total_iters += ring[s % kRing];
+        c->max_iters = std::max(c->max_iters, ring[s % kRing]);
+    }
+    c->steps = dstep;
+    c->ms_last = t_ode + t_cg;
+    return status_from_bits(bits);
+}

@@ -1,0 +1,404 @@
+"""Host-side mirror of Chaste's monodomain API over the GPU tissue.
+
+Names and argument meanings follow the reference so a Chaste user finds the
+same calls:
+
+* :class:`HeartConfig` -- ``heart/src/problem/HeartConfig.hpp`` (the fields
+  this path reads; defaults of ``HeartConfigDefaults.hpp:53-91``);
+* :class:`SimpleStimulus`, :class:`RegularStimulus`, :class:`ZeroStimulus` --
+  ``heart/src/stimulus``;
+* :func:`CellLuoRudy1991FromCellML`, :func:`CellTenTusscher2006EpiFromCellML`
+  -- the chaste_codegen cell classes (here: which generated model a node runs);
+* :class:`AbstractCardiacCellFactory`, :class:`PlaneStimulusCellFactory` --
+  ``heart/src/problem/cell_factories``;
+* :class:`MonodomainProblem` -- ``heart/src/problem/MonodomainProblem.hpp`` with
+  ``Initialise``/``Solve``/``GetSolution``/``GetTissue``;
+* :class:`GpuMonodomainTissue` -- the tissue view (``rGetIionicCacheReplicated``,
+  ``GetCardiacCell(i)`` ...), served from device memory.
+
+Everything numeric runs in libchastegpu.so.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .codegen import PARAM_NAMES
+
+DBL_MAX = 1.7976931348623157e308
+
+
+# ----------------------------------------------------------------- config --
+class HeartConfig:
+    """Singleton holding the options of the monodomain path."""
+
+    _instance = None
+
+    @classmethod
+    def Instance(cls) -> "HeartConfig":
+        if cls._instance is None:
+            cls._instance = cls()
+        return cls._instance
+
+    def __init__(self):
+        self.Reset()
+
+    def Reset(self):
+        self.simulation_duration = 10.0
+        self.ode_dt = 0.01
+        self.pde_dt = 0.01
+        self.printing_dt = 0.01
+        self.am = 1400.0
+        self.cm = 1.0
+        self.sigma = (1.75, 1.75, 1.75)
+        self.use_abs_tol = True
+        self.tol = 2e-4
+        self.ksp_pc = "jacobi"
+        self.mass_lumping = False
+        self.space_dimension = 3
+        self.slab = None          # (width, height, depth, h)
+        self.precision = "fp64"
+        self.activation_threshold = -40.0
+        self.check_state_ranges = False
+        self.device = 0
+
+    # HeartConfig.cpp:1581-1587, 2337
+    def SetOdeTimeStep(self, dt):
+        self.ode_dt = dt
+
+    def SetPdeTimeStep(self, dt):
+        self.pde_dt = dt
+
+    def SetPrintingTimeStep(self, dt):
+        self.printing_dt = dt
+
+    def SetOdePdeAndPrintingTimeSteps(self, ode, pde, printing):
+        self.ode_dt, self.pde_dt, self.printing_dt = ode, pde, printing
+
+    def GetOdeTimeStep(self):
+        return self.ode_dt
+
+    def GetPdeTimeStep(self):
+        return self.pde_dt
+
+    def SetSimulationDuration(self, t):
+        self.simulation_duration = t
+
+    def GetSimulationDuration(self):
+        return self.simulation_duration
+
+    def SetSurfaceAreaToVolumeRatio(self, am):
+        self.am = am
+
+    def GetSurfaceAreaToVolumeRatio(self):
+        return self.am
+
+    def SetCapacitance(self, cm):
+        self.cm = cm
+
+    def GetCapacitance(self):
+        return self.cm
+
+    def SetIntracellularConductivities(self, sigma):
+        s = tuple(float(x) for x in np.atleast_1d(sigma))
+        self.sigma = s + (s[-1],) * (3 - len(s))
+
+    # HeartConfig.cpp:2404-2412
+    def SetUseAbsoluteTolerance(self, tol):
+        self.use_abs_tol, self.tol = True, tol
+
+    def SetUseRelativeTolerance(self, tol):
+        self.use_abs_tol, self.tol = False, tol
+
+    def GetUseAbsoluteTolerance(self):
+        return self.use_abs_tol
+
+    def SetKSPSolver(self, name):
+        if name != "cg":
+            raise ValueError("the GPU tissue solves with CG (the monodomain matrix is SPD)")
+
+    def SetKSPPreconditioner(self, name):
+        if name not in ("jacobi", "none"):
+            raise ValueError(f"unsupported preconditioner {name!r} (jacobi or none)")
+        self.ksp_pc = name
+
+    def SetUseMassLumping(self, flag=True):
+        self.mass_lumping = bool(flag)
+
+    def SetFibreLength(self, length, h):
+        self.space_dimension, self.slab = 1, (length, 0.0, 0.0, h)
+
+    def SetSheetDimensions(self, w, hgt, h):
+        self.space_dimension, self.slab = 2, (w, hgt, 0.0, h)
+
+    def SetSlabDimensions(self, w, hgt, d, h):
+        self.space_dimension, self.slab = 3, (w, hgt, d, h)
+
+    def SetSpaceDimension(self, d):
+        self.space_dimension = d
+
+    # extension of this library: FP32 states + FP32 inner CG with FP64 refinement
+    def SetPrecision(self, name):
+        if name not in ("fp64", "mixed"):
+            raise ValueError(name)
+        self.precision = name
+
+
+# -------------------------------------------------------------- stimulus --
+@dataclass
+class ZeroStimulus:
+    def as_native(self):
+        return None
+
+    def GetStimulus(self, t):
+        return 0.0
+
+
+@dataclass
+class SimpleStimulus:
+    magnitude: float
+    duration: float
+    start: float = 0.0
+
+    def as_native(self):
+        return N.stimulus(N.STIM_SIMPLE, self.magnitude, self.duration, self.start)
+
+
+@dataclass
+class RegularStimulus:
+    magnitude: float
+    duration: float
+    period: float
+    start: float
+    stop: float = DBL_MAX
+
+    def as_native(self):
+        return N.stimulus(N.STIM_REGULAR, self.magnitude, self.duration, self.start, self.period, self.stop)
+
+
+# ------------------------------------------------------------------ cells --
+@dataclass
+class CellSpec:
+    """What a chaste_codegen cell object fixes for a node: model, solver, stimulus, parameters."""
+
+    model: int
+    stimulus: object
+    solver: str = "ForwardEuler"
+    params: dict = field(default_factory=dict)
+
+    def SetParameter(self, name, value):
+        if name not in PARAM_NAMES[self.model]:
+            raise KeyError(f"no parameter {name!r}; have {PARAM_NAMES[self.model]}")
+        self.params[name] = float(value)
+
+
+def CellLuoRudy1991FromCellML(stimulus=None, solver="ForwardEuler"):
+    return CellSpec(N.MODEL_LR91, stimulus or ZeroStimulus(), solver)
+
+
+def CellTenTusscher2006EpiFromCellML(stimulus=None, solver="RushLarsen"):
+    return CellSpec(N.MODEL_TT06, stimulus or ZeroStimulus(), solver)
+
+
+class AbstractCardiacCellFactory:
+    """Per-node cell creation (AbstractCardiacCellFactory.cpp:42-67)."""
+
+    def CreateCardiacCellForTissueNode(self, index, x):
+        raise NotImplementedError
+
+
+class PlaneStimulusCellFactory(AbstractCardiacCellFactory):
+    """PlaneStimulusCellFactory.hpp:62-86: stimulate the nodes with x^2 <= 1e-10."""
+
+    def __init__(self, cell=CellLuoRudy1991FromCellML, magnitude=-600.0, duration=0.5, solver=None):
+        self.cell = cell
+        self.stim = SimpleStimulus(magnitude, duration)
+        self.solver = solver
+
+    def CreateCardiacCellForTissueNode(self, index, x):
+        stim = self.stim if x[0] * x[0] <= 1e-10 else ZeroStimulus()
+        return self.cell(stim) if self.solver is None else self.cell(stim, self.solver)
+
+
+class CuboidStimulusCellFactory(AbstractCardiacCellFactory):
+    """Stimulus on the nodes inside an axis-aligned box (corner-cube protocols)."""
+
+    def __init__(self, cell, magnitude, duration, lo, hi, solver=None):
+        self.cell, self.solver = cell, solver
+        self.stim = SimpleStimulus(magnitude, duration)
+        self.lo, self.hi = np.asarray(lo, float), np.asarray(hi, float)
+
+    def CreateCardiacCellForTissueNode(self, index, x):
+        d = len(self.lo)
+        inside = bool(np.all(x[:d] >= self.lo) and np.all(x[:d] <= self.hi))
+        stim = self.stim if inside else ZeroStimulus()
+        return self.cell(stim) if self.solver is None else self.cell(stim, self.solver)
+
+
+# ----------------------------------------------------------------- tissue --
+class GpuMonodomainTissue:
+    """Device-resident tissue: the AbstractCardiacTissue view of a N.Tissue."""
+
+    def __init__(self, native: N.Tissue, xyz):
+        self.native = native
+        self.xyz = xyz
+
+    def rGetIionicCacheReplicated(self):
+        return self.native.caches()[0]
+
+    def rGetIntracellularStimulusCacheReplicated(self):
+        return self.native.caches()[1]
+
+    def GetCardiacCell(self, index):
+        return _CellView(self.native, index)
+
+    def GetNumNodes(self):
+        return self.native.n
+
+
+class _CellView:
+    """AbstractCardiacCellInterface view of one node (lazy device->host reads)."""
+
+    def __init__(self, native, index):
+        self.native, self.index = native, index
+
+    def rGetStateVariables(self):
+        return self.native.cell_state(self.index)
+
+    def GetStdVecStateVariables(self):
+        return list(self.rGetStateVariables())
+
+    def GetVoltage(self):
+        return float(self.rGetStateVariables()[0])
+
+    def GetIIonic(self):
+        return float(self.native.caches()[0][self.index])
+
+
+def slab_coordinates(dim, h, width, height=0.0, depth=0.0):
+    """Node coordinates in ConstructRegularSlabMesh order ((k*NY + j)*NX + i)."""
+    nx = int((width + 0.5 * h) / h) + 1
+    ny = int((height + 0.5 * h) / h) + 1 if dim > 1 else 1
+    nz = int((depth + 0.5 * h) / h) + 1 if dim > 2 else 1
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    return np.stack([i.ravel() * h, j.ravel() * h, k.ravel() * h], axis=1)
+
+
+# ---------------------------------------------------------------- problem --
+class MonodomainProblem:
+    """MonodomainProblem<DIM> (heart/src/problem/MonodomainProblem.cpp:45-77)."""
+
+    def __init__(self, cell_factory: AbstractCardiacCellFactory, dim=None):
+        self.factory = cell_factory
+        self.dim = dim
+        self.mesh = None
+        self.tissue = None
+        self.native = None
+        self.output_modifiers = []
+        self._initialised = False
+
+    def SetMesh(self, xyz, conn):
+        self.mesh = (np.asarray(xyz, float), np.asarray(conn, np.int32))
+
+    def GetTissue(self):
+        if self.tissue is None:
+            raise RuntimeError("Tissue not yet set up, you may need to call Initialise() before GetTissue().")
+        return self.tissue
+
+    def _config(self):
+        hc = HeartConfig.Instance()
+        cfg = N.default_config()
+        cfg.ode_time_step = hc.ode_dt
+        cfg.pde_time_step = hc.pde_dt
+        cfg.surface_area_to_volume_ratio = hc.am
+        cfg.capacitance = hc.cm
+        cfg.use_absolute_tolerance = 1 if hc.use_abs_tol else 0
+        cfg.ksp_tolerance = hc.tol
+        cfg.ksp_preconditioner = {"jacobi": N.PC_JACOBI, "none": N.PC_NONE}[hc.ksp_pc]
+        cfg.use_mass_lumping = 1 if hc.mass_lumping else 0
+        cfg.precision = N.PRECISION_MIXED if hc.precision == "mixed" else N.PRECISION_FP64
+        cfg.activation_threshold = hc.activation_threshold
+        cfg.check_state_ranges = 1 if hc.check_state_ranges else 0
+        cfg.device = hc.device
+        return cfg
+
+    def Initialise(self):
+        """Fix the mesh; the tissue itself is built by the first Solve, after HeartConfig
+        changes made between Initialise and Solve (as Chaste's tests make them)."""
+        hc = HeartConfig.Instance()
+        if self.mesh is None and hc.slab is None:
+            raise RuntimeError("no mesh: call SetMesh or HeartConfig.Set{Fibre,Sheet,Slab}Dimensions")
+        self._initialised = True
+
+    def _build(self):
+        hc = HeartConfig.Instance()
+        cfg = self._config()
+        if self.mesh is None:
+            w, hh, d, h = hc.slab
+            dim = self.dim or hc.space_dimension
+            xyz = slab_coordinates(dim, h, w, hh, d)
+        else:
+            xyz, conn = self.mesh
+            dim = conn.shape[1] - 1
+        specs = [self.factory.CreateCardiacCellForTissueNode(i, xyz[i]) for i in range(xyz.shape[0])]
+        models = {s.model for s in specs}
+        solvers = {s.solver for s in specs}
+        if len(models) != 1 or len(solvers) != 1:
+            raise ValueError("a GPU tissue runs one cell model with one ODE solver")
+        cfg.model = models.pop()
+        cfg.ode_method = N.ODE_RUSH_LARSEN if solvers.pop() == "RushLarsen" else N.ODE_FORWARD_EULER
+        native = N.Tissue(cfg)
+        if self.mesh is None:
+            native.set_slab_mesh(dim, hc.slab[3], hc.slab[0], hc.slab[1], hc.slab[2], hc.sigma)
+        else:
+            native.set_mesh(xyz, self.mesh[1], np.asarray(hc.sigma[:dim]))
+        names = PARAM_NAMES[cfg.model]
+        sets, pset = {}, np.zeros(native.n, np.int32)
+        for i, s in enumerate(specs):
+            pset[i] = sets.setdefault(tuple(sorted(s.params.items())), len(sets))
+        if len(sets) == 1 and not specs[0].params:
+            native.set_cells()
+        else:
+            table = np.ones((len(sets), len(names)))
+            for key, k in sets.items():
+                for name, val in key:
+                    table[k, names.index(name)] = val
+            native.set_cells(param_set=pset, param_table=table)
+        stims, sid, index = [], np.full(native.n, -1, np.int32), {}
+        for i, s in enumerate(specs):
+            nat = s.stimulus.as_native()
+            if nat is None:
+                continue
+            key = (nat.kind, nat.magnitude, nat.duration, nat.start, nat.period, nat.stop)
+            if key not in index:
+                index[key] = len(stims)
+                stims.append(nat)
+            sid[i] = index[key]
+        native.set_stimulus(sid, stims)
+        self.native = native
+        self.tissue = GpuMonodomainTissue(native, xyz)
+
+    def Solve(self):
+        """Advance to the simulation duration (AbstractCardiacProblem::Solve, printing-step loop)."""
+        if not self._initialised:
+            raise RuntimeError("call Initialise() before Solve()")
+        hc = HeartConfig.Instance()
+        if self.native is None:
+            self._build()
+        n_total = int(round(hc.simulation_duration / hc.pde_dt))
+        per_print = max(1, int(round(hc.printing_dt / hc.pde_dt)))
+        done = self.native.stats().steps
+        while done < n_total:
+            k = min(per_print, n_total - done)
+            self.native.step(k)
+            done += k
+            for m in self.output_modifiers:
+                m(done * hc.pde_dt, self.native)
+
+    def GetSolution(self):
+        return self.native.voltage()
+
+    def AddOutputModifier(self, fn):
+        self.output_modifiers.append(fn)

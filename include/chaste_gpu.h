@@ -129,6 +129,12 @@ int cg_set_stimulus(cg_ctx* ctx, const int* stim_id, const cg_stimulus* stims, i
 /* Advance n PDE steps (ODE -> RHS -> CG each), launched as a CUDA graph. */
 int cg_step(cg_ctx* ctx, int n_steps);
 
+/* cg_step with device-side event timing per phase, launched kernel by kernel
+ * (no graph): ms_solve_odes accumulates the ODE kernel (HeartEventHandler
+ * SOLVE_ODES), ms_linear_solve the fused RHS + CG kernel (ASSEMBLE_RHS +
+ * SOLVE_LINEAR_SYSTEM); global/src/timing/HeartEventHandler.hpp:55-71. */
+int cg_step_profiled(cg_ctx* ctx, int n_steps, double* ms_solve_odes, double* ms_linear_solve);
+
 int cg_get_voltage(cg_ctx* ctx, double* v);
 int cg_set_voltage(cg_ctx* ctx, const double* v);
 int cg_get_states(cg_ctx* ctx, double* states /* n_nodes x n_states, node-major */);

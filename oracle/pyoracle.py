@@ -12,7 +12,27 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
+
+
+def _host_tag():
+    """The oracle is compiled with -march=native, so each host CPU gets its own build."""
+    import hashlib
+    import platform
+
+    info = platform.machine()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    info += line
+                if line.startswith("flags"):
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:10]
+
+
+LIB_PATH = os.path.join(HERE, "build", f"liboracle-{_host_tag()}.so")
 
 LR91, TT06 = 0, 1
 FE, RL = 0, 1
@@ -41,7 +61,7 @@ class Config(C.Structure):
 
 
 def build():
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"OUT={LIB_PATH}"], check=True)
 
 
 _lib = None
@@ -50,8 +70,7 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
+        build()
         L = C.CDLL(LIB_PATH)
         dp = C.POINTER(C.c_double)
         ip = C.POINTER(C.c_int)

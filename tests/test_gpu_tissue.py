@@ -1,0 +1,178 @@
+"""GPU tissue through the C-ABI against the oracle and Chaste's tissue KATs."""
+import numpy as np
+import pytest
+
+from tests import tissue_cases as TC
+
+pytestmark = pytest.mark.gpu
+
+FP64_RTOL = 1e-6   # per-node Vm parity target in FP64 (relative to max(|V|, 1 mV))
+
+
+@pytest.fixture(scope="module")
+def N(native):
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return native
+
+
+def _cmp(v_gpu, v_orc):
+    return np.max(np.abs(v_gpu - v_orc) / np.maximum(np.abs(v_orc), 1.0))
+
+
+@pytest.mark.parametrize("use_csr", [False, True], ids=["slab_stencil", "csr"])
+def test_chaste_tissue_kats_on_gpu(N, oracle, kats, use_csr):
+    """TestMonodomainProblem.hpp KATs through the GPU path (Jacobi PC), and per-node parity with the oracle."""
+    for case in kats["tissue"]:
+        d = case["dim"]
+        kw = dict(model=TC.LR91, method=TC.FE, dt_ode=0.01, dt_pde=0.01, dim=d, h=case["h"],
+                  size=tuple(case["size"][:3]), sigma=(case["sigma"],) * 3,
+                  stim=(case["stim"], case["stim_duration"], 0.0), box_hi=(1e-5,) + (1e9,) * 2,
+                  am=case["am"], cm=case["cm"])
+        if "abs_tol" in case:
+            kw["abs_tol"] = case["abs_tol"]
+        else:
+            kw["rel_tol"] = case["rel_tol"]
+        g, _ = TC.make_gpu(N, use_csr=use_csr, **kw)
+        o, _ = TC.make_oracle(oracle, **kw)
+        nsteps = int(round(case["end"] / 0.01))
+        g.step(nsteps)
+        its_o = o.step(nsteps)
+        v = g.voltage()
+        assert np.abs(v[case["nodes"]] - np.array(case["V"])).max() <= case["tolerance"], case["name"]
+        assert _cmp(v, o.voltage()) <= FP64_RTOL, case["name"]
+        its_g = g.iteration_history(nsteps)
+        assert np.abs(its_g - its_o).max() <= 1, case["name"]
+        assert g.stats().operator_kind == (0 if use_csr else 1)
+
+
+def _parity_run(N, oracle, case, t_end, every, precision=0):
+    g, xyz = TC.make_gpu(N, precision=precision, **case)
+    o, _ = TC.make_oracle(oracle, **case)
+    steps = int(round(t_end / case["dt_pde"]))
+    per = int(round(every / case["dt_pde"]))
+    worst, vmax_err, its_g, its_o = 0.0, 0.0, [], []
+    for _ in range(steps // per):
+        g.step(per)
+        its_o.extend(o.step(per))
+        its_g.extend(g.iteration_history(per))
+        vg, vo = g.voltage(), o.voltage()
+        worst = max(worst, _cmp(vg, vo))
+        vmax_err = max(vmax_err, np.abs(vg - vo).max())
+    return g, o, worst, vmax_err, np.array(its_g), np.array(its_o)
+
+
+def test_lr91_2d_forward_euler_parity(N, oracle):
+    """Reduced 2D LR91 FE (dt_ode 0.01, dt_pde 0.1, rtol 1e-8): Vm every 1 ms vs the oracle."""
+    g, o, worst, vmax, its_g, its_o = _parity_run(N, oracle, TC.LR91_2D, 20.0, 1.0)
+    assert worst <= FP64_RTOL, worst
+    assert np.abs(its_g - its_o).max() <= 1
+    s_g, s_o = g.states(), o.states()
+    assert np.max(np.abs(s_g - s_o) / np.maximum(np.abs(s_o), 1e-3)) <= 1e-5
+    ig, _ = g.caches()
+    io, _ = o.caches()
+    assert np.max(np.abs(ig - io)) <= 1e-6 * max(1.0, np.abs(io).max())
+
+
+def test_tt06_3d_rush_larsen_parity(N, oracle):
+    """Reduced 3D TT06 RL slab (anisotropic sigma, corner stimulus): Vm every 1 ms vs the oracle."""
+    g, o, worst, vmax, its_g, its_o = _parity_run(N, oracle, TC.TT06_3D, 10.0, 1.0)
+    assert worst <= FP64_RTOL, worst
+    assert np.abs(its_g - its_o).max() <= 1
+
+
+def test_mixed_precision_against_fp64(N):
+    """Mixed mode (FP32 states, FP32 inner CG, FP64 refinement) within 0.5 mV of FP64 and activation within 1 ms."""
+    case = dict(TC.TT06_3D)
+    a, _ = TC.make_gpu(N, precision=0, **case)
+    b, _ = TC.make_gpu(N, precision=1, **case)
+    worst = 0.0
+    for _ in range(20):
+        a.step(10)
+        b.step(10)
+        worst = max(worst, np.abs(a.voltage() - b.voltage()).max())
+    assert worst <= 0.5, worst
+    ta, tb = a.activation_times(), b.activation_times()
+    assert np.all((ta >= 0) == (tb >= 0))
+    act = ta >= 0
+    assert act.sum() > 0
+    assert np.abs(ta[act] - tb[act]).max() <= 1.0
+
+
+def test_snapshot_restore_is_bitwise(N):
+    case = dict(TC.LR91_2D)
+    a, _ = TC.make_gpu(N, **case)
+    a.step(20)
+    blob = a.snapshot()
+    a.step(30)
+    v1 = a.voltage()
+    b, _ = TC.make_gpu(N, **case)
+    b.restore(blob)
+    b.step(30)
+    assert np.array_equal(v1, b.voltage())
+    assert b.stats().steps == 50
+
+
+def test_two_node_caches_match_standalone_cells(N, oracle):
+    """TestMonodomainTissue.hpp:133-237: the Iion cache equals a standalone ComputeExceptVoltage."""
+    O = oracle
+    cfg = N.default_config()
+    cfg.pde_time_step = 0.5
+    t = N.Tissue(cfg)
+    xyz = np.array([[0.0, 0, 0], [1.0, 0, 0]])
+    t.set_mesh(xyz, np.array([[0, 1]]), np.array([[1.75]]))
+    t.set_cells()
+    t.set_stimulus(np.array([0, -1]), [N.stimulus(N.STIM_SIMPLE, -600.0 * 1400.0, 0.5, 0.0)])
+    t.step(1)
+    iion, _ = t.caches()
+    for node, st in ((0, O.simple(-600.0 * 1400.0, 0.5, 0.0)), (1, None)):
+        y = O.initial_states(O.LR91)
+        ref = O.cell_except_voltage(O.LR91, O.FE, y, 0.0, 0.5, 0.01, st, am=1400.0)
+        assert abs(iion[node] - ref) <= 1e-10 * max(1.0, abs(ref))
+
+
+def test_cg_failure_is_reported_not_faulted(N):
+    """KSP_DIVERGED_ITS analogue: a 1-iteration cap returns CG_ERR_CG_MAXIT and stops later steps."""
+    case = dict(TC.LR91_2D)
+    case["rel_tol"] = 1e-14
+    g, _ = TC.make_gpu(N, max_iterations=1, **case)
+    with pytest.raises(N.ChasteGpuError) as e:
+        g.step(2)
+    assert e.value.status == 3
+    assert g.stats().steps == 1
+
+
+def test_nan_voltage_is_reported(N):
+    case = dict(TC.LR91_2D)
+    g, _ = TC.make_gpu(N, **case)
+    v = g.voltage()
+    v[5] = np.nan
+    g.set_voltage(v)
+    with pytest.raises(N.ChasteGpuError) as e:
+        g.step(1)
+    assert e.value.status == 5
+
+
+def test_monodomain_problem_api_on_gpu(N, kats):
+    """MonodomainProblem + PlaneStimulusCellFactory (the Chaste-facing API) reproduces TestMonodomainProblem1D."""
+    from chaste_b200 import heart as H
+
+    case = [c for c in kats["tissue"] if c["name"] == "TestMonodomainProblem1DWithRelativeTolerance"][0]
+    hc = H.HeartConfig.Instance()
+    hc.Reset()
+    hc.SetIntracellularConductivities(0.0005)
+    hc.SetSimulationDuration(2.0)
+    hc.SetSurfaceAreaToVolumeRatio(1.0)
+    hc.SetCapacitance(1.0)
+    hc.SetUseRelativeTolerance(1e-9)
+    hc.SetFibreLength(0.1, 0.01)
+    p = H.MonodomainProblem(H.PlaneStimulusCellFactory(H.CellLuoRudy1991FromCellML, -600.0, 0.5))
+    p.Initialise()
+    p.Solve()
+    v = p.GetSolution()
+    assert np.abs(v[case["nodes"]] - np.array(case["V"])).max() <= case["tolerance"]
+    cell = p.GetTissue().GetCardiacCell(3)
+    assert abs(cell.GetVoltage() - v[3]) == 0.0
+    hc.Reset()

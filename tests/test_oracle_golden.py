@@ -1,0 +1,108 @@
+"""The CPU oracle against Chaste's own golden vectors (heart/test ValidData files
+and hard-coded values), extracted into tests/golden/chaste_kats.json."""
+import numpy as np
+import pytest
+
+
+def _stim(O, d):
+    if d["kind"] == "simple":
+        return O.simple(d["magnitude"], d["duration"], d["start"])
+    return O.regular(d["magnitude"], d["duration"], d["period"], d["start"])
+
+
+def _print_precision(g):
+    """Half a unit of the 5th significant digit of each printed value."""
+    g = np.abs(np.asarray(g, float))
+    mag = np.floor(np.log10(np.where(g > 0, g, 1.0)))
+    return 0.5 * 10.0 ** (mag - 4) * (1 + 1e-6) + 1e-300
+
+
+def test_lr91_delayed_stimulus_trace(oracle, kats):
+    """TestIonicModels.hpp:406-467 (CheckCellModelResults, 1e-3 mV)."""
+    O, k = oracle, kats["lr91_delayed_stim"]
+    y = O.initial_states(O.LR91)
+    tr, y = O.cell_compute(O.LR91, O.FE, y, 0.0, k["end"], k["dt"], 0.0, _stim(O, k["stimulus"]))
+    v = tr[:: k["sample_every_steps"], 0]
+    assert len(v) == len(k["V"])
+    assert np.abs(v - np.array(k["V"])).max() <= k["tolerance"]
+    # GetIIonic after a further Compute(0, 60) on the same cell: 1.9411 +- 1e-3
+    O.cell_compute(O.LR91, O.FE, y, 0.0, 60.0, k["dt"], 0.0, _stim(O, k["stimulus"]))
+    assert abs(O.cell_iionic(O.LR91, y) - k["iionic_after_1000_plus_60ms"]) <= k["iionic_tolerance"]
+
+
+def test_lr91_regular_stimulus_all_states(oracle, kats):
+    """TestIonicModels.hpp:469-500; every column of Lr91RegularStimValidData.dat to print precision."""
+    O, k = oracle, kats["lr91_regular_stim"]
+    y = O.initial_states(O.LR91)
+    tr, _ = O.cell_compute(O.LR91, O.FE, y, 0.0, k["end"], k["dt"], 0.0, _stim(O, k["stimulus"]))
+    tr = tr[:: k["sample_every_steps"]]
+    cols = {"V": 0, "m": 1, "h": 2, "j": 3, "d": 4, "f": 5, "x": 6, "CaI": 7}
+    for name, idx in cols.items():
+        g = np.array(k["states"][name])
+        tol = _print_precision(g)
+        if name == "V":
+            tol = np.maximum(tol, k["tolerance"])
+        assert np.all(np.abs(tr[:, idx] - g) <= tol), name
+
+
+def test_tt06_forward_euler_trace(oracle, kats):
+    """TestIonicModels.hpp:793-835: TT06 FE dt 0.001 vs TenTusscherValidData.dat, GetIIonic."""
+    O, k = oracle, kats["tt06_simple_stim"]
+    y = O.initial_states(O.TT06)
+    assert abs(O.cell_iionic(O.TT06, y) - k["iionic_initial"]) <= k["iionic_tolerance"]
+    tr, y = O.cell_compute(O.TT06, O.FE, y, 0.0, k["end"], k["dt"], 0.0, _stim(O, k["stimulus"]))
+    v = tr[:: k["sample_every_steps"], 0]
+    assert np.abs(v - np.array(k["states"]["V"])).max() <= k["tolerance"]
+    assert abs(O.cell_iionic(O.TT06, y) - k["iionic_at_end"]) <= k["iionic_tolerance"]
+
+
+def test_rush_larsen_lr91_against_forward_euler(oracle):
+    """TestRushLarsen.hpp:107-202: clamped agreement and first-order convergence."""
+    O = oracle
+    y_rl = O.initial_states(O.LR91)
+    y_fe = O.initial_states(O.LR91)
+    O.cell_except_voltage(O.LR91, O.RL, y_rl, 0.0, 1.0, 0.01)
+    O.cell_except_voltage(O.LR91, O.FE, y_fe, 0.0, 1.0, 0.01)
+    assert np.abs(y_rl - y_fe).max() <= 1e-6
+    stim = O.simple(-25.5, 1.99, 0.0)
+    a, _ = O.cell_compute(O.LR91, O.RL, O.initial_states(O.LR91), 0.0, 1.0, 0.01, 0.01, stim)
+    b, _ = O.cell_compute(O.LR91, O.FE, O.initial_states(O.LR91), 0.0, 1.0, 0.01, 0.01, stim)
+    assert len(a) == 101
+    assert np.abs(a[-1] - b[-1]).max() <= 1e-2
+    s1, _ = O.cell_compute(O.LR91, O.RL, O.initial_states(O.LR91), 0.0, 1.0, 0.01, 0.0, stim)
+    s2, _ = O.cell_compute(O.LR91, O.RL, O.initial_states(O.LR91), 0.0, 1.0, 0.005, 0.0, stim)
+    ref, _ = O.cell_compute(O.LR91, O.FE, O.initial_states(O.LR91), 0.0, 1.0, 1e-6, 1e-2, stim)
+    ratio = (s1[-1] - ref[-1]) / (s2[-1] - ref[-1])
+    assert np.all(np.abs(ratio - 2.0) <= 0.1), ratio
+
+
+def run_tissue_kat(O, case, pc):
+    d = case["dim"]
+    xyz, conn, _ = O.slab_mesh(d, case["h"], *case["size"][:3])
+    abs_tol = "abs_tol" in case
+    cfg = O.Config(O.LR91, O.FE, 0.01, 0.01, case["am"], case["cm"], pc, 1 if abs_tol else 0,
+                   case["abs_tol"] if abs_tol else case["rel_tol"], 0, 10000)
+    sid = np.where(xyz[:, 0] ** 2 <= 1e-10, 0, -1).astype(np.int32)
+    t = O.Tissue(cfg, d, xyz, conn, np.full((conn.shape[0], d), case["sigma"]), sid,
+                 [O.simple(case["stim"], case["stim_duration"], 0.0)])
+    out = {}
+    if "midway" in case:
+        t.step(int(round(case["midway"]["end"] / 0.01)))
+        out["midway"] = t.voltage()
+        t.step(int(round((case["end"] - case["midway"]["end"]) / 0.01)))
+    else:
+        t.step(int(round(case["end"] / 0.01)))
+    out["end"] = t.voltage()
+    return out
+
+
+@pytest.mark.parametrize("pc", [2, 1], ids=["bjacobi_ilu0", "jacobi"])
+def test_monodomain_problem_kats(oracle, kats, pc):
+    """TestMonodomainProblem.hpp KATs (1D/2D/3D slabs, absolute and relative KSP tolerance)."""
+    for case in kats["tissue"]:
+        out = run_tissue_kat(oracle, case, pc)
+        if "midway" in case:
+            mid = case["midway"]
+            assert np.abs(out["midway"][mid["nodes"]] - mid["V"]).max() <= mid["tolerance"], case["name"]
+        err = np.abs(out["end"][case["nodes"]] - np.array(case["V"])).max()
+        assert err <= case["tolerance"], (case["name"], err)

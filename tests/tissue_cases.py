@@ -1,0 +1,63 @@
+"""Paired oracle / GPU tissue set-ups shared by the parity tests and the benchmark."""
+from __future__ import annotations
+
+import numpy as np
+
+LR91, TT06 = 0, 1
+FE, RL = 0, 1
+
+
+def slab_stim_ids(xyz, box_hi):
+    """Nodes with every coordinate <= box_hi[d] (corner box from the origin)."""
+    inside = np.ones(xyz.shape[0], bool)
+    for d, hi in enumerate(box_hi):
+        inside &= xyz[:, d] <= hi + 1e-12
+    return np.where(inside, 0, -1).astype(np.int32)
+
+
+def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
+             abs_tol=None, rel_tol=1e-8, precision=0, use_csr=False, param_set=None, param_table=None,
+             init_states=None, max_iterations=10000):
+    """A GPU tissue on a regular slab (stencil operator, or CSR through cg_set_mesh when use_csr)."""
+    from oracle import pyoracle as O  # mesh generator only: the same node/element order as the library
+
+    cfg = N.default_config()
+    cfg.model, cfg.ode_method = model, method
+    cfg.ode_time_step, cfg.pde_time_step = dt_ode, dt_pde
+    cfg.surface_area_to_volume_ratio, cfg.capacitance = am, cm
+    cfg.ksp_preconditioner = N.PC_JACOBI
+    if abs_tol is not None:
+        cfg.use_absolute_tolerance, cfg.ksp_tolerance = 1, abs_tol
+    else:
+        cfg.use_absolute_tolerance, cfg.ksp_tolerance = 0, rel_tol
+    cfg.precision = precision
+    cfg.max_iterations = max_iterations
+    t = N.Tissue(cfg)
+    xyz, conn, _ = O.slab_mesh(dim, h, *size)
+    if use_csr:
+        t.set_mesh(xyz, conn, np.asarray(sigma[:dim]))
+    else:
+        t.set_slab_mesh(dim, h, *size, sigma=sigma)
+    t.set_cells(init_states=init_states, param_set=param_set, param_table=param_table)
+    sid = slab_stim_ids(xyz, box_hi)
+    t.set_stimulus(sid, [N.stimulus(N.STIM_SIMPLE, *stim)])
+    return t, xyz
+
+
+def make_oracle(O, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
+                abs_tol=None, rel_tol=1e-8, param_set=None, param_table=None, init_states=None, **_):
+    xyz, conn, _ = O.slab_mesh(dim, h, *size)
+    use_abs = abs_tol is not None
+    cfg = O.Config(model, method, dt_ode, dt_pde, am, cm, O.PC_JACOBI, 1 if use_abs else 0,
+                   abs_tol if use_abs else rel_tol, 0, 10000)
+    sig = np.tile(np.asarray(sigma[:dim], float), (conn.shape[0], 1))
+    sid = slab_stim_ids(xyz, box_hi)
+    return O.Tissue(cfg, dim, xyz, conn, sig, sid, [O.simple(*stim)], param_id=param_set,
+                    param_table=param_table, init_states=init_states), xyz
+
+
+# Reduced versions of the benchmark configurations (same physics, smaller slabs)
+LR91_2D = dict(model=LR91, method=FE, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, size=(0.2, 0.2, 0.0),
+               sigma=(1.75, 1.75, 1.75), stim=(-5e5, 0.5, 0.0), box_hi=(0.0199, 1e9))
+TT06_3D = dict(model=TT06, method=RL, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01, size=(0.2, 0.07, 0.03),
+               sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0), box_hi=(0.03, 0.03, 0.03))
