@@ -238,6 +238,9 @@ int slab_class(const SlabGrid& g, int i, int j, int k) {
     return cx + 3 * cy + 9 * cz;
 }
 
+// Largest relative difference accepted between a row and its class row.
+constexpr double kSlabRowTolerance = 1e-12;
+
 bool build_slab_stencil(const SlabGrid& g, const HostCsr& csr, SlabStencil& st) {
     const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
     st.n_classes = g.dim == 1 ? 3 : (g.dim == 2 ? 18 : 27);
@@ -280,8 +283,20 @@ bool build_slab_stencil(const SlabGrid& g, const HostCsr& csr, SlabStencil& st) 
                         m[(size_t)c * no + o] = rm[o];
                     }
                 } else {
-                    if (std::memcmp(ra, &a[(size_t)c * no], sizeof(double) * no) != 0) return false;
-                    if (std::memcmp(rm, &m[(size_t)c * no], sizeof(double) * no) != 0) return false;
+                    // node coordinates are i*h, so element edges (i+1)*h - i*h differ from
+                    // h in the last bit: rows of one class agree to rounding, not bitwise
+                    const double* ca = &a[(size_t)c * no];
+                    const double* cm = &m[(size_t)c * no];
+                    double sa = 0.0, sm = 0.0;
+                    for (int o = 0; o < no; ++o) {
+                        sa = std::max(sa, std::fabs(ca[o]));
+                        sm = std::max(sm, std::fabs(cm[o]));
+                    }
+                    for (int o = 0; o < no; ++o) {
+                        if ((ra[o] == 0.0) != (ca[o] == 0.0) || (rm[o] == 0.0) != (cm[o] == 0.0)) return false;
+                        if (std::fabs(ra[o] - ca[o]) > kSlabRowTolerance * sa) return false;
+                        if (std::fabs(rm[o] - cm[o]) > kSlabRowTolerance * sm) return false;
+                    }
                 }
                 for (int o = 0; o < no; ++o)
                     if (ra[o] != 0.0 || rm[o] != 0.0) used[o] = 1;

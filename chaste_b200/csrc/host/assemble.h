@@ -41,7 +41,7 @@ bool slab_grid(int dim, double h, double w, double hh, double dd, SlabGrid& g);
 void slab_mesh(const SlabGrid& g, std::vector<double>& xyz, std::vector<int>& conn);
 
 // Matrix-free slab stencil: every row of A (and M) equals the row of its
-// boundary class; the table holds the coefficients per (class, offset).
+// boundary class up to rounding; the table holds the coefficients per (class, offset).
 struct SlabStencil {
     int n_offsets = 0;
     int offsets[27];            // linear index offsets, ascending
@@ -50,7 +50,8 @@ struct SlabStencil {
     std::vector<double> a, m;   // [class][offset]
 };
 int slab_class(const SlabGrid& g, int i, int j, int k);
-// Builds the table from the assembled CSR and verifies every row bitwise.
+// Builds the table from the assembled CSR (the first row of each class) and checks
+// that every row agrees with its class row to 1e-12 relative.
 bool build_slab_stencil(const SlabGrid& g, const HostCsr& csr, SlabStencil& st);
 
 }  // namespace chb
