@@ -334,6 +334,7 @@ class ModelEmitter:
         for k, e in self.live.items():
             if m.time in _free(e) and k != self.stim_sym:
                 raise ValueError(f"{k} depends on time beyond the stimulus")
+        self._fix_singularities()
         self._rl_analysis()
 
     # --------------------------------------------------------------------
@@ -364,6 +365,99 @@ class ModelEmitter:
 
         return sub(e)
 
+    # ------------------------------------------------------------------
+    # Removable singularities (GHK-type terms such as (V-V0)/(exp(c(V-V0))-1)).
+    # chaste_codegen replaces such an expression f(V), within a small window of
+    # the exponent argument U = c(V-V0) around 0, by the straight line through
+    # f(V0-eps) and f(V0+eps), eps = U_offset/|c|.  The same is done here; the
+    # offset is a per-precision constant (chb::singularity_offset<T>()).
+    def _affine_root(self, e):
+        """Root V0 and slope c if e (constants folded) is c*V + d, else None."""
+        V = self.V
+        e = self._fold_expr(e)
+        try:
+            ev = sp.sympify(str(e), locals={str(x): x for x in _free(e)})
+        except Exception:  # noqa: BLE001
+            return None
+        if _free(ev) != {V}:
+            return None
+        c = sp.diff(ev, V)
+        if not c.is_Number or c == 0:
+            return None
+        d = ev.xreplace({V: sp.Integer(0)})
+        if not d.is_Number:
+            return None
+        return float(-d / c), float(c)
+
+    def _zero_roots(self, b):
+        """Roots in V of b when b is affine in V or of the form +-(exp(E) - 1), E affine."""
+        out = []
+        r = self._affine_root(b)
+        if r is not None:
+            out.append(r)
+        if isinstance(b, sp.Add) and len(b.args) == 2:
+            ex = [a for a in b.args if a.has(sp.exp)]
+            cs = [a for a in b.args if a.is_number]
+            if len(ex) == 1 and len(cs) == 1 and abs(abs(float(cs[0])) - 1.0) < 1e-15:
+                term, sign = ex[0], 1.0
+                if isinstance(term, sp.Mul) and term.args[0].is_number and float(term.args[0]) == -1:
+                    term = sp.Mul(*term.args[1:], evaluate=False) if len(term.args) > 2 else term.args[1]
+                    sign = -1.0
+                # exp(E) - 1 or 1 - exp(E) vanish at E = 0; exp(E) + 1 never does
+                if isinstance(term, sp.exp) and sign * float(cs[0]) < 0:
+                    r = self._affine_root(term.args[0])
+                    if r is not None:
+                        out.append(r)
+        return out
+
+    def _factor_roots(self, e, in_den, num, den):
+        """Roots of the factors of a product (through nested products and reciprocals)."""
+        if isinstance(e, sp.Pow) and e.exp.is_Number and float(e.exp) < 0:
+            self._factor_roots(e.base, not in_den, num, den)
+            return
+        if isinstance(e, sp.Mul):
+            for a in e.args:
+                self._factor_roots(a, in_den, num, den)
+            return
+        for r in self._zero_roots(e):
+            (den if in_den else num).append(r)
+
+    def _fix_expr(self, e):
+        V = self.V
+        if isinstance(e, sp.Piecewise):
+            return sp.Piecewise(*[(self._fix_expr(x), c) for x, c in e.args])
+        if V not in _free(e):
+            return e
+        num, den = [], []
+        self._factor_roots(e, False, num, den)
+        pts = []
+        for v0, c in den:
+            if any(abs(v0 - w0) <= 1e-9 * max(1.0, abs(v0)) for w0, _ in num):
+                if not any(abs(v0 - p[0]) <= 1e-9 * max(1.0, abs(v0)) for p in pts):
+                    pts.append((v0, c))
+        for v0, c in pts:
+            eps = sp.Mul(self.ueps, sp.Float(1.0 / abs(c), 17), evaluate=False)
+            lo = sp.Add(sp.Float(v0, 17), sp.Mul(-1, eps, evaluate=False), evaluate=False)
+            hi = sp.Add(sp.Float(v0, 17), eps, evaluate=False)
+            with sp.evaluate(False):
+                fa = e.xreplace({V: lo})
+                fb = e.xreplace({V: hi})
+                line = sp.Add(fa, sp.Mul(sp.Add(V, sp.Mul(-1, lo)), sp.Add(fb, sp.Mul(-1, fa)),
+                                         sp.Pow(sp.Mul(2, eps), -1)))
+                cond = sp.StrictLessThan(sp.Abs(sp.Add(V, sp.Float(-v0, 17))), eps)
+            e = sp.Piecewise((line, cond), (e, True))
+            self.singular_points.append(v0)
+        return e
+
+    def _fix_singularities(self):
+        self.ueps = sp.Symbol("__ueps", real=True)
+        self.singular = {}
+        for k in list(self.live):
+            self.singular_points = []
+            self.live[k] = self._fix_expr(self.live[k])
+            if self.singular_points:
+                self.singular[k] = list(self.singular_points)
+
     def _rl_analysis(self):
         self.rl = {}
         for s in self.states[1:]:
@@ -386,6 +480,8 @@ class ModelEmitter:
             return "stim"
         if s == self.cm_arg:
             return "cm"
+        if s == getattr(self, "ueps", None):
+            return "chb::singularity_offset<T>()"
         if s in self.psyms:
             return f"p[{self.psyms.index(s)}]"
         if s in self.states:
@@ -411,7 +507,7 @@ class ModelEmitter:
 
     def _names(self):
         names = {}
-        for s in list(self.live) + list(self.states) + [self.stim_arg, self.cm_arg] + self.psyms:
+        for s in list(self.live) + list(self.states) + [self.stim_arg, self.cm_arg, self.ueps] + self.psyms:
             names[s] = self.cname(s)
         return names
 

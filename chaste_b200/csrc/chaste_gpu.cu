@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <new>
@@ -59,8 +60,10 @@ struct cg_ctx {
     uint8_t* d_pset = nullptr;
     void* d_params = nullptr;
     uint8_t* d_cls8 = nullptr;
-    double *d_r = nullptr, *d_p0 = nullptr, *d_p1 = nullptr, *d_q = nullptr;
-    float *d_r32 = nullptr, *d_p32a = nullptr, *d_p32b = nullptr, *d_e32 = nullptr, *d_q32 = nullptr;
+    double *d_r = nullptr, *d_zp = nullptr, *d_p = nullptr, *d_q = nullptr;
+    float *d_r32 = nullptr, *d_z32 = nullptr, *d_p32 = nullptr, *d_q32 = nullptr, *d_e32 = nullptr;
+    long long halo = 0;           // zero entries on both sides of stencil-read vectors
+    int interior_cls = 0;
     double* d_partials = nullptr;
     GridSync* d_gs = nullptr;
     int* d_status = nullptr;
@@ -106,6 +109,24 @@ namespace {
         int rc_ = (x);                \
         if (rc_ != CG_OK) return rc_; \
     } while (0)
+
+template <typename P>
+int dalloc(cg_ctx* c, P** p, size_t bytes);
+
+// Allocate n entries with c->halo zeroed entries before and after; *p points at entry 0.
+template <typename P>
+int dalloc_haloed(cg_ctx* c, P** p, size_t n) {
+    P* base = nullptr;
+    const size_t tot = n + 2 * (size_t)c->halo;
+    int rc = dalloc(c, &base, tot * sizeof(P));
+    if (rc != 0) return rc;
+    if (cudaMemset(base, 0, tot * sizeof(P)) != cudaSuccess) {
+        cudaGetLastError();
+        return CG_ERR_CUDA;
+    }
+    *p = base + c->halo;
+    return 0;
+}
 
 template <typename P>
 int dalloc(cg_ctx* c, P** p, size_t bytes) {
@@ -266,19 +287,39 @@ int cg_destroy(cg_ctx* c) {
 // ---------------------------------------------------------------- mesh --
 namespace {
 
+using CgKernel = void (*)(CgArgs);
+
+// The CG kernel instance for this context: CSR, or the slab stencil with the
+// offset count unrolled at compile time (3 in 1D, 9 in 2D, 15 in 3D).
+template <bool MIXED>
+CgKernel pick_cg_kernel_t(const cg_ctx* c) {
+    if (!c->slab) return MIXED ? cg_mixed_kernel<false, 0> : cg_fp64_kernel<false, 0>;
+    switch (c->stencil.n_offsets) {
+        case 3: return MIXED ? cg_mixed_kernel<true, 3> : cg_fp64_kernel<true, 3>;
+        case 7: return MIXED ? cg_mixed_kernel<true, 7> : cg_fp64_kernel<true, 7>;
+        case 9: return MIXED ? cg_mixed_kernel<true, 9> : cg_fp64_kernel<true, 9>;
+        case 15: return MIXED ? cg_mixed_kernel<true, 15> : cg_fp64_kernel<true, 15>;
+        default: return MIXED ? cg_mixed_kernel<true, 0> : cg_fp64_kernel<true, 0>;
+    }
+}
+
+CgKernel pick_cg_kernel(const cg_ctx* c) {
+    return c->mixed() ? pick_cg_kernel_t<true>(c) : pick_cg_kernel_t<false>(c);
+}
+
 int alloc_vectors(cg_ctx* c) {
     const size_t n = (size_t)c->n;
-    CG_TRY(dalloc(c, &c->d_V, n * sizeof(double)));
+    CG_TRY(dalloc_haloed(c, &c->d_V, n));
+    CG_TRY(dalloc_haloed(c, &c->d_zp, n));
     CG_TRY(dalloc(c, &c->d_r, n * sizeof(double)));
-    CG_TRY(dalloc(c, &c->d_p0, n * sizeof(double)));
-    CG_TRY(dalloc(c, &c->d_p1, n * sizeof(double)));
-    if (!c->slab) CG_TRY(dalloc(c, &c->d_q, n * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_p, n * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_q, n * sizeof(double)));
     if (c->mixed()) {
+        CG_TRY(dalloc_haloed(c, &c->d_z32, n));
         CG_TRY(dalloc(c, &c->d_r32, n * sizeof(float)));
-        CG_TRY(dalloc(c, &c->d_p32a, n * sizeof(float)));
-        CG_TRY(dalloc(c, &c->d_p32b, n * sizeof(float)));
+        CG_TRY(dalloc(c, &c->d_p32, n * sizeof(float)));
+        CG_TRY(dalloc(c, &c->d_q32, n * sizeof(float)));
         CG_TRY(dalloc(c, &c->d_e32, n * sizeof(float)));
-        if (!c->slab) CG_TRY(dalloc(c, &c->d_q32, n * sizeof(float)));
     }
     CG_TRY(dalloc(c, &c->d_act, n * sizeof(double)));
     CG_TRY(dalloc(c, &c->d_gs, sizeof(GridSync)));
@@ -292,21 +333,14 @@ int alloc_vectors(cg_ctx* c) {
     CG_CUDA(cudaMemsetAsync(c->d_step, 0, sizeof(long long), s));
     CG_CUDA(cudaMemsetAsync(c->d_ring, 0, kRing * sizeof(int), s));
     CG_CUDA(cudaMemsetAsync(c->d_refine, 0, sizeof(int), s));
-    CG_CUDA(cudaMemsetAsync(c->d_V, 0, n * sizeof(double), s));
     CG_CUDA(cudaMemsetAsync(c->d_r, 0, n * sizeof(double), s));
-    CG_CUDA(cudaMemsetAsync(c->d_p0, 0, n * sizeof(double), s));
-    CG_CUDA(cudaMemsetAsync(c->d_p1, 0, n * sizeof(double), s));
+    CG_CUDA(cudaMemsetAsync(c->d_p, 0, n * sizeof(double), s));
+    CG_CUDA(cudaMemsetAsync(c->d_q, 0, n * sizeof(double), s));
     // launch shapes: the CG kernel is cooperative, so its grid must be co-resident
     int sms = 0;
     CG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
     int per_sm = 0;
-    if (c->mixed()) {
-        if (c->slab) CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_mixed_kernel<true>, 512, 0));
-        else CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_mixed_kernel<false>, 512, 0));
-    } else {
-        if (c->slab) CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fp64_kernel<true>, 512, 0));
-        else CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fp64_kernel<false>, 512, 0));
-    }
+    CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_cg_kernel(c), 512, 0));
     if (per_sm < 1) return CG_ERR_UNSUPPORTED;
     const long long want = ((long long)n + 511) / 512;
     c->cg_blocks = (int)std::max(1LL, std::min(want, (long long)per_sm * sms));
@@ -331,10 +365,18 @@ int upload_operator(cg_ctx* c) {
         CG_CUDA(cudaMemcpyAsync(c->d_atab32, a32.data(), tab * sizeof(float), cudaMemcpyHostToDevice, s));
         CG_CUDA(cudaMemcpyAsync(c->d_mtab32, m32.data(), tab * sizeof(float), cudaMemcpyHostToDevice, s));
         std::vector<uint8_t> cls((size_t)c->n);
+        std::vector<long long> count(st.n_classes, 0);
         const int NX = c->grid.NX(), NY = c->grid.NY(), NZ = c->grid.NZ();
         for (int k = 0; k < NZ; ++k)
             for (int j = 0; j < NY; ++j)
-                for (int i = 0; i < NX; ++i) cls[((size_t)k * NY + j) * NX + i] = (uint8_t)slab_class(c->grid, i, j, k);
+                for (int i = 0; i < NX; ++i) {
+                    const int cl = slab_class(c->grid, i, j, k);
+                    cls[((size_t)k * NY + j) * NX + i] = (uint8_t)cl;
+                    count[cl]++;
+                }
+        c->interior_cls = (int)(std::max_element(count.begin(), count.end()) - count.begin());
+        c->halo = 0;
+        for (int o = 0; o < st.n_offsets; ++o) c->halo = std::max<long long>(c->halo, std::abs(st.offsets[o]));
         CG_TRY(dalloc(c, &c->d_cls8, cls.size()));
         CG_CUDA(cudaMemcpyAsync(c->d_cls8, cls.data(), cls.size(), cudaMemcpyHostToDevice, s));
         c->diag_slot = -1;
@@ -460,7 +502,7 @@ int upload_cells_t(cg_ctx* c, const double* init, const int* pset, const double*
         c->d_states = p;
         CG_TRY(dalloc(c, &p, n * sizeof(T)));
         c->d_iion = p;
-        CG_TRY(dalloc(c, &p, n * sizeof(T)));
+        CG_TRY(dalloc_haloed(c, &p, n));
         c->d_z = p;
     }
     CG_TRY(ensure_stimulus_buffers(c));
@@ -544,6 +586,12 @@ CgArgs make_cg_args(cg_ctx* c) {
         const SlabStencil& st = c->stencil;
         a.slab.n_off = st.n_offsets;
         a.slab.n_cls = st.n_classes;
+        a.slab.interior = c->interior_cls;
+        for (int o = 0; o < st.n_offsets; ++o) {
+            a.slab.ia[o] = st.a[(size_t)c->interior_cls * st.n_offsets + o];
+            a.slab.im[o] = st.m[(size_t)c->interior_cls * st.n_offsets + o];
+            a.slab.ia32[o] = (float)a.slab.ia[o];
+        }
         for (int o = 0; o < st.n_offsets; ++o) a.slab.off[o] = st.offsets[o];
         a.slab.a_tab = c->d_atab;
         a.slab.m_tab = c->d_mtab;
@@ -563,14 +611,14 @@ CgArgs make_cg_args(cg_ctx* c) {
     a.zrhs32 = c->mixed() ? (const float*)c->d_z : nullptr;
     a.cls8 = c->d_cls8;
     a.r = c->d_r;
-    a.p0 = c->d_p0;
-    a.p1 = c->d_p1;
+    a.zp = c->d_zp;
+    a.p0 = c->d_p;
     a.q = c->d_q;
     a.r32 = c->d_r32;
-    a.p32a = c->d_p32a;
-    a.p32b = c->d_p32b;
-    a.e32 = c->d_e32;
+    a.z32 = c->d_z32;
+    a.p32 = c->d_p32;
     a.q32 = c->d_q32;
+    a.e32 = c->d_e32;
     a.partials = c->d_partials;
     a.gs = c->d_gs;
     a.status = c->d_status;
@@ -601,12 +649,7 @@ cudaError_t launch_cg(cg_ctx* c) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (c->mixed()) {
-        if (c->slab) return cudaLaunchKernelEx(&cfg, cg_mixed_kernel<true>, a);
-        return cudaLaunchKernelEx(&cfg, cg_mixed_kernel<false>, a);
-    }
-    if (c->slab) return cudaLaunchKernelEx(&cfg, cg_fp64_kernel<true>, a);
-    return cudaLaunchKernelEx(&cfg, cg_fp64_kernel<false>, a);
+    return cudaLaunchKernelEx(&cfg, pick_cg_kernel(c), a);
 }
 
 cudaError_t launch_step(cg_ctx* c) {

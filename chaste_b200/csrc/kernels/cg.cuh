@@ -4,12 +4,13 @@
 // convergence test of KSPConvergedDefault) from the guess V
 // (LinearSystem::Solve, linalg/src/LinearSystem.cpp:833-837, 1099).
 //
-// Per iteration two grid-wide reductions (p.Ap, then z.z and z.r) are done by
-// the bounded GridSync; every block derives the same scalars from the
-// deterministic block-order sums, so the loop exits uniformly.  Traffic per
-// iteration and node (slab operator, FP64): phase A reads r, p_old, class and
-// writes p_new (q = A p_new is formed from r and p_old on the fly); phase B
-// reads x, p_new, r, class and writes x, r, recomputing q from p_new.
+// Per iteration there are two grid-wide reductions (p.Ap, then z.z and z.r),
+// done by the bounded GridSync; every block derives the same scalars from the
+// deterministic block-order sums, so the loop exits uniformly.  The search
+// direction update and the product are fused through the recurrence
+//   p' = z + beta p,  A p' = A z + beta A p,
+// so each iteration applies the operator once (to the preconditioned residual
+// z, which is stored) and phase B touches only node-local values.
 #pragma once
 
 #include "common.cuh"
@@ -21,19 +22,19 @@ struct CgArgs {
     SlabOp slab;
     CsrOp csr;
     int n;
-    double* x;                  // V: initial guess in, solution out
-    const double* zrhs;         // z (FP64 path)
-    const float* zrhs32;        // z (mixed path)
+    double* x;                  // V: initial guess in, solution out (haloed)
+    const double* zrhs;         // per-node RHS term z (FP64 path, haloed)
+    const float* zrhs32;        // z (mixed path, haloed)
     const uint8_t* cls8;        // slab class per node
     double* r;
-    double* p0;
-    double* p1;
-    double* q;                  // CSR only
+    double* zp;                 // preconditioned residual B r (haloed)
+    double* p0;                 // search direction
+    double* q;                  // A p
     float* r32;                 // mixed path workspace
-    float* p32a;
-    float* p32b;
-    float* e32;
+    float* z32;                 // (haloed)
+    float* p32;
     float* q32;
+    float* e32;
     double* partials;           // gridDim.x * 4
     GridSync* gs;
     int* status;
@@ -49,28 +50,31 @@ struct CgArgs {
 };
 
 template <bool SLAB>
-__device__ __forceinline__ double dinv_of(const CgArgs& a, const SlabShared<double>& sh, int j) {
-    if (a.pc == 0) return 1.0;
-    if constexpr (SLAB) return sh.dinv[a.cls8[j]];
-    else return a.csr.dinv[j];
-}
-
-template <bool SLAB>
 __device__ __forceinline__ int class_of(const CgArgs& a, int i) {
     if constexpr (SLAB) return a.cls8[i];
     else return 0;
 }
 
-template <bool SLAB, class Load>
-__device__ __forceinline__ double rowA(const CgArgs& a, const SlabShared<double>& sh, int c, int i, Load ld) {
-    if constexpr (SLAB) return slab_row<double, double>(&sh.a[c * a.slab.n_off], sh.off, a.slab.n_off, i, ld);
-    else return csr_row<double, double>(a.csr.rowptr, a.csr.cols, a.csr.a, i, ld);
+template <bool SLAB>
+__device__ __forceinline__ double dinv_of(const CgArgs& a, const SlabShared<double>& sh, int c, int i) {
+    if (a.pc == 0) return 1.0;
+    if constexpr (SLAB) return sh.dinv[c];
+    else return a.csr.dinv[i];
 }
 
-template <bool SLAB, class Load>
-__device__ __forceinline__ double rowM(const CgArgs& a, const SlabShared<double>& sh, int c, int i, Load ld) {
-    if constexpr (SLAB) return slab_row<double, double>(&sh.m[c * a.slab.n_off], sh.off, a.slab.n_off, i, ld);
-    else return csr_row<double, double>(a.csr.rowptr, a.csr.cols, a.csr.m, i, ld);
+// y_i = (A x)_i or (M x)_i for the row of node i (class c)
+template <bool SLAB, int NOFF, bool MASS, typename X>
+__device__ __forceinline__ double apply_row(const CgArgs& a, const SlabShared<double>& sh, const int* soff,
+                                            int c, int i, const X* __restrict__ x) {
+    if constexpr (!SLAB) {
+        return csr_row<double, double>(a.csr.rowptr, a.csr.cols, MASS ? a.csr.m : a.csr.a, i, x);
+    } else if constexpr (NOFF > 0) {
+        if (c == a.slab.interior) return slab_row<NOFF, double, double>(MASS ? a.slab.im : a.slab.ia, a.slab.off, NOFF, i, x);
+        return slab_row<NOFF, double, double>(MASS ? &sh.m[c * NOFF] : &sh.a[c * NOFF], a.slab.off, NOFF, i, x);
+    } else {
+        const int no = a.slab.n_off;
+        return slab_row<0, double, double>(MASS ? &sh.m[c * no] : &sh.a[c * no], soff, no, i, x);
+    }
 }
 
 __device__ __forceinline__ void cg_finish(const CgArgs& a, long long step, int its, int bits) {
@@ -81,37 +85,43 @@ __device__ __forceinline__ void cg_finish(const CgArgs& a, long long step, int i
     }
 }
 
-template <bool SLAB>
+template <bool SLAB, int NOFF>
 __global__ void __launch_bounds__(512) cg_fp64_kernel(CgArgs a) {
     __shared__ SlabShared<double> sh;
+    __shared__ int soff[kMaxOffsets];
     __shared__ double red[32 * 4];
     __shared__ double red_out[4];
-    if constexpr (SLAB) slab_load_shared<double>(a.slab, sh, a.diag_slot);
+    if constexpr (SLAB) {
+        for (int k = threadIdx.x; k < a.slab.n_off; k += blockDim.x) soff[k] = a.slab.off[k];
+        slab_load_shared<double>(a.slab, sh, a.diag_slot);
+    }
     if (*(volatile int*)a.status & ~kStatusStateRange) return;
     const long long step = *a.step;
     const int n = a.n;
     const int stride = gridDim.x * blockDim.x;
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-    const double* __restrict__ z = a.zrhs;
     double* __restrict__ x = a.x;
     double* __restrict__ r = a.r;
+    double* __restrict__ zp = a.zp;
+    double* __restrict__ q = a.q;
     double res[4];
 
-    // ---- phase 0: r = M z - A x, norms of B b and B r
+    // ---- phase 0: r = M z - A x, z = B r, norms of B b and B r
     {
         double v[4] = {0, 0, 0, 0};
         for (int i = t0; i < n; i += stride) {
             const int c = class_of<SLAB>(a, i);
-            const double b = rowM<SLAB>(a, sh, c, i, [&](int j) { return z[j]; });
-            const double av = rowA<SLAB>(a, sh, c, i, [&](int j) { return x[j]; });
+            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs);
+            const double av = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, x);
             const double rr = b - av;
-            const double d = dinv_of<SLAB>(a, sh, i);
+            const double d = dinv_of<SLAB>(a, sh, c, i);
             const double w = d * b, zz = d * rr;
             v[0] += fabs(b);
             v[1] += w * w;
             v[2] += zz * zz;
             v[3] += rr * zz;
             r[i] = rr;
+            zp[i] = zz;
         }
         block_reduce<4>(v, red, red_out);
         if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status)) return;
@@ -124,11 +134,11 @@ __global__ void __launch_bounds__(512) cg_fp64_kernel(CgArgs a) {
         double v[2] = {0, 0};
         for (int i = t0; i < n; i += stride) {
             const int c = class_of<SLAB>(a, i);
-            const double b = rowM<SLAB>(a, sh, c, i, [&](int j) { return z[j]; });
-            const double d = dinv_of<SLAB>(a, sh, i);
-            const double zz = d * b;
+            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs);
+            const double zz = dinv_of<SLAB>(a, sh, c, i) * b;
             x[i] = 0.0;
             r[i] = b;
+            zp[i] = zz;
             v[0] += zz * zz;
             v[1] += b * zz;
         }
@@ -146,27 +156,22 @@ __global__ void __launch_bounds__(512) cg_fp64_kernel(CgArgs a) {
     if (dp >= a.dtol * rnorm0) return cg_finish(a, step, 0, kStatusCgDiverged);
 
     double betaold = 0.0;
-    double* po = a.p0;
-    double* pn = a.p1;
+    double* __restrict__ p = a.p0;   // p and A p are only read at their own row: updated in place
     int it = 0;
     for (; it < a.maxit; ++it) {
         if (beta == 0.0) return cg_finish(a, step, it + 1, 0);
         const double bc = it == 0 ? 0.0 : beta / betaold;
-        // ---- phase A: p_new = B r + bc p_old ; q = A p_new ; p_new . q
+        const bool first = it == 0;
+        // ---- phase A: p = z + bc p ; A p = A z + bc A p ; p . A p
         {
             double v[1] = {0};
-            const double* __restrict__ pold = po;
-            const bool first = it == 0;
-            auto pl = [&](int j) {
-                const double zj = dinv_of<SLAB>(a, sh, j) * r[j];
-                return first ? zj : zj + bc * pold[j];
-            };
             for (int i = t0; i < n; i += stride) {
                 const int c = class_of<SLAB>(a, i);
-                const double qi = rowA<SLAB>(a, sh, c, i, pl);
-                const double pi = pl(i);
-                pn[i] = pi;
-                if constexpr (!SLAB) a.q[i] = qi;
+                const double az = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, zp);
+                const double qi = first ? az : az + bc * q[i];
+                const double pi = first ? zp[i] : zp[i] + bc * p[i];
+                q[i] = qi;
+                p[i] = pi;
                 v[0] += pi * qi;
             }
             block_reduce<1>(v, red, red_out);
@@ -175,20 +180,16 @@ __global__ void __launch_bounds__(512) cg_fp64_kernel(CgArgs a) {
         const double dpi = res[0];
         if (!(dpi > 0.0)) return cg_finish(a, step, it + 1, isfinite(dpi) ? kStatusCgDiverged : kStatusNaN);
         const double alpha = beta / dpi;
-        // ---- phase B: x += alpha p ; r -= alpha q ; z = B r ; z.z, z.r
+        // ---- phase B: x += alpha p ; r -= alpha A p ; z = B r ; z.z, z.r
         {
             double v[2] = {0, 0};
-            const double* __restrict__ pnew = pn;
             for (int i = t0; i < n; i += stride) {
                 const int c = class_of<SLAB>(a, i);
-                double qi;
-                if constexpr (SLAB) qi = rowA<SLAB>(a, sh, c, i, [&](int j) { return pnew[j]; });
-                else qi = a.q[i];
-                const double pi = pnew[i];
-                x[i] += alpha * pi;
-                const double rr = r[i] - alpha * qi;
+                x[i] += alpha * p[i];
+                const double rr = r[i] - alpha * q[i];
                 r[i] = rr;
-                const double zz = dinv_of<SLAB>(a, sh, i) * rr;
+                const double zz = dinv_of<SLAB>(a, sh, c, i) * rr;
+                zp[i] = zz;
                 v[0] += zz * zz;
                 v[1] += zz * rr;
             }
@@ -201,9 +202,6 @@ __global__ void __launch_bounds__(512) cg_fp64_kernel(CgArgs a) {
         if (dp >= a.dtol * rnorm0) return cg_finish(a, step, it + 1, kStatusCgDiverged);
         betaold = beta;
         beta = res[1];
-        double* tmp = po;
-        po = pn;
-        pn = tmp;
     }
     cg_finish(a, step, it, kStatusCgMaxIt);
 }

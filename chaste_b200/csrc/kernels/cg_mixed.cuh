@@ -7,7 +7,8 @@
 //                                 sweep is expected to reach ttol)
 //      x += e ; r = b - A x      (FP64)
 // The inner vectors are float (half the bytes of the FP64 path); scalars and
-// reductions stay in double.
+// reductions stay in double.  The inner loop uses the same fused recurrence
+// as the FP64 kernel (one operator application per iteration).
 #pragma once
 
 #include "cg.cuh"
@@ -15,25 +16,35 @@
 namespace chb {
 
 template <bool SLAB>
-__device__ __forceinline__ float dinv32_of(const CgArgs& a, const SlabShared<float>& s32, int j) {
+__device__ __forceinline__ float dinv32_of(const CgArgs& a, const SlabShared<float>& s32, int c, int i) {
     if (a.pc == 0) return 1.0f;
-    if constexpr (SLAB) return s32.dinv[a.cls8[j]];
-    else return a.csr.dinv32[j];
+    if constexpr (SLAB) return s32.dinv[c];
+    else return a.csr.dinv32[i];
 }
 
-template <bool SLAB, class Load>
-__device__ __forceinline__ float rowA32(const CgArgs& a, const SlabShared<float>& s32, int c, int i, Load ld) {
-    if constexpr (SLAB) return slab_row<float, float>(&s32.a[c * a.slab.n_off], s32.off, a.slab.n_off, i, ld);
-    else return csr_row<float, float>(a.csr.rowptr, a.csr.cols, a.csr.a32, i, ld);
+template <bool SLAB, int NOFF>
+__device__ __forceinline__ float apply_row32(const CgArgs& a, const SlabShared<float>& s32, const int* soff,
+                                             int c, int i, const float* __restrict__ x) {
+    if constexpr (!SLAB) {
+        return csr_row<float, float>(a.csr.rowptr, a.csr.cols, a.csr.a32, i, x);
+    } else if constexpr (NOFF > 0) {
+        if (c == a.slab.interior) return slab_row<NOFF, float, float>(a.slab.ia32, a.slab.off, NOFF, i, x);
+        return slab_row<NOFF, float, float>(&s32.a[c * NOFF], a.slab.off, NOFF, i, x);
+    } else {
+        const int no = a.slab.n_off;
+        return slab_row<0, float, float>(&s32.a[c * no], soff, no, i, x);
+    }
 }
 
-template <bool SLAB>
+template <bool SLAB, int NOFF>
 __global__ void __launch_bounds__(512) cg_mixed_kernel(CgArgs a) {
     __shared__ SlabShared<double> sh;
     __shared__ SlabShared<float> s32;
+    __shared__ int soff[kMaxOffsets];
     __shared__ double red[32 * 4];
     __shared__ double red_out[4];
     if constexpr (SLAB) {
+        for (int k = threadIdx.x; k < a.slab.n_off; k += blockDim.x) soff[k] = a.slab.off[k];
         slab_load_shared<double>(a.slab, sh, a.diag_slot);
         slab_load_shared<float>(a.slab, s32, a.diag_slot);
     }
@@ -42,9 +53,11 @@ __global__ void __launch_bounds__(512) cg_mixed_kernel(CgArgs a) {
     const int n = a.n;
     const int stride = gridDim.x * blockDim.x;
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-    const float* __restrict__ z = a.zrhs32;
     double* __restrict__ x = a.x;
     float* __restrict__ r32 = a.r32;
+    float* __restrict__ z32 = a.z32;
+    float* __restrict__ p32 = a.p32;
+    float* __restrict__ q32 = a.q32;
     float* __restrict__ e32 = a.e32;
     double res[4];
     double rnorm0 = 0.0, ttol = 0.0, dp = 0.0, rz = 0.0;
@@ -52,23 +65,25 @@ __global__ void __launch_bounds__(512) cg_mixed_kernel(CgArgs a) {
     int sweeps = 0;
 
     for (int sweep = 0;; ++sweep) {
-        // ---- FP64 residual r = M z - A x; FP32 copy for the inner solve
+        // ---- FP64 residual r = M z - A x; its FP32 copy and B r start the inner solve
         {
             double v[4] = {0, 0, 0, 0};
             for (int i = t0; i < n; i += stride) {
                 const int c = class_of<SLAB>(a, i);
-                const double b = rowM<SLAB>(a, sh, c, i, [&](int j) { return (double)z[j]; });
-                const double av = rowA<SLAB>(a, sh, c, i, [&](int j) { return x[j]; });
+                const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs32);
+                const double av = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, x);
                 const double rr = b - av;
-                const double d = dinv_of<SLAB>(a, sh, i);
+                const double d = dinv_of<SLAB>(a, sh, c, i);
                 const double w = d * b, zz = d * rr;
                 v[0] += fabs(b);
                 v[1] += w * w;
                 v[2] += zz * zz;
                 const float rf = (float)rr;
+                const float zf = dinv32_of<SLAB>(a, s32, c, i) * rf;
                 r32[i] = rf;
+                z32[i] = zf;
                 e32[i] = 0.0f;
-                v[3] += (double)rf * (double)(dinv32_of<SLAB>(a, s32, i) * rf);
+                v[3] += (double)rf * (double)zf;
             }
             block_reduce<4>(v, red, red_out);
             if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status)) return;
@@ -94,27 +109,21 @@ __global__ void __launch_bounds__(512) cg_mixed_kernel(CgArgs a) {
         const double target = fmin(0.5, fmax(1e-6, 0.3 * ttol / dp));
         const double dp_in0 = dp;
         double beta = rz, betaold = 0.0;
-        float* po = a.p32a;
-        float* pn = a.p32b;
         int it = 0;
         bool inner_done = false;
         for (; it < a.maxit && !inner_done; ++it) {
             if (beta == 0.0) break;
             const float bc = it == 0 ? 0.0f : (float)(beta / betaold);
+            const bool first = it == 0;
             {
                 double v[1] = {0};
-                const float* __restrict__ pold = po;
-                const bool first = it == 0;
-                auto pl = [&](int j) {
-                    const float zj = dinv32_of<SLAB>(a, s32, j) * r32[j];
-                    return first ? zj : zj + bc * pold[j];
-                };
                 for (int i = t0; i < n; i += stride) {
                     const int c = class_of<SLAB>(a, i);
-                    const float qi = rowA32<SLAB>(a, s32, c, i, pl);
-                    const float pi = pl(i);
-                    pn[i] = pi;
-                    if constexpr (!SLAB) a.q32[i] = qi;
+                    const float az = apply_row32<SLAB, NOFF>(a, s32, soff, c, i, z32);
+                    const float qi = first ? az : az + bc * q32[i];
+                    const float pi = first ? z32[i] : z32[i] + bc * p32[i];
+                    q32[i] = qi;
+                    p32[i] = pi;
                     v[0] += (double)pi * (double)qi;
                 }
                 block_reduce<1>(v, red, red_out);
@@ -125,16 +134,13 @@ __global__ void __launch_bounds__(512) cg_mixed_kernel(CgArgs a) {
             const float alpha = (float)(beta / dpi);
             {
                 double v[2] = {0, 0};
-                const float* __restrict__ pnew = pn;
                 for (int i = t0; i < n; i += stride) {
                     const int c = class_of<SLAB>(a, i);
-                    float qi;
-                    if constexpr (SLAB) qi = rowA32<SLAB>(a, s32, c, i, [&](int j) { return pnew[j]; });
-                    else qi = a.q32[i];
-                    e32[i] += alpha * pnew[i];
-                    const float rr = r32[i] - alpha * qi;
+                    e32[i] += alpha * p32[i];
+                    const float rr = r32[i] - alpha * q32[i];
                     r32[i] = rr;
-                    const float zz = dinv32_of<SLAB>(a, s32, i) * rr;
+                    const float zz = dinv32_of<SLAB>(a, s32, c, i) * rr;
+                    z32[i] = zz;
                     v[0] += (double)zz * (double)zz;
                     v[1] += (double)zz * (double)rr;
                 }
@@ -145,12 +151,9 @@ __global__ void __launch_bounds__(512) cg_mixed_kernel(CgArgs a) {
             betaold = beta;
             beta = res[1];
             if (!(dp_in > target * dp_in0)) inner_done = true;
-            float* tmp = po;
-            po = pn;
-            pn = tmp;
         }
         total_its += it;
-        // ---- x += e (FP64); the next residual pass needs every x updated
+        // ---- x += e (FP64); the next residual pass reads neighbours' x
         {
             for (int i = t0; i < n; i += stride) x[i] += (double)e32[i];
             double v[1] = {0};

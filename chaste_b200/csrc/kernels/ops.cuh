@@ -13,10 +13,18 @@ constexpr int kMaxClasses = 27;
 // boundary class (3 per axis; x2 for the stagger parity in 2D) in a small
 // coefficient table, so a product streams only the vector and a 1-byte class
 // per node.  Offsets are in ascending column order, the order a sorted CSR row
-// sums in.
+// sums in.  Vectors read through the stencil carry a zero halo of `halo`
+// entries on both sides, so every i + off[o] of a node i is a valid address and
+// the row needs no bounds test (outside neighbours have coefficient 0).
 struct SlabOp {
     int n_off, n_cls;
+    int interior;          // the most frequent class
     int off[kMaxOffsets];
+    // the interior class row, passed by value so unrolled loops read it as
+    // constant-bank operands (no registers, no shared-memory loads)
+    double ia[kMaxOffsets];
+    double im[kMaxOffsets];
+    float ia32[kMaxOffsets];
     const double* a_tab;   // [cls][off]
     const double* m_tab;
     const float* a_tab32;
@@ -29,7 +37,6 @@ struct SlabShared {
     T a[kMaxClasses * kMaxOffsets];
     T m[kMaxClasses * kMaxOffsets];
     T dinv[kMaxClasses];
-    int off[kMaxOffsets];
 };
 
 template <typename T>
@@ -48,7 +55,6 @@ __device__ void slab_load_shared(const SlabOp& op, SlabShared<T>& sh, int diag_s
         sh.a[k] = at[k];
         sh.m[k] = mt[k];
     }
-    for (int k = threadIdx.x; k < op.n_off; k += blockDim.x) sh.off[k] = op.off[k];
     __syncthreads();
     for (int c = threadIdx.x; c < op.n_cls; c += blockDim.x) {
         const T d = sh.a[c * op.n_off + diag_slot];
@@ -57,14 +63,16 @@ __device__ void slab_load_shared(const SlabOp& op, SlabShared<T>& sh, int diag_s
     __syncthreads();
 }
 
-// sum_o coef[o] * ld(i + off[o]) over the nonzero coefficients (a zero marks a
-// neighbour outside the slab, whose index is never formed into a load)
-template <typename T, typename Acc, class Load>
-__device__ __forceinline__ Acc slab_row(const T* coef, const int* off, int n_off, int i, Load ld) {
+// sum_o coef[o] * x[i + off[o]]; NOFF > 0 unrolls a fixed offset count, 0 loops n_off.
+template <int NOFF, typename T, typename Acc, typename X>
+__device__ __forceinline__ Acc slab_row(const T* coef, const int* __restrict__ off, int n_off, int i,
+                                        const X* __restrict__ x) {
     Acc acc = Acc(0);
-    for (int o = 0; o < n_off; ++o) {
-        const T c = coef[o];
-        if (c != T(0)) acc += (Acc)c * (Acc)ld(i + off[o]);
+    if constexpr (NOFF > 0) {
+#pragma unroll
+        for (int o = 0; o < NOFF; ++o) acc += (Acc)coef[o] * (Acc)x[i + off[o]];
+    } else {
+        for (int o = 0; o < n_off; ++o) acc += (Acc)coef[o] * (Acc)x[i + off[o]];
     }
     return acc;
 }
@@ -80,12 +88,12 @@ struct CsrOp {
     const float* __restrict__ dinv32;
 };
 
-template <typename T, typename Acc, class Load>
+template <typename T, typename Acc, typename X>
 __device__ __forceinline__ Acc csr_row(const int* __restrict__ rp, const int* __restrict__ ci,
-                                       const T* __restrict__ v, int i, Load ld) {
+                                       const T* __restrict__ v, int i, const X* __restrict__ x) {
     Acc acc = Acc(0);
     const int e = rp[i + 1];
-    for (int k = rp[i]; k < e; ++k) acc += (Acc)v[k] * (Acc)ld(ci[k]);
+    for (int k = rp[i]; k < e; ++k) acc += (Acc)v[k] * (Acc)x[ci[k]];
     return acc;
 }
 

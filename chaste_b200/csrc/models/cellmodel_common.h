@@ -25,6 +25,17 @@
 
 namespace chb {
 
+// Half-width, in units of the exponent argument U, of the window around a
+// removable singularity of a GHK-type term within which the emitted code
+// interpolates linearly (as chaste_codegen's singularity fixes do).  FP32 needs
+// a wider window: exp(U) - 1 loses all digits once |U| nears float epsilon.
+template <typename T>
+CHB_HD constexpr T singularity_offset();
+template <>
+CHB_HD constexpr double singularity_offset<double>() { return 1e-7; }
+template <>
+CHB_HD constexpr float singularity_offset<float>() { return 2e-3f; }
+
 // Forward-Euler step of the non-voltage states with V clamped at y[0]
 // (AbstractCardiacCell::ComputeExceptVoltage with SetVoltageDerivativeToZero,
 // heart/src/odes/AbstractCardiacCell.cpp:90-105, one EulerIvpOdeSolver step,

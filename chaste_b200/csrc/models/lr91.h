@@ -33,7 +33,7 @@ struct LuoRudy1991 {
         const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*v_plateau_potassium_current__Kp*(y[0] - (-T(87.8929017138025))));
         const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*log((y[7]/T(1.0)))));
         const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
-        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0)))))) : T(1.0));
+        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
         const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
         const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*v_time_dependent_potassium_current_Xi_gate__Xi*(y[0] - (-T(77.56758438531939))));
         const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
@@ -41,7 +41,7 @@ struct LuoRudy1991 {
         const T v_time_independent_potassium_current_K1_gate__K1_infinity = (v_time_independent_potassium_current_K1_gate__alpha_K1/(v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1));
         const T v_time_independent_potassium_current__g_K1__scaled = (T(0.6047)*p[3]);
         const T v_time_independent_potassium_current__i_K1 = (v_time_independent_potassium_current__g_K1__scaled*v_time_independent_potassium_current_K1_gate__K1_infinity*(y[0] - (-T(87.8929017138025))));
-        const T v_fast_sodium_current_m_gate__alpha_m = ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - exp(((-T(0.1))*(y[0] + T(47.13))))));
+        const T v_fast_sodium_current_m_gate__alpha_m = (((chb::singularity_offset<T>()*T(10.0)) > fabs((y[0] + T(47.13)))) ? (((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) + ((y[0] - (-T(47.13) - (chb::singularity_offset<T>()*T(10.0))))*(((T(0.32)*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) - ((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(10.0))))) : ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - exp(((-T(0.1))*(y[0] + T(47.13)))))));
         const T v_fast_sodium_current_m_gate__beta_m = (T(0.08)*exp(((-y[0])/T(11.0))));
         const T v_fast_sodium_current_h_gate__alpha_h = ((y[0] < (-T(40.0))) ? (T(0.135)*exp(((T(80.0) + y[0])/(-T(6.8))))) : T(0.0));
         const T v_fast_sodium_current_h_gate__beta_h = ((y[0] < (-T(40.0))) ? ((T(3.56)*exp((T(0.079)*y[0]))) + (T(310000.0)*exp((T(0.35)*y[0])))) : (T(1.0)/(T(0.13)*(T(1.0) + exp(((y[0] + T(10.66))/(-T(11.1))))))));
@@ -78,7 +78,7 @@ struct LuoRudy1991 {
         const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*v_plateau_potassium_current__Kp*(y[0] - (-T(87.8929017138025))));
         const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*log((y[7]/T(1.0)))));
         const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
-        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0)))))) : T(1.0));
+        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
         const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
         const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*v_time_dependent_potassium_current_Xi_gate__Xi*(y[0] - (-T(77.56758438531939))));
         const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
@@ -86,7 +86,7 @@ struct LuoRudy1991 {
         const T v_time_independent_potassium_current_K1_gate__K1_infinity = (v_time_independent_potassium_current_K1_gate__alpha_K1/(v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1));
         const T v_time_independent_potassium_current__g_K1__scaled = (T(0.6047)*p[3]);
         const T v_time_independent_potassium_current__i_K1 = (v_time_independent_potassium_current__g_K1__scaled*v_time_independent_potassium_current_K1_gate__K1_infinity*(y[0] - (-T(87.8929017138025))));
-        const T v_fast_sodium_current_m_gate__alpha_m = ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - exp(((-T(0.1))*(y[0] + T(47.13))))));
+        const T v_fast_sodium_current_m_gate__alpha_m = (((chb::singularity_offset<T>()*T(10.0)) > fabs((y[0] + T(47.13)))) ? (((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) + ((y[0] - (-T(47.13) - (chb::singularity_offset<T>()*T(10.0))))*(((T(0.32)*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) - ((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(10.0))))) : ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - exp(((-T(0.1))*(y[0] + T(47.13)))))));
         const T v_fast_sodium_current_m_gate__beta_m = (T(0.08)*exp(((-y[0])/T(11.0))));
         const T v_fast_sodium_current_h_gate__alpha_h = ((y[0] < (-T(40.0))) ? (T(0.135)*exp(((T(80.0) + y[0])/(-T(6.8))))) : T(0.0));
         const T v_fast_sodium_current_h_gate__beta_h = ((y[0] < (-T(40.0))) ? ((T(3.56)*exp((T(0.079)*y[0]))) + (T(310000.0)*exp((T(0.35)*y[0])))) : (T(1.0)/(T(0.13)*(T(1.0) + exp(((y[0] + T(10.66))/(-T(11.1))))))));
@@ -126,7 +126,7 @@ struct LuoRudy1991 {
         const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*v_plateau_potassium_current__Kp*(y[0] - (-T(87.8929017138025))));
         const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*log((y[7]/T(1.0)))));
         const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
-        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0)))))) : T(1.0));
+        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
         const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
         const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*v_time_dependent_potassium_current_Xi_gate__Xi*(y[0] - (-T(77.56758438531939))));
         const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));

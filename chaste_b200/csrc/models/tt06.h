@@ -26,7 +26,7 @@ struct TenTusscher2006Epi {
     CHB_HD static void rhs(const T* __restrict__ y, T stim, T cm,
                                   const T* __restrict__ p, T* __restrict__ dy) {
         (void)stim; (void)cm; (void)p;
-        const T v_L_type_Ca_current__i_CaL = (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0)));
+        const T v_L_type_Ca_current__i_CaL = (((chb::singularity_offset<T>()*T(13.356880329847824)) > fabs((y[0] - T(15.0)))) ? ((((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))) + ((y[0] - (T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))))*((((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))) - (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))))/(T(2.0)*(chb::singularity_offset<T>()*T(13.356880329847824))))) : (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))));
         const T v_reversal_potentials__E_Ca = (((T(0.5)*T(8314.472)*T(310.0))/T(96485.3415))*log((T(2.0)/y[14])));
         const T v_calcium_background_current__i_b_Ca = (T(0.000592)*(y[0] - v_reversal_potentials__E_Ca));
         const T v_calcium_pump_current__i_p_Ca = ((T(0.1238)*y[14])/(y[14] + T(0.0005)));
@@ -125,7 +125,7 @@ struct TenTusscher2006Epi {
                                        const T* __restrict__ p, T* __restrict__ rate,
                                        T* __restrict__ inf) {
         (void)stim; (void)cm; (void)p; (void)inf;
-        const T v_L_type_Ca_current__i_CaL = (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0)));
+        const T v_L_type_Ca_current__i_CaL = (((chb::singularity_offset<T>()*T(13.356880329847824)) > fabs((y[0] - T(15.0)))) ? ((((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))) + ((y[0] - (T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))))*((((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))) - (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))))/(T(2.0)*(chb::singularity_offset<T>()*T(13.356880329847824))))) : (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))));
         const T v_reversal_potentials__E_Ca = (((T(0.5)*T(8314.472)*T(310.0))/T(96485.3415))*log((T(2.0)/y[14])));
         const T v_calcium_background_current__i_b_Ca = (T(0.000592)*(y[0] - v_reversal_potentials__E_Ca));
         const T v_calcium_pump_current__i_p_Ca = ((T(0.1238)*y[14])/(y[14] + T(0.0005)));
@@ -235,7 +235,7 @@ struct TenTusscher2006Epi {
     CHB_HD static T iionic(const T* __restrict__ y, T cm, const T* __restrict__ p) {
         (void)cm; (void)p;
         const T stim = T(0.0); (void)stim;
-        const T v_L_type_Ca_current__i_CaL = (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0)));
+        const T v_L_type_Ca_current__i_CaL = (((chb::singularity_offset<T>()*T(13.356880329847824)) > fabs((y[0] - T(15.0)))) ? ((((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))) + ((y[0] - (T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))))*((((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) + (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))) - (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*((T(15.0) - (chb::singularity_offset<T>()*T(13.356880329847824))) - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))))/(T(2.0)*(chb::singularity_offset<T>()*T(13.356880329847824))))) : (((((T(3.98e-05)*p[1])*y[7]*y[8]*y[9]*y[10]*T(4.0)*(y[0] - T(15.0))*(T(96485.3415)*T(96485.3415)))/(T(8314.472)*T(310.0)))*((T(0.25)*y[16]*exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0))))) - T(2.0)))/(exp(((T(2.0)*(y[0] - T(15.0))*T(96485.3415))/(T(8314.472)*T(310.0)))) - T(1.0))));
         const T v_reversal_potentials__E_Ca = (((T(0.5)*T(8314.472)*T(310.0))/T(96485.3415))*log((T(2.0)/y[14])));
         const T v_calcium_background_current__i_b_Ca = (T(0.000592)*(y[0] - v_reversal_potentials__E_Ca));
         const T v_calcium_pump_current__i_p_Ca = ((T(0.1238)*y[14])/(y[14] + T(0.0005)));

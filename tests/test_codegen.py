@@ -42,3 +42,47 @@ def test_rush_larsen_state_classification():
     rl = {n for n, f in zip(names, flags) if f}
     # the twelve gates plus R_prime (affine in itself); V and the concentrations by forward Euler
     assert rl == {"Xr1", "Xr2", "Xs", "m", "h", "j", "d", "f", "f2", "fCass", "s", "r", "R_prime"}
+
+
+def test_removable_singularities_are_finite_in_both_precisions(tmp_path):
+    """GHK-type 0/0 points (LR91 alpha_m at -47.13 mV and Xi at -77 mV, TT06 i_CaL at 15 mV) give
+    finite values in float and double, continuous with their neighbourhood."""
+    src = tmp_path / "s.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <cmath>
+#include "lr91.h"
+#include "tt06.h"
+template <class M, typename T> double iion_at(double v) {
+    T y[M::kNumStates], p[M::kNumParams];
+    for (int i = 0; i < M::kNumStates; ++i) y[i] = (T)M::kInitialStates[i];
+    for (int i = 0; i < M::kNumParams; ++i) p[i] = T(1);
+    y[0] = (T)v;
+    T dy[M::kNumStates];
+    M::template rhs<T>(y, T(0), T(1), p, dy);
+    double s = 0;
+    for (int i = 0; i < M::kNumStates; ++i) s += (double)dy[i];
+    return s + (double)M::template iionic<T>(y, T(1), p);
+}
+int main() {
+    const double pts[3] = {-47.13, -77.0, 15.0};
+    for (double v : pts) {
+        double a = iion_at<chb::LuoRudy1991, float>(v), b = iion_at<chb::LuoRudy1991, double>(v);
+        double c = iion_at<chb::TenTusscher2006Epi, float>(v), d = iion_at<chb::TenTusscher2006Epi, double>(v);
+        double e = iion_at<chb::TenTusscher2006Epi, double>(v + 1e-3);
+        std::printf("%.17g %.17g %.17g %.17g %.17g\n", a, b, c, d, e);
+    }
+}
+''')
+    exe = tmp_path / "s"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "chaste_b200", "csrc", "models"),
+                    str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    import math
+
+    for line in filter(None, out):
+        a, b, c, d, e = map(float, line.split())
+        assert all(math.isfinite(x) for x in (a, b, c, d, e))
+        assert abs(a - b) <= 1e-3 * max(1.0, abs(b))
+        assert abs(c - d) <= 1e-3 * max(1.0, abs(d))
+        assert abs(d - e) <= 1e-1 * max(1.0, abs(d))
