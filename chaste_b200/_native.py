@@ -93,6 +93,8 @@ SIGNATURES = {
     "cg_restore": (C.c_int, [_vp, _vp, C.c_size_t]),
     "cg_destroy": (C.c_int, [_vp]),
     "cg_status_string": (C.c_char_p, [C.c_int]),
+    "cg_slab_solve_noalloc": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double,
+                                        C.c_double, _dp, _vp, _vp, _vp, _ip]),
 }
 
 _lib = None

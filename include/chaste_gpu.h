@@ -160,6 +160,30 @@ int cg_restore(cg_ctx* ctx, const void* host_buffer, size_t bytes);
 int cg_destroy(cg_ctx* ctx);
 const char* cg_status_string(int status);
 
+/* Allocation-free diffusion solve of one PDE step on a regular slab.
+ *
+ * No counterpart in the reference: Chaste always owns its PETSc vectors.  This
+ * entry point is for callers that cannot allocate device memory (an embedding
+ * program whose pool owns every device buffer, or code running where
+ * cudaMalloc is not permitted): it solves (Am*Cm/dt*M + K) x = M z with the
+ * same CG + Jacobi/none preconditioning, tolerance and stopping test as
+ * cg_step, reading the caller's device buffers d_z and d_x (n doubles each;
+ * d_x holds the initial guess on entry and the solution on return), and uses
+ * a fixed device array inside the library for all of its workspace.
+ *
+ * Limit: slabs of at most 32768 nodes whose x-y plane (NX*NY + NX + 1) also
+ * fits in 32768; larger sizes are rejected with CG_ERR_ARG.  The array is
+ * reserved on every GPU that loads the library until the process exits and is
+ * shared by all calls: calls that overlap on the GPU race, so serialise them.
+ * The first call on a device resolves the array's device address and should be
+ * made before any stream capture.  stream may be NULL (legacy default stream);
+ * the call returns after the solve has completed on it.  cfg supplies
+ * pde_time_step, Am, Cm, the KSP tolerance/preconditioner, max_iterations and
+ * mass lumping; FP64 only. */
+int cg_slab_solve_noalloc(const cg_config* cfg, int dim, double h, double width, double height,
+                          double depth, const double* sigma, const double* d_z, double* d_x,
+                          void* stream, int* iterations);
+
 #ifdef __cplusplus
 }
 #endif
