@@ -151,19 +151,19 @@ class Printer:
                     bs = self.p(b)
                     return f"({bs}*{bs}*{bs})"
                 if xv == 0.5:
-                    return f"sqrt({self.p(b)})"
+                    return f"m_sqrt({self.p(b)})"
                 if xv == -1:
                     return f"(T(1.0)/{self.p(b)})"
                 if xv == int(xv) and 4 <= xv <= 8:
                     bs = self.p(b)
                     return "(" + "*".join([bs] * int(xv)) + ")"
-            return f"pow({self.p(b)}, {self.p(x)})"
+            return f"m_pow({self.p(b)}, {self.p(x)})"
         if isinstance(e, sp.exp):
-            return f"exp({self.p(e.args[0])})"
+            return f"m_exp({self.p(e.args[0])})"
         if isinstance(e, sp.log):
             if len(e.args) == 2:
-                return f"(log({self.p(e.args[0])})/log({self.p(e.args[1])}))"
-            return f"log({self.p(e.args[0])})"
+                return f"(m_log({self.p(e.args[0])})/m_log({self.p(e.args[1])}))"
+            return f"m_log({self.p(e.args[0])})"
         if isinstance(e, sp.floor):
             return f"floor({self.p(e.args[0])})"
         if isinstance(e, sp.Abs):

@@ -343,7 +343,7 @@ int alloc_vectors(cg_ctx* c) {
     CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_cg_kernel(c), 512, 0));
     if (per_sm < 1) return CG_ERR_UNSUPPORTED;
     const long long want = ((long long)n + 511) / 512;
-    c->cg_blocks = (int)std::max(1LL, std::min(want, (long long)per_sm * sms));
+    c->cg_blocks = (int)std::max(1LL, std::min({want, (long long)per_sm * sms, (long long)kMaxGridBlocks}));
     CG_TRY(dalloc(c, &c->d_partials, (size_t)c->cg_blocks * 4 * sizeof(double)));
     c->ode_blocks = (int)std::max(1LL, std::min(((long long)n + 255) / 256, (long long)sms * 16));
     CG_CUDA(cudaStreamSynchronize(s));

@@ -106,7 +106,8 @@ __global__ void __launch_bounds__(512) cg_mixed_kernel(CgArgs a) {
         }
         sweeps++;
         // ---- FP32 PCG on A e = r
-        const double target = fmin(0.5, fmax(1e-6, 0.3 * ttol / dp));
+        // aim one decade below what reaching ttol needs, so that one sweep usually suffices
+        const double target = fmin(0.5, fmax(1e-6, 0.1 * ttol / dp));
         const double dp_in0 = dp;
         double beta = rz, betaold = 0.0;
         int it = 0;

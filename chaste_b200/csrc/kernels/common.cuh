@@ -71,6 +71,7 @@ struct GridSync {
 };
 
 constexpr long long kBarrierSpinLimit = 20000000;   // x ~100 ns sleep ~ 2 s
+constexpr int kMaxGridBlocks = 512;                  // largest grid a persistent kernel is launched with
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -124,10 +125,19 @@ __device__ bool grid_reduce(GridSync* gs, double* partials, const double* block_
         if (ticket == gridDim.x - 1) {
             __threadfence();
             __syncwarp();
+            // all loads of a lane are issued before any is used (grids of at most
+            // kMaxGridBlocks blocks), so the reduction costs one L2 round trip
 #pragma unroll
             for (int k = 0; k < NV; ++k) {
+                double vals[kMaxGridBlocks / 32];
+#pragma unroll
+                for (int m = 0; m < kMaxGridBlocks / 32; ++m) {
+                    const unsigned b = lane + 32u * m;
+                    vals[m] = b < gridDim.x ? __ldcg(&partials[b * NV + k]) : 0.0;
+                }
                 double s = 0.0;
-                for (unsigned b = lane; b < gridDim.x; b += 32) s += __ldcg(&partials[b * NV + k]);
+#pragma unroll
+                for (int m = 0; m < kMaxGridBlocks / 32; ++m) s += vals[m];
                 s = warp_sum(s);
                 if (lane == 0) gs->result[k] = s;
             }

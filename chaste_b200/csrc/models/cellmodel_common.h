@@ -15,7 +15,7 @@
 #define CHB_HD __host__ __device__ __forceinline__
 #define CHB_UNROLL _Pragma("unroll")
 #else
-#define CHB_HD
+#define CHB_HD inline
 #define CHB_UNROLL
 #endif
 
@@ -24,6 +24,41 @@
 #endif
 
 namespace chb {
+
+// Elementary functions seen by the generated model code (which calls exp/log/
+// sqrt as m_exp/m_log/m_sqrt/m_pow).  Double precision always calls the correctly rounded library
+// functions; single precision on the device uses the SFU-based fast
+// intrinsics (MUFU.EX2/LG2) when CHB_FAST_FP32 is 1 -- the mixed-precision
+// path trades their few-ulp error for throughput and is checked against FP64.
+#ifndef CHB_FAST_FP32
+#define CHB_FAST_FP32 1
+#endif
+CHB_HD double m_exp(double x) { return ::exp(x); }
+CHB_HD double m_log(double x) { return ::log(x); }
+CHB_HD double m_sqrt(double x) { return ::sqrt(x); }
+CHB_HD double m_pow(double x, double y) { return ::pow(x, y); }
+CHB_HD float m_exp(float x) {
+#if defined(__CUDA_ARCH__) && CHB_FAST_FP32
+    return __expf(x);
+#else
+    return ::expf(x);
+#endif
+}
+CHB_HD float m_log(float x) {
+#if defined(__CUDA_ARCH__) && CHB_FAST_FP32
+    return __logf(x);
+#else
+    return ::logf(x);
+#endif
+}
+CHB_HD float m_sqrt(float x) { return ::sqrtf(x); }
+CHB_HD float m_pow(float x, float y) {
+#if defined(__CUDA_ARCH__) && CHB_FAST_FP32
+    return __powf(x, y);
+#else
+    return ::powf(x, y);
+#endif
+}
 
 // Half-width, in units of the exponent argument U, of the window around a
 // removable singularity of a GHK-type term within which the emitted code
@@ -59,7 +94,7 @@ CHB_HD void rl_step_except_voltage(T* y, T stim, T cm, const T* p, T dt) {
 CHB_UNROLL
     for (int i = 1; i < Model::kNumStates; ++i) {
         if (Model::rush_larsen(i)) {
-            y[i] = inf[i] + (y[i] - inf[i]) * exp(rate[i] * dt);
+            y[i] = inf[i] + (y[i] - inf[i]) * m_exp(rate[i] * dt);
         } else {
             y[i] += dt * rate[i];
         }
@@ -87,7 +122,7 @@ CHB_HD void rl_step(T* y, T stim, T cm, const T* p, T dt) {
 CHB_UNROLL
     for (int i = 1; i < Model::kNumStates; ++i) {
         if (Model::rush_larsen(i)) {
-            y[i] = inf[i] + (y[i] - inf[i]) * exp(rate[i] * dt);
+            y[i] = inf[i] + (y[i] - inf[i]) * m_exp(rate[i] * dt);
         } else {
             y[i] += dt * rate[i];
         }

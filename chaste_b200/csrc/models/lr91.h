@@ -29,30 +29,30 @@ struct LuoRudy1991 {
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
         const T v_fast_sodium_current__i_Na = ((T(23.0)*p[0])*(y[1]*y[1]*y[1])*y[2]*y[3]*(y[0] - T(54.79446393509185)));
         const T v_membrane__I_stim = stim;
-        const T v_plateau_potassium_current__Kp = (T(1.0)/(T(1.0) + exp(((T(7.488) - y[0])/T(5.98)))));
+        const T v_plateau_potassium_current__Kp = (T(1.0)/(T(1.0) + m_exp(((T(7.488) - y[0])/T(5.98)))));
         const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*v_plateau_potassium_current__Kp*(y[0] - (-T(87.8929017138025))));
-        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*log((y[7]/T(1.0)))));
+        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*m_log((y[7]/T(1.0)))));
         const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
-        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
+        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(m_exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*m_exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
         const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
         const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*v_time_dependent_potassium_current_Xi_gate__Xi*(y[0] - (-T(77.56758438531939))));
-        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
-        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (((T(0.49124)*exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31)))))))/(T(1.0) + exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753))))));
+        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + m_exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
+        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (((T(0.49124)*m_exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*m_exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31)))))))/(T(1.0) + m_exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753))))));
         const T v_time_independent_potassium_current_K1_gate__K1_infinity = (v_time_independent_potassium_current_K1_gate__alpha_K1/(v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1));
         const T v_time_independent_potassium_current__g_K1__scaled = (T(0.6047)*p[3]);
         const T v_time_independent_potassium_current__i_K1 = (v_time_independent_potassium_current__g_K1__scaled*v_time_independent_potassium_current_K1_gate__K1_infinity*(y[0] - (-T(87.8929017138025))));
-        const T v_fast_sodium_current_m_gate__alpha_m = (((chb::singularity_offset<T>()*T(10.0)) > fabs((y[0] + T(47.13)))) ? (((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) + ((y[0] - (-T(47.13) - (chb::singularity_offset<T>()*T(10.0))))*(((T(0.32)*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) - ((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(10.0))))) : ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - exp(((-T(0.1))*(y[0] + T(47.13)))))));
-        const T v_fast_sodium_current_m_gate__beta_m = (T(0.08)*exp(((-y[0])/T(11.0))));
-        const T v_fast_sodium_current_h_gate__alpha_h = ((y[0] < (-T(40.0))) ? (T(0.135)*exp(((T(80.0) + y[0])/(-T(6.8))))) : T(0.0));
-        const T v_fast_sodium_current_h_gate__beta_h = ((y[0] < (-T(40.0))) ? ((T(3.56)*exp((T(0.079)*y[0]))) + (T(310000.0)*exp((T(0.35)*y[0])))) : (T(1.0)/(T(0.13)*(T(1.0) + exp(((y[0] + T(10.66))/(-T(11.1))))))));
-        const T v_fast_sodium_current_j_gate__alpha_j = ((y[0] < (-T(40.0))) ? (((((-T(127140.0))*exp((T(0.2444)*y[0]))) - (T(3.474e-05)*exp(((-T(0.04391))*y[0]))))*(y[0] + T(37.78)))/(T(1.0) + exp((T(0.311)*(y[0] + T(79.23)))))) : T(0.0));
-        const T v_fast_sodium_current_j_gate__beta_j = ((y[0] < (-T(40.0))) ? ((T(0.1212)*exp(((-T(0.01052))*y[0])))/(T(1.0) + exp(((-T(0.1378))*(y[0] + T(40.14)))))) : ((T(0.3)*exp(((-T(2.535e-07))*y[0])))/(T(1.0) + exp(((-T(0.1))*(y[0] + T(32.0)))))));
-        const T v_slow_inward_current_d_gate__alpha_d = ((T(0.095)*exp(((-T(0.01))*(y[0] - T(5.0)))))/(T(1.0) + exp(((-T(0.072))*(y[0] - T(5.0))))));
-        const T v_slow_inward_current_d_gate__beta_d = ((T(0.07)*exp(((-T(0.017))*(y[0] + T(44.0)))))/(T(1.0) + exp((T(0.05)*(y[0] + T(44.0))))));
-        const T v_slow_inward_current_f_gate__alpha_f = ((T(0.012)*exp(((-T(0.008))*(y[0] + T(28.0)))))/(T(1.0) + exp((T(0.15)*(y[0] + T(28.0))))));
-        const T v_slow_inward_current_f_gate__beta_f = ((T(0.0065)*exp(((-T(0.02))*(y[0] + T(30.0)))))/(T(1.0) + exp(((-T(0.2))*(y[0] + T(30.0))))));
-        const T v_time_dependent_potassium_current_X_gate__alpha_X = ((T(0.0005)*exp((T(0.083)*(y[0] + T(50.0)))))/(T(1.0) + exp((T(0.057)*(y[0] + T(50.0))))));
-        const T v_time_dependent_potassium_current_X_gate__beta_X = ((T(0.0013)*exp(((-T(0.06))*(y[0] + T(20.0)))))/(T(1.0) + exp(((-T(0.04))*(y[0] + T(20.0))))));
+        const T v_fast_sodium_current_m_gate__alpha_m = (((chb::singularity_offset<T>()*T(10.0)) > fabs((y[0] + T(47.13)))) ? (((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) + ((y[0] - (-T(47.13) - (chb::singularity_offset<T>()*T(10.0))))*(((T(0.32)*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) - ((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(10.0))))) : ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*(y[0] + T(47.13)))))));
+        const T v_fast_sodium_current_m_gate__beta_m = (T(0.08)*m_exp(((-y[0])/T(11.0))));
+        const T v_fast_sodium_current_h_gate__alpha_h = ((y[0] < (-T(40.0))) ? (T(0.135)*m_exp(((T(80.0) + y[0])/(-T(6.8))))) : T(0.0));
+        const T v_fast_sodium_current_h_gate__beta_h = ((y[0] < (-T(40.0))) ? ((T(3.56)*m_exp((T(0.079)*y[0]))) + (T(310000.0)*m_exp((T(0.35)*y[0])))) : (T(1.0)/(T(0.13)*(T(1.0) + m_exp(((y[0] + T(10.66))/(-T(11.1))))))));
+        const T v_fast_sodium_current_j_gate__alpha_j = ((y[0] < (-T(40.0))) ? (((((-T(127140.0))*m_exp((T(0.2444)*y[0]))) - (T(3.474e-05)*m_exp(((-T(0.04391))*y[0]))))*(y[0] + T(37.78)))/(T(1.0) + m_exp((T(0.311)*(y[0] + T(79.23)))))) : T(0.0));
+        const T v_fast_sodium_current_j_gate__beta_j = ((y[0] < (-T(40.0))) ? ((T(0.1212)*m_exp(((-T(0.01052))*y[0])))/(T(1.0) + m_exp(((-T(0.1378))*(y[0] + T(40.14)))))) : ((T(0.3)*m_exp(((-T(2.535e-07))*y[0])))/(T(1.0) + m_exp(((-T(0.1))*(y[0] + T(32.0)))))));
+        const T v_slow_inward_current_d_gate__alpha_d = ((T(0.095)*m_exp(((-T(0.01))*(y[0] - T(5.0)))))/(T(1.0) + m_exp(((-T(0.072))*(y[0] - T(5.0))))));
+        const T v_slow_inward_current_d_gate__beta_d = ((T(0.07)*m_exp(((-T(0.017))*(y[0] + T(44.0)))))/(T(1.0) + m_exp((T(0.05)*(y[0] + T(44.0))))));
+        const T v_slow_inward_current_f_gate__alpha_f = ((T(0.012)*m_exp(((-T(0.008))*(y[0] + T(28.0)))))/(T(1.0) + m_exp((T(0.15)*(y[0] + T(28.0))))));
+        const T v_slow_inward_current_f_gate__beta_f = ((T(0.0065)*m_exp(((-T(0.02))*(y[0] + T(30.0)))))/(T(1.0) + m_exp(((-T(0.2))*(y[0] + T(30.0))))));
+        const T v_time_dependent_potassium_current_X_gate__alpha_X = ((T(0.0005)*m_exp((T(0.083)*(y[0] + T(50.0)))))/(T(1.0) + m_exp((T(0.057)*(y[0] + T(50.0))))));
+        const T v_time_dependent_potassium_current_X_gate__beta_X = ((T(0.0013)*m_exp(((-T(0.06))*(y[0] + T(20.0)))))/(T(1.0) + m_exp(((-T(0.04))*(y[0] + T(20.0))))));
         dy[0] = (((-T(1.0))/T(1.0))*(v_membrane__I_stim + v_fast_sodium_current__i_Na + v_slow_inward_current__i_si + v_time_dependent_potassium_current__i_K + v_time_independent_potassium_current__i_K1 + v_plateau_potassium_current__i_Kp + v_background_current__i_b));
         dy[1] = ((v_fast_sodium_current_m_gate__alpha_m*(T(1.0) - y[1])) - (v_fast_sodium_current_m_gate__beta_m*y[1]));
         dy[2] = ((v_fast_sodium_current_h_gate__alpha_h*(T(1.0) - y[2])) - (v_fast_sodium_current_h_gate__beta_h*y[2]));
@@ -74,30 +74,30 @@ struct LuoRudy1991 {
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
         const T v_fast_sodium_current__i_Na = ((T(23.0)*p[0])*(y[1]*y[1]*y[1])*y[2]*y[3]*(y[0] - T(54.79446393509185)));
         const T v_membrane__I_stim = stim;
-        const T v_plateau_potassium_current__Kp = (T(1.0)/(T(1.0) + exp(((T(7.488) - y[0])/T(5.98)))));
+        const T v_plateau_potassium_current__Kp = (T(1.0)/(T(1.0) + m_exp(((T(7.488) - y[0])/T(5.98)))));
         const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*v_plateau_potassium_current__Kp*(y[0] - (-T(87.8929017138025))));
-        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*log((y[7]/T(1.0)))));
+        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*m_log((y[7]/T(1.0)))));
         const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
-        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
+        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(m_exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*m_exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
         const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
         const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*v_time_dependent_potassium_current_Xi_gate__Xi*(y[0] - (-T(77.56758438531939))));
-        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
-        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (((T(0.49124)*exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31)))))))/(T(1.0) + exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753))))));
+        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + m_exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
+        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (((T(0.49124)*m_exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*m_exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31)))))))/(T(1.0) + m_exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753))))));
         const T v_time_independent_potassium_current_K1_gate__K1_infinity = (v_time_independent_potassium_current_K1_gate__alpha_K1/(v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1));
         const T v_time_independent_potassium_current__g_K1__scaled = (T(0.6047)*p[3]);
         const T v_time_independent_potassium_current__i_K1 = (v_time_independent_potassium_current__g_K1__scaled*v_time_independent_potassium_current_K1_gate__K1_infinity*(y[0] - (-T(87.8929017138025))));
-        const T v_fast_sodium_current_m_gate__alpha_m = (((chb::singularity_offset<T>()*T(10.0)) > fabs((y[0] + T(47.13)))) ? (((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) + ((y[0] - (-T(47.13) - (chb::singularity_offset<T>()*T(10.0))))*(((T(0.32)*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) - ((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(10.0))))) : ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - exp(((-T(0.1))*(y[0] + T(47.13)))))));
-        const T v_fast_sodium_current_m_gate__beta_m = (T(0.08)*exp(((-y[0])/T(11.0))));
-        const T v_fast_sodium_current_h_gate__alpha_h = ((y[0] < (-T(40.0))) ? (T(0.135)*exp(((T(80.0) + y[0])/(-T(6.8))))) : T(0.0));
-        const T v_fast_sodium_current_h_gate__beta_h = ((y[0] < (-T(40.0))) ? ((T(3.56)*exp((T(0.079)*y[0]))) + (T(310000.0)*exp((T(0.35)*y[0])))) : (T(1.0)/(T(0.13)*(T(1.0) + exp(((y[0] + T(10.66))/(-T(11.1))))))));
-        const T v_fast_sodium_current_j_gate__alpha_j = ((y[0] < (-T(40.0))) ? (((((-T(127140.0))*exp((T(0.2444)*y[0]))) - (T(3.474e-05)*exp(((-T(0.04391))*y[0]))))*(y[0] + T(37.78)))/(T(1.0) + exp((T(0.311)*(y[0] + T(79.23)))))) : T(0.0));
-        const T v_fast_sodium_current_j_gate__beta_j = ((y[0] < (-T(40.0))) ? ((T(0.1212)*exp(((-T(0.01052))*y[0])))/(T(1.0) + exp(((-T(0.1378))*(y[0] + T(40.14)))))) : ((T(0.3)*exp(((-T(2.535e-07))*y[0])))/(T(1.0) + exp(((-T(0.1))*(y[0] + T(32.0)))))));
-        const T v_slow_inward_current_d_gate__alpha_d = ((T(0.095)*exp(((-T(0.01))*(y[0] - T(5.0)))))/(T(1.0) + exp(((-T(0.072))*(y[0] - T(5.0))))));
-        const T v_slow_inward_current_d_gate__beta_d = ((T(0.07)*exp(((-T(0.017))*(y[0] + T(44.0)))))/(T(1.0) + exp((T(0.05)*(y[0] + T(44.0))))));
-        const T v_slow_inward_current_f_gate__alpha_f = ((T(0.012)*exp(((-T(0.008))*(y[0] + T(28.0)))))/(T(1.0) + exp((T(0.15)*(y[0] + T(28.0))))));
-        const T v_slow_inward_current_f_gate__beta_f = ((T(0.0065)*exp(((-T(0.02))*(y[0] + T(30.0)))))/(T(1.0) + exp(((-T(0.2))*(y[0] + T(30.0))))));
-        const T v_time_dependent_potassium_current_X_gate__alpha_X = ((T(0.0005)*exp((T(0.083)*(y[0] + T(50.0)))))/(T(1.0) + exp((T(0.057)*(y[0] + T(50.0))))));
-        const T v_time_dependent_potassium_current_X_gate__beta_X = ((T(0.0013)*exp(((-T(0.06))*(y[0] + T(20.0)))))/(T(1.0) + exp(((-T(0.04))*(y[0] + T(20.0))))));
+        const T v_fast_sodium_current_m_gate__alpha_m = (((chb::singularity_offset<T>()*T(10.0)) > fabs((y[0] + T(47.13)))) ? (((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) + ((y[0] - (-T(47.13) - (chb::singularity_offset<T>()*T(10.0))))*(((T(0.32)*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))) - ((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(10.0))))) : ((T(0.32)*(y[0] + T(47.13)))/(T(1.0) - m_exp(((-T(0.1))*(y[0] + T(47.13)))))));
+        const T v_fast_sodium_current_m_gate__beta_m = (T(0.08)*m_exp(((-y[0])/T(11.0))));
+        const T v_fast_sodium_current_h_gate__alpha_h = ((y[0] < (-T(40.0))) ? (T(0.135)*m_exp(((T(80.0) + y[0])/(-T(6.8))))) : T(0.0));
+        const T v_fast_sodium_current_h_gate__beta_h = ((y[0] < (-T(40.0))) ? ((T(3.56)*m_exp((T(0.079)*y[0]))) + (T(310000.0)*m_exp((T(0.35)*y[0])))) : (T(1.0)/(T(0.13)*(T(1.0) + m_exp(((y[0] + T(10.66))/(-T(11.1))))))));
+        const T v_fast_sodium_current_j_gate__alpha_j = ((y[0] < (-T(40.0))) ? (((((-T(127140.0))*m_exp((T(0.2444)*y[0]))) - (T(3.474e-05)*m_exp(((-T(0.04391))*y[0]))))*(y[0] + T(37.78)))/(T(1.0) + m_exp((T(0.311)*(y[0] + T(79.23)))))) : T(0.0));
+        const T v_fast_sodium_current_j_gate__beta_j = ((y[0] < (-T(40.0))) ? ((T(0.1212)*m_exp(((-T(0.01052))*y[0])))/(T(1.0) + m_exp(((-T(0.1378))*(y[0] + T(40.14)))))) : ((T(0.3)*m_exp(((-T(2.535e-07))*y[0])))/(T(1.0) + m_exp(((-T(0.1))*(y[0] + T(32.0)))))));
+        const T v_slow_inward_current_d_gate__alpha_d = ((T(0.095)*m_exp(((-T(0.01))*(y[0] - T(5.0)))))/(T(1.0) + m_exp(((-T(0.072))*(y[0] - T(5.0))))));
+        const T v_slow_inward_current_d_gate__beta_d = ((T(0.07)*m_exp(((-T(0.017))*(y[0] + T(44.0)))))/(T(1.0) + m_exp((T(0.05)*(y[0] + T(44.0))))));
+        const T v_slow_inward_current_f_gate__alpha_f = ((T(0.012)*m_exp(((-T(0.008))*(y[0] + T(28.0)))))/(T(1.0) + m_exp((T(0.15)*(y[0] + T(28.0))))));
+        const T v_slow_inward_current_f_gate__beta_f = ((T(0.0065)*m_exp(((-T(0.02))*(y[0] + T(30.0)))))/(T(1.0) + m_exp(((-T(0.2))*(y[0] + T(30.0))))));
+        const T v_time_dependent_potassium_current_X_gate__alpha_X = ((T(0.0005)*m_exp((T(0.083)*(y[0] + T(50.0)))))/(T(1.0) + m_exp((T(0.057)*(y[0] + T(50.0))))));
+        const T v_time_dependent_potassium_current_X_gate__beta_X = ((T(0.0013)*m_exp(((-T(0.06))*(y[0] + T(20.0)))))/(T(1.0) + m_exp(((-T(0.04))*(y[0] + T(20.0))))));
         rate[0] = (((-T(1.0))/T(1.0))*(v_membrane__I_stim + v_fast_sodium_current__i_Na + v_slow_inward_current__i_si + v_time_dependent_potassium_current__i_K + v_time_independent_potassium_current__i_K1 + v_plateau_potassium_current__i_Kp + v_background_current__i_b));
         inf[1] = (-(v_fast_sodium_current_m_gate__alpha_m/(-v_fast_sodium_current_m_gate__alpha_m - v_fast_sodium_current_m_gate__beta_m)));
         rate[1] = (-v_fast_sodium_current_m_gate__alpha_m - v_fast_sodium_current_m_gate__beta_m);
@@ -122,15 +122,15 @@ struct LuoRudy1991 {
         const T stim = T(0.0); (void)stim;
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
         const T v_fast_sodium_current__i_Na = ((T(23.0)*p[0])*(y[1]*y[1]*y[1])*y[2]*y[3]*(y[0] - T(54.79446393509185)));
-        const T v_plateau_potassium_current__Kp = (T(1.0)/(T(1.0) + exp(((T(7.488) - y[0])/T(5.98)))));
+        const T v_plateau_potassium_current__Kp = (T(1.0)/(T(1.0) + m_exp(((T(7.488) - y[0])/T(5.98)))));
         const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*v_plateau_potassium_current__Kp*(y[0] - (-T(87.8929017138025))));
-        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*log((y[7]/T(1.0)))));
+        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*m_log((y[7]/T(1.0)))));
         const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
-        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
+        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? (((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) + ((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*(((T(2.837)*(m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))) - ((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0)))/(((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))/(T(2.0)*(chb::singularity_offset<T>()*T(1.0))))) : ((T(2.837)*(m_exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0)))/((y[0] + T(77.0))*m_exp((T(0.04)*(y[0] + T(35.0))))))) : T(1.0));
         const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
         const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*v_time_dependent_potassium_current_Xi_gate__Xi*(y[0] - (-T(77.56758438531939))));
-        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
-        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (((T(0.49124)*exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31)))))))/(T(1.0) + exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753))))));
+        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (T(1.02)/(T(1.0) + m_exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215))))));
+        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (((T(0.49124)*m_exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*m_exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31)))))))/(T(1.0) + m_exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753))))));
         const T v_time_independent_potassium_current_K1_gate__K1_infinity = (v_time_independent_potassium_current_K1_gate__alpha_K1/(v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1));
         const T v_time_independent_potassium_current__g_K1__scaled = (T(0.6047)*p[3]);
         const T v_time_independent_potassium_current__i_K1 = (v_time_independent_potassium_current__g_K1__scaled*v_time_independent_potassium_current_K1_gate__K1_infinity*(y[0] - (-T(87.8929017138025))));

@@ -41,6 +41,7 @@ namespace {
 // Largest slab (in nodes) the static scratch serves.
 constexpr int kNoAllocMaxNodes = 32768;
 constexpr int kNoAllocMaxBlocks = 256;
+static_assert(kNoAllocMaxBlocks <= kMaxGridBlocks, "grid larger than the reduction supports");
 
 // Layout of the scratch array, in bytes.  x, z and B r are read through the
 // stencil, so each has a zero halo of up to kNoAllocMaxNodes entries per side.
