@@ -319,7 +319,7 @@ int alloc_vectors(cg_ctx* c) {
         CG_TRY(dalloc(c, &c->d_r32, n * sizeof(float)));
         CG_TRY(dalloc(c, &c->d_p32, n * sizeof(float)));
         CG_TRY(dalloc(c, &c->d_q32, n * sizeof(float)));
-        CG_TRY(dalloc(c, &c->d_e32, n * sizeof(float)));
+        CG_TRY(dalloc_haloed(c, &c->d_e32, n));
     }
     CG_TRY(dalloc(c, &c->d_act, n * sizeof(double)));
     CG_TRY(dalloc(c, &c->d_gs, sizeof(GridSync)));

@@ -86,7 +86,7 @@ __device__ __forceinline__ void cg_finish(const CgArgs& a, long long step, int i
 }
 
 template <bool SLAB, int NOFF>
-__global__ void __launch_bounds__(512) cg_fp64_kernel(CgArgs a) {
+__global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
     __shared__ SlabShared<double> sh;
     __shared__ int soff[kMaxOffsets];
     __shared__ double red[32 * 4];
