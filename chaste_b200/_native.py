@@ -93,6 +93,12 @@ SIGNATURES = {
     "cg_restore": (C.c_int, [_vp, _vp, C.c_size_t]),
     "cg_destroy": (C.c_int, [_vp]),
     "cg_status_string": (C.c_char_p, [C.c_int]),
+    "cg_batch_create": (C.c_int, [C.c_int, C.c_int, _ip, _dp, C.POINTER(Stimulus), C.c_double, C.c_double,
+                                  C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "cg_batch_autotune": (C.c_int, [_vp, C.c_int, _ip]),
+    "cg_batch_run": (C.c_int, [_vp, _dp]),
+    "cg_batch_results": (C.c_int, [_vp, _dp, _dp, _ip, _ip, C.POINTER(C.c_float), _dp, _dp]),
+    "cg_batch_destroy": (C.c_int, [_vp]),
     "cg_slab_solve_noalloc": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, _dp, _vp, _vp, _vp, _ip]),
 }
@@ -255,6 +261,56 @@ class Tissue:
     def close(self):
         if getattr(self, "h", None):
             lib().cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+class CellBatch:
+    """A population of single cells run in FP64 and FP32 side by side (cg_batch)."""
+
+    def __init__(self, model, beats, params=None, stim=None, dt=0.01, beat_length=1000.0, max_aps=None, device=0):
+        beats = np.ascontiguousarray(beats, dtype=np.int32)
+        self.n = beats.size
+        self.model = model
+        self.n_states = num_states(model)
+        self.max_beats = max(1, int(beats.max()))
+        self.max_aps = int(max_aps or self.max_beats + 1)
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        st = stim if stim is not None else stimulus(STIM_REGULAR, -52.0, 1.0, 50.0, 1000.0)
+        h = C.c_void_p()
+        check(lib().cg_batch_create(model, self.n, iptr(beats), dptr(p), C.byref(st), dt, beat_length,
+                                    self.max_aps, device, C.byref(h)), "cg_batch_create")
+        self.h = h
+
+    def autotune(self, steps=2000):
+        tpb = C.c_int()
+        check(lib().cg_batch_autotune(self.h, steps, C.byref(tpb)), "cg_batch_autotune")
+        return tpb.value
+
+    def run(self):
+        ms = C.c_double()
+        check(lib().cg_batch_run(self.h, C.byref(ms)), "cg_batch_run")
+        return ms.value
+
+    def results(self):
+        n, ma, mb, S = self.n, self.max_aps, self.max_beats, self.n_states
+        a64, a32 = np.zeros((n, ma)), np.zeros((n, ma))
+        k64, k32 = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        dv = np.zeros((n, mb), np.float32)
+        s64, s32 = np.zeros((n, S)), np.zeros((n, S))
+        check(lib().cg_batch_results(self.h, dptr(a64), dptr(a32), iptr(k64), iptr(k32),
+                                     dv.ctypes.data_as(C.POINTER(C.c_float)), dptr(s64), dptr(s32)),
+              "cg_batch_results")
+        return dict(apd64=a64, apd32=a32, n_ap64=k64, n_ap32=k32, max_dv=dv, states64=s64, states32=s32)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cg_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

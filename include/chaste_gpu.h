@@ -160,6 +160,30 @@ int cg_restore(cg_ctx* ctx, const void* host_buffer, size_t bytes);
 int cg_destroy(cg_ctx* ctx);
 const char* cg_status_string(int status);
 
+/* ------------------------------------------------- single-cell populations --
+ * Many independent cells, each run for its own number of beats, integrated by
+ * Rush-Larsen (AbstractRushLarsenCardiacCell::Compute,
+ * heart/src/odes/AbstractRushLarsenCardiacCell.cpp:57-104) in FP64 and in FP32
+ * within one launch per beat, with APD90 of every action potential measured as
+ * CellProperties::CalculateActionPotentialDurations does
+ * (heart/src/postprocessing/CellProperties.cpp:55-312, threshold -30 mV).
+ * params: n_cells x n_params scale factors (or NULL for ones); stim: the
+ * stimulus every cell receives (uA/uF; e.g. RegularStimulus(-52, 1, 1000, start)). */
+typedef struct cg_batch cg_batch;
+int cg_batch_create(int model, int n_cells, const int* beats, const double* params, const cg_stimulus* stim,
+                    double dt, double beat_length, int max_aps, int device, cg_batch** out);
+/* Times each candidate block size on `steps` steps and keeps the fastest;
+ * the population is reset to its initial state afterwards. */
+int cg_batch_autotune(cg_batch* b, int steps, int* threads_per_block);
+/* Runs every beat (one CUDA-graph replay per beat); ms = device time. */
+int cg_batch_run(cg_batch* b, double* ms);
+/* apd64/apd32: n_cells x max_aps (-1 where no AP), n_ap: APs completed per cell,
+ * max_dv: n_cells x max_beats largest |V32 - V64| per beat (0.1 ms samples),
+ * states: n_cells x n_states final states.  Any pointer may be NULL. */
+int cg_batch_results(cg_batch* b, double* apd64, double* apd32, int* n_ap64, int* n_ap32, float* max_dv,
+                     double* states64, double* states32);
+int cg_batch_destroy(cg_batch* b);
+
 /* Allocation-free diffusion solve of one PDE step on a regular slab.
  *
  * No counterpart in the reference: Chaste always owns its PETSc vectors.  This

@@ -44,6 +44,13 @@ out = {
         "states": read_dat("heart/test/data/ionicmodels/TenTusscherValidData.dat"),
         "iionic_at_end": -0.1843, "iionic_initial": 0.0012, "iionic_tolerance": 1e-3,
     },
+    "cellprops_lr91_regular": {
+        "source": "heart/test/postprocessing/TestCellProperties.hpp:195-245",
+        "stimulus": {"kind": "regular", "magnitude": -80.0, "duration": 0.5, "period": 1000.0, "start": 100.0},
+        "dt": 0.01, "end": 3450.0, "n_aps": 4,
+        "last_complete_apd90": 362.0155, "last_peak": 43.1665, "last_resting": -84.4395,
+        "tolerance_apd": 0.01, "tolerance_v": 1e-4,
+    },
     "tissue": [
         {"name": "TestMonodomainProblem1D", "dim": 1, "h": 0.01, "size": [0.1, 0, 0],
          "sigma": 0.0005, "am": 1.0, "cm": 1.0, "stim": -600.0, "stim_duration": 0.5,

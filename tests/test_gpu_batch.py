@@ -1,0 +1,53 @@
+"""Batched single-cell populations (cg_batch_*) against the oracle's single-cell Compute."""
+import numpy as np
+import pytest
+
+from tests import cellprops
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def N(native):
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return native
+
+
+def population(n, seed=20261203, max_beats=3):
+    rng = np.random.default_rng(seed)
+    params = np.ones((n, 9))
+    params[:, :6] = np.exp(rng.normal(0.0, 0.2, size=(n, 6)))   # g_Na, g_CaL, g_Kr, g_Ks, g_K1, g_to
+    beats = rng.integers(1, max_beats + 1, size=n).astype(np.int32)
+    return params, beats
+
+
+def test_population_matches_oracle_cells(N, oracle):
+    O = oracle
+    n = 64
+    params, beats = population(n)
+    beats[:2] = 2
+    b = N.CellBatch(N.MODEL_TT06, beats, params)
+    tpb = b.autotune(steps=500)
+    assert tpb in (32, 64, 128, 256)
+    b.run()
+    r = b.results()
+    stim = O.regular(-52.0, 1.0, 1000.0, 50.0)
+    for cell in (0, 1):
+        y = O.initial_states(O.TT06)
+        tr, y = O.cell_compute(O.TT06, O.RL, y, 0.0, 1000.0 * beats[cell], 0.01, 0.0, stim, params=params[cell])
+        t = np.arange(tr.shape[0]) * 0.01
+        ref = cellprops.apds(t, tr[:, 0], 90.0)
+        got = r["apd64"][cell, : r["n_ap64"][cell]]
+        assert len(ref) == len(got) == beats[cell]
+        assert np.max(np.abs(np.array(ref) - got)) <= 1e-6
+        assert np.max(np.abs(r["states64"][cell] - y) / np.maximum(np.abs(y), 1e-3)) <= 1e-6
+    # FP32 against FP64: every AP found, APD90 within 1 ms, finite per-beat Vm error
+    assert np.array_equal(r["n_ap64"], r["n_ap32"])
+    for cell in range(n):
+        k = r["n_ap64"][cell]
+        assert np.max(np.abs(r["apd64"][cell, :k] - r["apd32"][cell, :k])) <= 1.0
+    dv = r["max_dv"][np.arange(n)[:, None], np.arange(b.max_beats)[None, :]]
+    assert np.all(np.isfinite(dv))

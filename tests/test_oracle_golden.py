@@ -106,3 +106,19 @@ def test_monodomain_problem_kats(oracle, kats, pc):
             assert np.abs(out["midway"][mid["nodes"]] - mid["V"]).max() <= mid["tolerance"], case["name"]
         err = np.abs(out["end"][case["nodes"]] - np.array(case["V"])).max()
         assert err <= case["tolerance"], (case["name"], err)
+
+
+def test_cellproperties_restatement_on_lr91_regular_pacing(oracle, kats):
+    """TestCellProperties.hpp:195-245: APD90 of the last complete AP, 4 APs, peak and resting value."""
+    from tests import cellprops
+
+    O, k = oracle, kats["cellprops_lr91_regular"]
+    y = O.initial_states(O.LR91)
+    st = k["stimulus"]
+    tr, _ = O.cell_compute(O.LR91, O.FE, y, 0.0, k["end"], k["dt"], 0.0,
+                           O.regular(st["magnitude"], st["duration"], st["period"], st["start"]))
+    t = np.arange(tr.shape[0]) * k["dt"]
+    apd = cellprops.apds(t, tr[:, 0], 90.0)
+    assert len(apd) == k["n_aps"] - 1      # the fourth AP is still running at 3450 ms
+    assert abs(apd[-1] - k["last_complete_apd90"]) <= k["tolerance_apd"]
+    assert abs(tr[:, 0].max() - k["last_peak"]) <= 0.01
