@@ -644,11 +644,89 @@ class ModelEmitter:
             else:
                 A(f"        return {pr(tot)};")
         A("    }")
+        # ---- reverse-mode products (adjoint of one forward-Euler step and of GetIIonic)
+        lines.extend(self._emit_vjp("vjp_rhs", [(self.odes[s_], f"w[{i}]") for i, s_ in enumerate(self.states)],
+                                    "w: weights of dy[0..S-1]"))
+        tot = sp.Add(*self.currents, evaluate=False)
+        scale = None if not self.current_per_cap else self.cm_arg
+        if scale is None and f_area is not None and abs(f_area - 1) > 1e-15:
+            tot = sp.Mul(sp.Float(f_area, 17), tot, evaluate=False)
+        elif scale is not None:
+            tot = sp.Mul(tot, scale, evaluate=False)
+        lines.extend(self._emit_vjp("vjp_iionic", [(tot, "w[0]")], "w[0]: weight of iionic", stim_zero=True))
         A("};")
         A("")
         A("}  // namespace chb")
         return "\n".join(lines) + "\n"
 
+
+def _sym_diff(e, x):
+    """d e / d x on an evaluated copy of a structure-preserving expression."""
+    ev = sp.sympify(str(e), locals={str(s): s for s in _free(e)})
+    return sp.diff(ev, x)
+
+
+def _vjp_body(self, outputs, pr, stim_zero=False):
+    """Statements for: forward recompute, then adjoints a_v of every symbol."""
+    needed = self._needed([o for o, _ in outputs])
+    body = []
+    for s_ in needed:
+        body.append(f"        const T {self.cname(s_)} = {pr(self._fold_expr(self.live[s_]))};")
+    adj = {}
+
+    def aname(s_):
+        if s_ not in adj:
+            adj[s_] = "a_" + self.cname(s_).replace("[", "_").replace("]", "").replace(".", "_")
+            body.append(f"        T {adj[s_]} = T(0.0);")
+        return adj[s_]
+
+    targets = set(self.states) | set(self.psyms)
+    acc = []
+    for expr, w in outputs:
+        e = self._fold_expr(expr)
+        for x in sorted(_free(e), key=str):
+            if x in targets or x in self.live:
+                d = _sym_diff(e, x)
+                if d != 0:
+                    acc.append((aname(x), f"{w}*({pr(d)})"))
+    body.extend(f"        {a} += {t};" for a, t in acc)
+    for s_ in reversed(needed):
+        if s_ not in adj:
+            continue
+        e = self._fold_expr(self.live[s_])
+        for x in sorted(_free(e), key=str):
+            if x in targets or x in self.live:
+                d = _sym_diff(e, x)
+                if d != 0:
+                    body.append(f"        {aname(x)} += {adj[s_]}*({pr(d)});")
+    return body, adj
+
+
+def _emit_vjp(self, fname, outputs, wdoc, stim_zero=False):
+    pr = Printer(self._names())
+    L = []
+    L.append("")
+    L.append(f"    // Reverse-mode product for {fname[4:]}: gy[j] += sum_i w_i d(out_i)/d(y_j),")
+    L.append(f"    // gp[k] += sum_i w_i d(out_i)/d(p_k)  ({wdoc}; y[0] is the voltage).")
+    L.append("    template <typename T>")
+    L.append(f"    CHB_HD static void {fname}(const T* __restrict__ y, T stim, T cm, const T* __restrict__ p,")
+    L.append("                                const T* __restrict__ w, T* __restrict__ gy, T* __restrict__ gp) {")
+    L.append("        (void)stim; (void)cm; (void)p; (void)w; (void)gy; (void)gp;")
+    if stim_zero:
+        L.append("        stim = T(0.0);")
+    body, adj = _vjp_body(self, outputs, pr, stim_zero)
+    L.extend(body)
+    for i, st in enumerate(self.states):
+        if st in adj:
+            L.append(f"        gy[{i}] += {adj[st]};")
+    for k, ps in enumerate(self.psyms):
+        if ps in adj:
+            L.append(f"        gp[{k}] += {adj[ps]};")
+    L.append("    }")
+    return L
+
+
+ModelEmitter._emit_vjp = _emit_vjp
 
 MODELS = [("LuoRudy1991.cellml", "LuoRudy1991", "lr91"),
           ("TenTusscher2006Epi.cellml", "TenTusscher2006Epi", "tt06")]

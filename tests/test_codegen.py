@@ -86,3 +86,60 @@ int main() {
         assert abs(a - b) <= 1e-3 * max(1.0, abs(b))
         assert abs(c - d) <= 1e-3 * max(1.0, abs(d))
         assert abs(d - e) <= 1e-1 * max(1.0, abs(d))
+
+
+def test_generated_vjps_match_finite_differences(tmp_path):
+    """The emitted reverse-mode products of the RHS and of GetIIonic against central differences."""
+    src = tmp_path / "v.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <cmath>
+#include <initializer_list>
+#include "lr91.h"
+#include "tt06.h"
+template <class M> double check(double vshift) {
+    const int S = M::kNumStates, P = M::kNumParams;
+    double y[S], p[P], w[S], gy[S], gp[P], dy1[S], dy2[S], worst = 0;
+    for (int i = 0; i < S; ++i) { y[i] = M::kInitialStates[i]; w[i] = std::sin(1.0 + i); }
+    y[0] += vshift;
+    for (int k = 0; k < P; ++k) p[k] = 1.0 + 0.1 * k;
+    for (int i = 0; i < S; ++i) gy[i] = 0;
+    for (int k = 0; k < P; ++k) gp[k] = 0;
+    M::template vjp_rhs<double>(y, -10.0, 1.0, p, w, gy, gp);
+    for (int j = 0; j < S + P; ++j) {
+        double* x = j < S ? &y[j] : &p[j - S];
+        const double h = 1e-6 * std::fmax(std::fabs(*x), 1e-3), x0 = *x;
+        *x = x0 + h; M::template rhs<double>(y, -10.0, 1.0, p, dy1);
+        *x = x0 - h; M::template rhs<double>(y, -10.0, 1.0, p, dy2);
+        *x = x0;
+        double fd = 0;
+        for (int i = 0; i < S; ++i) fd += w[i] * (dy1[i] - dy2[i]) / (2 * h);
+        const double g = j < S ? gy[j] : gp[j - S];
+        worst = std::fmax(worst, std::fabs(g - fd) / std::fmax(1.0, std::fabs(fd)));
+    }
+    for (int i = 0; i < S; ++i) gy[i] = 0;
+    for (int k = 0; k < P; ++k) gp[k] = 0;
+    double one = 1.0;
+    M::template vjp_iionic<double>(y, 0.0, 1.0, p, &one, gy, gp);
+    for (int j = 0; j < S + P; ++j) {
+        double* x = j < S ? &y[j] : &p[j - S];
+        const double h = 1e-6 * std::fmax(std::fabs(*x), 1e-3), x0 = *x;
+        *x = x0 + h; const double a = M::template iionic<double>(y, 1.0, p);
+        *x = x0 - h; const double b = M::template iionic<double>(y, 1.0, p);
+        *x = x0;
+        const double fd = (a - b) / (2 * h), g = j < S ? gy[j] : gp[j - S];
+        worst = std::fmax(worst, std::fabs(g - fd) / std::fmax(1.0, std::fabs(fd)));
+    }
+    return worst;
+}
+int main() {
+    double w = 0;
+    for (double dv : {0.0, 30.0, 90.0}) { w = std::fmax(w, check<chb::LuoRudy1991>(dv)); w = std::fmax(w, check<chb::TenTusscher2006Epi>(dv)); }
+    std::printf("%.3e\n", w);
+}
+''')
+    exe = tmp_path / "v"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "chaste_b200", "csrc", "models"),
+                    str(src), "-o", str(exe)], check=True)
+    worst = float(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
+    assert worst <= 1e-5, worst
