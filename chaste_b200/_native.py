@@ -64,6 +64,17 @@ class Stats(C.Structure):
     ]
 
 
+class CableConfig(C.Structure):
+    _fields_ = [
+        ("model", C.c_int), ("n_nodes", C.c_int), ("h", C.c_double), ("conductivity", C.c_double),
+        ("surface_area_to_volume_ratio", C.c_double), ("capacitance", C.c_double),
+        ("time_step", C.c_double), ("n_steps", C.c_int), ("n_regions", C.c_int),
+        ("n_stimulated_nodes", C.c_int), ("stimulus_magnitude", C.c_double),
+        ("stimulus_duration", C.c_double), ("ksp_tolerance", C.c_double), ("max_iterations", C.c_int),
+        ("checkpoint_every", C.c_int),
+    ]
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _vp = C.c_void_p
@@ -99,6 +110,11 @@ SIGNATURES = {
     "cg_batch_run": (C.c_int, [_vp, _dp]),
     "cg_batch_results": (C.c_int, [_vp, _dp, _dp, _ip, _ip, C.POINTER(C.c_float), _dp, _dp]),
     "cg_batch_destroy": (C.c_int, [_vp]),
+    "cg_cable_default_config": (None, [C.POINTER(CableConfig)]),
+    "cg_cable_create": (C.c_int, [C.POINTER(CableConfig), _ip, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "cg_cable_forward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp]),
+    "cg_cable_backward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
+    "cg_cable_destroy": (C.c_int, [_vp]),
     "cg_slab_solve_noalloc": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, _dp, _vp, _vp, _vp, _ip]),
 }

@@ -184,6 +184,61 @@ int cg_batch_results(cg_batch* b, double* apd64, double* apd32, int* n_ap64, int
                      double* states64, double* states32);
 int cg_batch_destroy(cg_batch* b);
 
+/* ------------------------------------------ cables for parameter fitting --
+ * A 1D monodomain cable (P1 elements, forward Euler ODE step equal to the PDE
+ * step, CG + Jacobi with PETSc's stopping test) whose parameters vary over R
+ * contiguous regions, with the loss
+ *     L = mean over steps n and probes k of (V_{n+1}(probe_k) - target[n][k])^2
+ * and its gradient by the discrete adjoint of the operator-split step.  The
+ * forward step is the one cg_step takes (MonodomainSolver.cpp:92-101,
+ * MonodomainAssembler.cpp:43-66, AbstractCardiacTissue::SolveCellSystems with
+ * ComputeExceptVoltage); the adjoint has no counterpart in the reference.
+ *
+ * Parameters of one set: n_regions rows of (n_params cell scale factors,
+ * conductivity scale), so n_regions * (cg_num_params(model) + 1) doubles.
+ * Node i lies in region floor(i R / n_nodes), element e (nodes e, e+1) in
+ * region floor(e R / (n_nodes - 1)), both capped at R - 1.
+ * Device pointers throughout; each call returns once its work on `stream`
+ * (NULL: legacy default stream) has finished. */
+typedef struct {
+    int model;                     /* CG_MODEL_* */
+    int n_nodes;                   /* 2 .. 1024 */
+    double h;                      /* node spacing, cm */
+    double conductivity;           /* mS/cm, before the region scale */
+    double surface_area_to_volume_ratio;
+    double capacitance;
+    double time_step;              /* ms (ODE and PDE) */
+    int n_steps;
+    int n_regions;                 /* 1 .. 8 */
+    int n_stimulated_nodes;        /* nodes 0 .. k-1 */
+    double stimulus_magnitude;     /* uA/cm^3, SimpleStimulus from t = 0 */
+    double stimulus_duration;      /* ms */
+    double ksp_tolerance;          /* relative */
+    int max_iterations;
+    int checkpoint_every;          /* steps between adjoint checkpoints */
+} cg_cable_config;
+
+typedef struct cg_cable cg_cable;
+/* 1000 nodes of h = 0.01 cm, LR91, sigma 1.75, Am 1400, Cm 1, dt 0.01 ms,
+ * 400 ms, 4 regions, -5e5 uA/cm^3 for 0.5 ms on x < 0.02 cm, rtol 1e-8,
+ * checkpoints every 200 steps. */
+void cg_cable_default_config(cg_cable_config* cfg);
+/* probes: n_probes distinct node indices (host). */
+int cg_cable_create(const cg_cable_config* cfg, const int* probes, int n_probes, int device, cg_cable** out);
+/* n_sets parameter sets in one launch (one CTA each).  d_targets (n_steps x
+ * n_probes) and d_loss (n_sets) may both be NULL; d_traces (n_sets x n_steps x
+ * n_probes) may be NULL; d_iterations (n_sets, total CG iterations) may be NULL.
+ * keep_checkpoints: store the states every checkpoint_every steps for
+ * cg_cable_backward (needs d_targets). */
+int cg_cable_forward(cg_cable* c, int n_sets, const double* d_params, const double* d_targets, double* d_loss,
+                     double* d_traces, int* d_iterations, int keep_checkpoints, void* stream);
+/* dL/dparams (n_sets x R x (n_params + 1)) of the sets of the last forward
+ * call made with keep_checkpoints, which must have had the same parameters
+ * and targets. */
+int cg_cable_backward(cg_cable* c, int n_sets, const double* d_params, const double* d_targets, double* d_grad,
+                      void* stream);
+int cg_cable_destroy(cg_cable* c);
+
 /* Allocation-free diffusion solve of one PDE step on a regular slab.
  *
  * No counterpart in the reference: Chaste always owns its PETSc vectors.  This

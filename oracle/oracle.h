@@ -106,6 +106,29 @@ void orc_tissue_get_caches(const orc_tissue* t, double* iion, double* istim);
 int orc_tissue_matrix(const orc_tissue* t, int which /*0 A, 1 M*/, int* rowptr, int* cols, double* vals);
 void orc_set_threads(int n);
 
+/* --------------------------------------------------------------- cable -- */
+/* A 1D cable with the ODE step equal to the PDE step, parameters varying over
+ * R regions (node i in region floor(i R / n), element e in floor(e R / (n-1)),
+ * capped at R-1); params: R rows of (cell scale factors, conductivity scale).
+ * Nodes 0..n_stim-1 get SimpleStimulus(stim_mag, stim_dur, 0). */
+typedef struct {
+    int model;
+    int n_nodes;
+    double h, sigma, am, cm, dt;
+    int n_steps, n_regions, n_stim;
+    double stim_mag, stim_dur, rtol;
+    int max_iterations;
+    int checkpoint_every;   /* adjoint: steps between stored states (0: one segment) */
+} orc_cable_config;
+
+/* Loss L = mean over steps and probes of (V_{n+1}(probe) - target)^2, the probe
+ * traces (n_steps x n_probes) when traces is non-null, and dL/dparams by the
+ * discrete adjoint when grad is non-null (each segment of checkpoint_every
+ * steps recomputed from its checkpoint; n_nodes * n_states times both the
+ * segment length and the checkpoint count must stay <= 4e7).  Returns 0, -1 when CG reached maxit, -4 on bad arguments. */
+int orc_cable_run(const orc_cable_config* c, const double* params, const int* probes, int n_probes,
+                  const double* targets, double* loss, double* traces, double* grad);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,14 @@ class Config(C.Structure):
                 ("mass_lumping", C.c_int), ("max_iterations", C.c_int)]
 
 
+class CableConfig(C.Structure):
+    _fields_ = [("model", C.c_int), ("n_nodes", C.c_int), ("h", C.c_double), ("sigma", C.c_double),
+                ("am", C.c_double), ("cm", C.c_double), ("dt", C.c_double), ("n_steps", C.c_int),
+                ("n_regions", C.c_int), ("n_stim", C.c_int), ("stim_mag", C.c_double),
+                ("stim_dur", C.c_double), ("rtol", C.c_double), ("max_iterations", C.c_int),
+                ("checkpoint_every", C.c_int)]
+
+
 def build():
     subprocess.run(["make", "-s", "-C", HERE, f"OUT={LIB_PATH}"], check=True)
 
@@ -104,6 +112,8 @@ def lib():
         L.orc_tissue_matrix.restype = C.c_int
         L.orc_tissue_matrix.argtypes = [C.c_void_p, C.c_int, ip, ip, dp]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_cable_run.restype = C.c_int
+        L.orc_cable_run.argtypes = [C.POINTER(CableConfig), dp, ip, C.c_int, dp, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -226,3 +236,18 @@ class Tissue:
         if getattr(self, "h", None):
             lib().orc_tissue_destroy(self.h)
             self.h = None
+
+
+def cable_run(cfg: CableConfig, params, probes, targets=None, traces=False, gradient=False):
+    """orc_cable_run: returns dict(loss, traces, grad) (None where not asked)."""
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    probes = np.ascontiguousarray(probes, dtype=np.int32)
+    tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.float64)
+    loss = C.c_double(0.0)
+    tr = np.zeros((cfg.n_steps, probes.size)) if traces else None
+    g = np.zeros_like(params) if gradient else None
+    rc = lib().orc_cable_run(C.byref(cfg), _dp(params), _ip(probes), probes.size, _dp(tg),
+                             C.byref(loss) if tg is not None else None, _dp(tr), _dp(g))
+    if rc != 0:
+        raise RuntimeError(f"orc_cable_run failed with code {rc}")
+    return dict(loss=loss.value if tg is not None else None, traces=tr, grad=g)
