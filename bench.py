@@ -33,7 +33,7 @@ WORKLOADS = {
     "tt06_slab_3d": dict(model=1, method=1, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01,
                          size=(2.0, 0.7, 0.3), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
                          box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8,
-                         name="3D TT06-epi Rush-Larsen slab 2x0.7x0.3 cm h=0.01 (442,371 nodes)"),
+                         name="3D TT06-epi Rush-Larsen slab 2x0.7x0.3 cm h=0.01 (201x71x31 = 442,401 nodes)"),
     # BASELINE config 5 (2.1M nodes), used for profiling at a size beyond L2
     "tt06_slab_3d_large": dict(model=1, method=1, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.0125,
                                size=(2.0, 2.0, 1.0), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
@@ -61,8 +61,13 @@ def ode_bytes_per_node(model, w):
     return 2 * (s - 1) * w + 8 + 1 + 2 * w
 
 
-def cg_bytes(mixed, its, sweeps):
+def cg_bytes(mixed, its, sweeps, pipelined=False):
     """Algorithmic bytes per node of one diffusion solve on the slab operator."""
+    if mixed and pipelined:
+        # residual pass: z32, V, class in; r64 and B r out.  per inner iteration only m = B w is
+        # written and read back through the stencil (the other vectors stay in registers);
+        # per sweep: e written and read, x and r64 read and written, B r written
+        return (4 + 8 + 1 + 8 + 4) + its * (4 + 4) + sweeps * ((4 + 4) + 16 + 16 + 4)
     if not mixed:
         # phase 0: V, z, class in; r out.  per iteration: (r, p_old, cls) -> p_new ; (x, p_new, r, cls) -> (x, r)
         return (8 + 8 + 1 + 8) + its * ((8 + 8 + 1 + 8) + (8 + 8 + 8 + 1 + 16))
@@ -184,8 +189,10 @@ def run_ours(args, rank, world, device):
             a, b = t.step_profiled(1)
             ms_ode += a
             ms_cg += b
+        st = t.stats()
         results[label] = dict(tissue=t, ms_total=ms_total, its=its, sweeps=sweeps, ms_ode=ms_ode / k_prof,
-                              ms_cg=ms_cg / k_prof, clocks=clk.summary(), steps_done=t.stats().steps)
+                              ms_cg=ms_cg / k_prof, clocks=clk.summary(), steps_done=st.steps,
+                              pipelined=st.pipelined_nodes_per_thread, cg_blocks=st.cg_blocks)
     n = results["fp64"]["tissue"].n
     # accuracy of the mixed path against FP64 at the same simulated time
     v64 = results["fp64"]["tissue"].voltage()
@@ -206,7 +213,8 @@ def run_ours(args, rank, world, device):
         sec = r["ms_total"] / 1e3
         out[label] = dict(node_steps_per_s=n * args.steps / sec, ms_per_step=r["ms_total"] / args.steps,
                           mean_cg_iterations=r["its"] / args.steps, ms_ode=r["ms_ode"], ms_cg=r["ms_cg"],
-                          sweeps=r["sweeps"] / args.steps, clocks=r["clocks"])
+                          sweeps=r["sweeps"] / args.steps, clocks=r["clocks"], pipelined=r["pipelined"],
+                          cg_blocks=r["cg_blocks"])
     return dict(n=n, out=out, vm_err=vm_err, head=head, e2e_s=e2e_s, wl=wl)
 
 
@@ -218,7 +226,7 @@ def roofline(res, args):
     mixed = head == "mixed"
     w = 4 if mixed else 8
     b_ode = ode_bytes_per_node(res["wl"]["model"], w) * n
-    b_cg = cg_bytes(mixed, o["mean_cg_iterations"], o["sweeps"] if mixed else 0) * n
+    b_cg = cg_bytes(mixed, o["mean_cg_iterations"], o["sweeps"] if mixed else 0, o.get("pipelined", 0) > 0) * n
     ach_ode = b_ode / (o["ms_ode"] / 1e3) / 1e9
     ach_cg = b_cg / (o["ms_cg"] / 1e3) / 1e9
     dom = "ode" if o["ms_ode"] >= o["ms_cg"] else "cg"

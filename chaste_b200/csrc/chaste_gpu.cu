@@ -62,6 +62,7 @@ struct cg_ctx {
     uint8_t* d_cls8 = nullptr;
     double *d_r = nullptr, *d_zp = nullptr, *d_p = nullptr, *d_q = nullptr;
     float *d_r32 = nullptr, *d_z32 = nullptr, *d_p32 = nullptr, *d_q32 = nullptr, *d_e32 = nullptr;
+    float *d_m32a = nullptr, *d_m32b = nullptr;
     long long halo = 0;           // zero entries on both sides of stencil-read vectors
     int interior_cls = 0;
     double* d_partials = nullptr;
@@ -81,6 +82,7 @@ struct cg_ctx {
     // launch shapes
     int ode_blocks = 0;
     int cg_blocks = 0;
+    int pipe_nodes = 0;   // > 0: mixed slab solve by cg_mixed_pipe_kernel with this many nodes per thread
     int diag_slot = 0;
     // stats
     long long steps = 0;
@@ -303,7 +305,30 @@ CgKernel pick_cg_kernel_t(const cg_ctx* c) {
     }
 }
 
+template <int NOFF>
+CgKernel pick_pipe_kernel(int k) {
+    switch (k) {
+        case 1: return cg_mixed_pipe_kernel<NOFF, 1>;
+        case 2: return cg_mixed_pipe_kernel<NOFF, 2>;
+        case 3: return cg_mixed_pipe_kernel<NOFF, 3>;
+        default: return cg_mixed_pipe_kernel<NOFF, 4>;
+    }
+}
+
+// The pipelined mixed solve, for slabs with an unrolled offset count whose
+// nodes fit in registers (at most 4 per thread of the co-resident grid).
+CgKernel pick_pipe(const cg_ctx* c, int k) {
+    switch (c->stencil.n_offsets) {
+        case 3: return pick_pipe_kernel<3>(k);
+        case 7: return pick_pipe_kernel<7>(k);
+        case 9: return pick_pipe_kernel<9>(k);
+        case 15: return pick_pipe_kernel<15>(k);
+        default: return nullptr;
+    }
+}
+
 CgKernel pick_cg_kernel(const cg_ctx* c) {
+    if (c->pipe_nodes > 0) return pick_pipe(c, c->pipe_nodes);
     return c->mixed() ? pick_cg_kernel_t<true>(c) : pick_cg_kernel_t<false>(c);
 }
 
@@ -320,6 +345,8 @@ int alloc_vectors(cg_ctx* c) {
         CG_TRY(dalloc(c, &c->d_p32, n * sizeof(float)));
         CG_TRY(dalloc(c, &c->d_q32, n * sizeof(float)));
         CG_TRY(dalloc_haloed(c, &c->d_e32, n));
+        CG_TRY(dalloc_haloed(c, &c->d_m32a, n));
+        CG_TRY(dalloc_haloed(c, &c->d_m32b, n));
     }
     CG_TRY(dalloc(c, &c->d_act, n * sizeof(double)));
     CG_TRY(dalloc(c, &c->d_gs, sizeof(GridSync)));
@@ -344,7 +371,17 @@ int alloc_vectors(cg_ctx* c) {
     if (per_sm < 1) return CG_ERR_UNSUPPORTED;
     const long long want = ((long long)n + 511) / 512;
     c->cg_blocks = (int)std::max(1LL, std::min({want, (long long)per_sm * sms, (long long)kMaxGridBlocks}));
-    CG_TRY(dalloc(c, &c->d_partials, (size_t)c->cg_blocks * 4 * sizeof(double)));
+    c->pipe_nodes = 0;
+    if (c->mixed() && c->slab && pick_pipe(c, 1)) {
+        const long long threads = (long long)c->cg_blocks * 512;
+        const long long k = ((long long)n + threads - 1) / threads;
+        int per_sm_pipe = 0;
+        if (k <= 4) {
+            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, pick_pipe(c, (int)k), 512, 0));
+            if ((long long)per_sm_pipe * sms >= c->cg_blocks) c->pipe_nodes = (int)k;
+        }
+    }
+    CG_TRY(dalloc(c, &c->d_partials, (size_t)2 * c->cg_blocks * kPartialStride * sizeof(double)));
     c->ode_blocks = (int)std::max(1LL, std::min(((long long)n + 255) / 256, (long long)sms * 16));
     CG_CUDA(cudaStreamSynchronize(s));
     return CG_OK;
@@ -619,6 +656,8 @@ CgArgs make_cg_args(cg_ctx* c) {
     a.p32 = c->d_p32;
     a.q32 = c->d_q32;
     a.e32 = c->d_e32;
+    a.m32a = c->d_m32a;
+    a.m32b = c->d_m32b;
     a.partials = c->d_partials;
     a.gs = c->d_gs;
     a.status = c->d_status;
@@ -897,6 +936,8 @@ int cg_get_stats(cg_ctx* c, cg_stats* s) {
     s->max_cg_iterations = c->max_iters;
     s->operator_kind = c->slab ? 1 : 0;
     s->ms_last_call = c->ms_last;
+    s->pipelined_nodes_per_thread = c->pipe_nodes;
+    s->cg_blocks = c->cg_blocks;
     if (c->have_cells && c->steps > 0) {
         CG_CUDA(cudaSetDevice(c->device));
         CG_CUDA(cudaMemcpy(&s->last_cg_iterations, c->d_ring + ((c->steps - 1) % kRing), sizeof(int),

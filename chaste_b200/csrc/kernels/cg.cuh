@@ -34,7 +34,9 @@ struct CgArgs {
     float* z32;                 // (haloed)
     float* p32;
     float* q32;
-    float* e32;
+    float* e32;                 // (haloed)
+    float* m32a;                // pipelined inner solve: alternating haloed buffers of B w
+    float* m32b;
     double* partials;           // gridDim.x * 4
     GridSync* gs;
     int* status;
@@ -86,7 +88,7 @@ __device__ __forceinline__ void cg_finish(const CgArgs& a, long long step, int i
 }
 
 template <bool SLAB, int NOFF>
-__global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
+__device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& round) {
     __shared__ SlabShared<double> sh;
     __shared__ int soff[kMaxOffsets];
     __shared__ double red[32 * 4];
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
             zp[i] = zz;
         }
         block_reduce<4>(v, red, red_out);
-        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status)) return;
+        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status, round)) return;
     }
     double rnorm0 = sqrt(res[1]);
     double dp = sqrt(res[2]);
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
         }
         double o2[2];
         block_reduce<2>(v, red, red_out);
-        if (!grid_reduce<2>(a.gs, a.partials, red_out, o2, a.status)) return;
+        if (!grid_reduce<2>(a.gs, a.partials, red_out, o2, a.status, round)) return;
         dp = sqrt(o2[0]);
         beta = o2[1];
         rnorm0 = dp;
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
                 v[0] += pi * qi;
             }
             block_reduce<1>(v, red, red_out);
-            if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status)) return;
+            if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
         }
         const double dpi = res[0];
         if (!(dpi > 0.0)) return cg_finish(a, step, it + 1, isfinite(dpi) ? kStatusCgDiverged : kStatusNaN);
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
                 v[1] += zz * rr;
             }
             block_reduce<2>(v, red, red_out);
-            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status)) return;
+            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
         }
         dp = sqrt(res[0]);
         if (!isfinite(dp)) return cg_finish(a, step, it + 1, kStatusNaN);
@@ -204,6 +206,13 @@ __global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
         beta = res[1];
     }
     cg_finish(a, step, it, kStatusCgMaxIt);
+}
+
+template <bool SLAB, int NOFF>
+__global__ void __launch_bounds__(512, 2) cg_fp64_kernel(CgArgs a) {
+    unsigned round = 0;
+    cg_fp64_kernel_body<SLAB, NOFF>(a, round);
+    grid_exit(a.gs);
 }
 
 }  // namespace chb

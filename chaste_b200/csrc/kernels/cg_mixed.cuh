@@ -36,7 +36,7 @@ __device__ __forceinline__ float apply_row32(const CgArgs& a, const SlabShared<f
 }
 
 template <bool SLAB, int NOFF>
-__global__ void __launch_bounds__(512, 2) cg_mixed_kernel(CgArgs a) {
+__device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& round) {
     __shared__ SlabShared<double> sh;
     __shared__ SlabShared<float> s32;
     __shared__ int soff[kMaxOffsets];
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(512, 2) cg_mixed_kernel(CgArgs a) {
             v[3] += (double)rf * (double)zf;
         }
         block_reduce<4>(v, red, red_out);
-        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status)) return;
+        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status, round)) return;
     }
     rnorm0 = sqrt(res[1]);
     dp = sqrt(res[2]);
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(512, 2) cg_mixed_kernel(CgArgs a) {
                     v[0] += (double)pi * (double)qi;
                 }
                 block_reduce<1>(v, red, red_out);
-                if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status)) return;
+                if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
             }
             const double dpi = res[0];
             if (!(dpi > 0.0)) break;   // the FP64 residual update decides what happens next
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(512, 2) cg_mixed_kernel(CgArgs a) {
                     v[1] += (double)zz * (double)rr;
                 }
                 block_reduce<2>(v, red, red_out);
-                if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status)) return;
+                if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
             }
             const double dp_in = sqrt(res[0]);
             betaold = beta;
@@ -177,13 +177,222 @@ __global__ void __launch_bounds__(512, 2) cg_mixed_kernel(CgArgs a) {
                 v[1] += (double)rf * (double)zf;
             }
             block_reduce<2>(v, red, red_out);
-            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status)) return;
+            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
         }
         dp = sqrt(res[0]);
         rz = res[1];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.refine_out = sweeps;
     cg_finish(a, step, total_its, 0);
+}
+
+template <bool SLAB, int NOFF>
+__global__ void __launch_bounds__(512, 2) cg_mixed_kernel(CgArgs a) {
+    unsigned round = 0;
+    cg_mixed_kernel_body<SLAB, NOFF>(a, round);
+    grid_exit(a.gs);
+}
+
+// ---------------------------------------------------------------------------
+// Slab-stencil variant with a pipelined inner solve (Ghysels & Vanroose,
+// "Hiding global synchronization latency in the preconditioned Conjugate
+// Gradient algorithm", Parallel Computing 40, 2014): the two inner products of
+// an iteration, (r,u) and (w,u), are reduced together, and the vector the next
+// operator application needs, m = B w, is published before that one grid-wide
+// reduction, which therefore doubles as the halo barrier.  m alternates
+// between two haloed buffers, so a block may publish iteration i+1 while its
+// neighbours still read iteration i.  Every thread keeps the inner vectors of
+// its KMAX nodes (t0 + k * stride) in registers; only m and, at the end of a
+// sweep, the correction e go through memory.  One grid-wide synchronisation
+// per inner iteration instead of two.
+//
+// The FP64 residual passes and the outer stopping test are those of
+// cg_mixed_kernel; the inner iteration stops on the preconditioned norm
+// sqrt((r, B r)) reaching `target` of its start value.
+// Stencil row over a vector that other blocks of this launch have written: the
+// loads go to L2 (ld.global.cg), never to a possibly stale L1 or read-only line.
+template <int NOFF, typename Acc, typename T, typename X>
+__device__ __forceinline__ Acc slab_row_l2(const T* coef, const int* off, int i, const X* x) {
+    Acc acc = Acc(0);
+#pragma unroll
+    for (int o = 0; o < NOFF; ++o) acc += (Acc)coef[o] * (Acc)__ldcg(x + i + off[o]);
+    return acc;
+}
+
+template <int NOFF>
+__device__ __forceinline__ float apply_a32_l2(const CgArgs& a, const SlabShared<float>& s32, int c, int i,
+                                              const float* x) {
+    if (c == a.slab.interior) return slab_row_l2<NOFF, float>(a.slab.ia32, a.slab.off, i, x);
+    return slab_row_l2<NOFF, float>(&s32.a[c * NOFF], a.slab.off, i, x);
+}
+
+template <int NOFF>
+__device__ __forceinline__ double apply_a64_l2(const CgArgs& a, const SlabShared<double>& sh, int c, int i,
+                                               const float* x) {
+    if (c == a.slab.interior) return slab_row_l2<NOFF, double>(a.slab.ia, a.slab.off, i, x);
+    return slab_row_l2<NOFF, double>(&sh.a[c * NOFF], a.slab.off, i, x);
+}
+
+template <int NOFF, int KMAX>
+__device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsigned& round) {
+    __shared__ SlabShared<double> sh;
+    __shared__ SlabShared<float> s32;
+    __shared__ double red[32 * 4];
+    __shared__ double red_out[4];
+    slab_load_shared<double>(a.slab, sh, a.diag_slot);
+    slab_load_shared<float>(a.slab, s32, a.diag_slot);
+    if (*(volatile int*)a.status & ~kStatusStateRange) return;
+    const long long step = *a.step;
+    const int n = a.n;
+    const int stride = gridDim.x * blockDim.x;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    double* __restrict__ x = a.x;
+    double* __restrict__ r64 = a.r;
+    float* z32 = a.z32;
+    float* e32 = a.e32;
+    int node[KMAX], cls[KMAX];
+    float dinv[KMAX];
+    bool on[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        node[k] = t0 + k * stride;
+        on[k] = node[k] < n;
+        cls[k] = on[k] ? (int)a.cls8[node[k]] : 0;
+        dinv[k] = on[k] ? (a.pc ? s32.dinv[cls[k]] : 1.0f) : 0.0f;
+    }
+    float r[KMAX], u[KMAX], w[KMAX], m[KMAX], zq[KMAX], q[KMAX], sv[KMAX], p[KMAX], e[KMAX];
+    double res[4];
+
+    // ---- FP64 residual r = M z - A x; its FP32 copy r and u = B r (published in z32)
+    {
+        double v[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            r[k] = u[k] = 0.0f;
+            if (!on[k]) continue;
+            const int i = node[k], c = cls[k];
+            const double b = apply_row<true, NOFF, true>(a, sh, nullptr, c, i, a.zrhs32);
+            const double av = apply_row<true, NOFF, false>(a, sh, nullptr, c, i, x);
+            const double rr = b - av;
+            const double d = dinv_of<true>(a, sh, c, i);
+            const double wb = d * b, zz = d * rr;
+            v[0] += fabs(b);
+            v[1] += wb * wb;
+            v[2] += zz * zz;
+            r64[i] = rr;
+            r[k] = (float)rr;
+            u[k] = dinv[k] * r[k];
+            z32[i] = u[k];
+        }
+        block_reduce<4>(v, red, red_out);
+        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status, round)) return;
+    }
+    double rnorm0 = sqrt(res[1]);
+    double dp = sqrt(res[2]);
+    if (rnorm0 == 0.0) rnorm0 = dp;
+    const double ttol = fmax(a.rtol * rnorm0, a.abstol);
+    int total_its = 0, sweeps = 0;
+
+    for (int sweep = 0;; ++sweep) {
+        if (!isfinite(dp)) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *a.refine_out = sweeps;
+            return cg_finish(a, step, total_its, kStatusNaN);
+        }
+        if (dp <= ttol) break;
+        if (dp >= a.dtol * rnorm0 || sweep >= a.max_refine) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *a.refine_out = sweeps;
+            return cg_finish(a, step, total_its, dp >= a.dtol * rnorm0 ? kStatusCgDiverged : kStatusCgMaxIt);
+        }
+        sweeps++;
+        const double target = fmin(0.5, fmax(3e-5, 0.1 * ttol / dp));
+        // w = A u (u was published before the last grid-wide reduction)
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            w[k] = on[k] ? apply_a32_l2<NOFF>(a, s32, cls[k], node[k], z32) : 0.0f;
+            zq[k] = q[k] = sv[k] = p[k] = e[k] = 0.0f;
+        }
+        double gamma_old = 1.0, alpha_old = 1.0, g0 = 0.0;
+        int it = 0;
+        for (;; ++it) {
+            float* mb = (it & 1) ? a.m32b : a.m32a;
+            double v[2] = {0, 0};
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) {
+                v[0] += (double)r[k] * (double)u[k];
+                v[1] += (double)w[k] * (double)u[k];
+                m[k] = dinv[k] * w[k];
+                if (on[k]) mb[node[k]] = m[k];
+            }
+            block_reduce<2>(v, red, red_out);
+            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
+            const double gamma = res[0], delta = res[1];
+            if (it == 0) g0 = gamma;
+            if (!(gamma > 0.0) || !(gamma > target * target * g0) || it >= a.maxit) break;
+            const double beta = it == 0 ? 0.0 : gamma / gamma_old;
+            const double denom = it == 0 ? delta : delta - beta * gamma / alpha_old;
+            if (!(denom > 0.0)) break;   // breakdown: the FP64 residual update decides what follows
+            const double alpha = gamma / denom;
+            const float af = (float)alpha, bf = (float)beta;
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) {
+                const float nk = on[k] ? apply_a32_l2<NOFF>(a, s32, cls[k], node[k], mb) : 0.0f;
+                zq[k] = nk + bf * zq[k];
+                q[k] = m[k] + bf * q[k];
+                sv[k] = w[k] + bf * sv[k];
+                p[k] = u[k] + bf * p[k];
+                e[k] += af * p[k];
+                r[k] -= af * sv[k];
+                u[k] -= af * q[k];
+                w[k] -= af * zq[k];
+            }
+            gamma_old = gamma;
+            alpha_old = alpha;
+        }
+        total_its += it;
+        if (it == 0) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *a.refine_out = sweeps;
+            return cg_finish(a, step, total_its, kStatusCgDiverged);
+        }
+        // ---- publish e, then x += e and r -= A e in FP64 (e of the neighbours complete)
+        {
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k)
+                if (on[k]) e32[node[k]] = e[k];
+            double v[1] = {0};
+            block_reduce<1>(v, red, red_out);
+            if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
+        }
+        {
+            double v[1] = {0};
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) {
+                r[k] = u[k] = 0.0f;
+                if (!on[k]) continue;
+                const int i = node[k], c = cls[k];
+                const double ae = apply_a64_l2<NOFF>(a, sh, c, i, e32);
+                x[i] += (double)e[k];
+                const double rr = r64[i] - ae;
+                r64[i] = rr;
+                const double zz = dinv_of<true>(a, sh, c, i) * rr;
+                v[0] += zz * zz;
+                r[k] = (float)rr;
+                u[k] = dinv[k] * r[k];
+                z32[i] = u[k];
+            }
+            block_reduce<1>(v, red, red_out);
+            if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
+        }
+        dp = sqrt(res[0]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.refine_out = sweeps;
+    cg_finish(a, step, total_its, 0);
+}
+
+template <int NOFF, int KMAX>
+__global__ void __launch_bounds__(512, 2) cg_mixed_pipe_kernel(CgArgs a) {
+    unsigned round = 0;
+    cg_mixed_pipe_kernel_body<NOFF, KMAX>(a, round);
+    grid_exit(a.gs);
 }
 
 }  // namespace chb

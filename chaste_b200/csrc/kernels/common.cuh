@@ -61,17 +61,38 @@ struct DevTimeStepper {
 
 // ------------------------------------------------------------------------
 // Grid-wide reduction + barrier for persistent kernels launched cooperatively
-// (all blocks co-resident).  Every wait is bounded: on timeout the block sets
+// (all blocks co-resident).
+//
+// Arrival is a monotonic counter: at its k-th reduction (k = 0, 1, ...) a block
+// writes its partial sums into buffer k % 2, adds 1 to `count` (release) and
+// waits until `count` reaches (k + 1) * gridDim (acquire).  Every block then
+// sums all partials itself, lane l taking blocks l, l+32, ... and a fixed
+// shuffle tree finishing, so all blocks obtain bitwise the same totals with
+// no broadcast round trip.  Two buffers suffice: a block can write round k+1
+// only after every block has arrived at round k, i.e. has finished reading
+// round k-1.  The counter is returned to zero by the last block to leave the
+// kernel (grid_exit), so each launch starts from zero.
+//
+// Every wait is bounded (about 2 s of %globaltimer): on timeout the block sets
 // kStatusBarrierTimeout and returns false, and later waits see the flag and
 // return at once, so the kernel always terminates.
 struct GridSync {
     unsigned int count;
-    unsigned int gen;
+    unsigned int gen;     // unused (layout kept)
+    unsigned int exit;
+    unsigned int pad;
     double result[8];
 };
 
-constexpr long long kBarrierSpinLimit = 20000000;   // x ~100 ns sleep ~ 2 s
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
 constexpr int kMaxGridBlocks = 512;                  // largest grid a persistent kernel is launched with
+constexpr int kPartialStride = 4;                    // doubles per block and buffer (NV <= 4)
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -100,79 +121,88 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double* smem /* 32
     __syncthreads();
 }
 
-// All blocks contribute NV partial sums; out[] receives the grid totals,
-// identical in every block because the last block to arrive sums the partials
-// in a fixed order (lane l takes blocks l, l+32, ..., then a fixed shuffle tree).
+// All blocks contribute NV partial sums (partials: 2 x gridDim x kPartialStride
+// doubles); out[] receives the grid totals, identical in every block.  `round`
+// counts this block's reductions in the launch (start at 0; same sequence in
+// every block).  The partials are read by the first kReduceWarps warps, thread
+// t taking blocks t, t + 32 kReduceWarps, ... (at most 4 loads, issued together),
+// then each warp's shuffle tree and the warps in order; the order is fixed, so
+// every block gets bitwise the same sums.  Needs blockDim >= 32 * kReduceWarps.
+constexpr int kReduceWarps = 4;
+
 template <int NV>
-__device__ bool grid_reduce(GridSync* gs, double* partials, const double* block_vals,
-                            double* out, int* status) {
-    const int lane = threadIdx.x & 31;
+__device__ bool grid_reduce(GridSync* gs, double* partials, const double* block_vals, double* out, int* status,
+                            unsigned& round) {
+    static_assert(NV >= 1 && NV <= kPartialStride, "at most four sums per reduction");
+    constexpr int kLoads = kMaxGridBlocks / (32 * kReduceWarps);
     __shared__ int s_ok;
-    __shared__ double s_res[8];
-    if (threadIdx.x < 32) {
-        unsigned my_gen = 0, ticket = 0;
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) partials[blockIdx.x * NV + k] = block_vals[k];
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(gs->gen);
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count);
-            my_gen = gen.load(cuda::memory_order_acquire);
-            ticket = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-        }
-        ticket = __shfl_sync(0xffffffffu, ticket, 0);
-        my_gen = __shfl_sync(0xffffffffu, my_gen, 0);
+    __shared__ double s_part[kReduceWarps][kPartialStride];
+    double* buf = partials + (size_t)(round & 1u) * gridDim.x * kPartialStride;
+    const unsigned target = (round + 1u) * gridDim.x;
+    round++;
+    if (threadIdx.x == 0) {
         int ok = 1;
-        if (ticket == gridDim.x - 1) {
-            __threadfence();
-            __syncwarp();
-            // all loads of a lane are issued before any is used (grids of at most
-            // kMaxGridBlocks blocks), so the reduction costs one L2 round trip
 #pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                double vals[kMaxGridBlocks / 32];
-#pragma unroll
-                for (int m = 0; m < kMaxGridBlocks / 32; ++m) {
-                    const unsigned b = lane + 32u * m;
-                    vals[m] = b < gridDim.x ? __ldcg(&partials[b * NV + k]) : 0.0;
-                }
-                double s = 0.0;
-#pragma unroll
-                for (int m = 0; m < kMaxGridBlocks / 32; ++m) s += vals[m];
-                s = warp_sum(s);
-                if (lane == 0) gs->result[k] = s;
-            }
-            __syncwarp();
-            if (lane == 0) {
-                cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(gs->gen);
-                cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count);
-                cnt.store(0u, cuda::memory_order_relaxed);
-                gen.fetch_add(1u, cuda::memory_order_release);
-            }
-        } else if (lane == 0) {
-            cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(gs->gen);
-            long long spins = 0;
-            while (gen.load(cuda::memory_order_acquire) == my_gen) {
-                if (++spins > kBarrierSpinLimit || (*(volatile int*)status & kStatusBarrierTimeout)) {
+        for (int k = 0; k < NV; ++k) buf[blockIdx.x * kPartialStride + k] = block_vals[k];
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count);
+        cnt.fetch_add(1u, cuda::memory_order_release);
+        if (cnt.load(cuda::memory_order_acquire) < target) {
+            const unsigned long long t0 = global_ns();
+            while (cnt.load(cuda::memory_order_acquire) < target) {
+                if ((*(volatile int*)status & kStatusBarrierTimeout) || global_ns() - t0 > kBarrierTimeoutNs) {
                     atomicOr(status, kStatusBarrierTimeout);
                     ok = 0;
                     break;
                 }
-                __nanosleep(100);
+                __nanosleep(32);
             }
         }
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (lane == 0) {
-            __threadfence();
-            s_ok = ok;
-            if (ok)
-                for (int k = 0; k < NV; ++k) s_res[k] = __ldcg(&gs->result[k]);
-        }
+        s_ok = ok;
     }
     __syncthreads();
     if (!s_ok) return false;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < kReduceWarps) {
+        __threadfence();
 #pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = s_res[k];
+        for (int k = 0; k < NV; ++k) {
+            double vals[kLoads];
+#pragma unroll
+            for (int m = 0; m < kLoads; ++m) {
+                const unsigned b = threadIdx.x + 32u * kReduceWarps * m;
+                vals[m] = b < gridDim.x ? __ldcg(&buf[b * kPartialStride + k]) : 0.0;
+            }
+            double s = 0.0;
+#pragma unroll
+            for (int m = 0; m < kLoads; ++m) s += vals[m];
+            s = warp_sum(s);
+            if (lane == 0) s_part[warp][k] = s;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double s = s_part[0][k];
+#pragma unroll
+        for (int w = 1; w < kReduceWarps; ++w) s += s_part[w][k];
+        out[k] = s;
+    }
+    __syncthreads();   // s_part / s_ok are rewritten by the next reduction
     return true;
+}
+
+// Called once by every block as it leaves a kernel that used grid_reduce: the
+// last block out returns the arrival counter to zero for the next launch.
+__device__ __forceinline__ void grid_exit(GridSync* gs) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> ex(gs->exit);
+        if (ex.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count);
+            cnt.store(0u, cuda::memory_order_relaxed);
+            ex.store(0u, cuda::memory_order_release);
+        }
+    }
 }
 
 }  // namespace chb

@@ -54,7 +54,7 @@ constexpr size_t kOffR = kOffZp + kHaloed;
 constexpr size_t kOffP = kOffR + kPlain;
 constexpr size_t kOffQ = kOffP + kPlain;
 constexpr size_t kOffPartials = kOffQ + kPlain;
-constexpr size_t kOffTabA = kOffPartials + kNoAllocMaxBlocks * 4 * sizeof(double);
+constexpr size_t kOffTabA = kOffPartials + 2 * kNoAllocMaxBlocks * kPartialStride * sizeof(double);
 constexpr size_t kOffTabM = kOffTabA + kMaxClasses * kMaxOffsets * sizeof(double);
 constexpr size_t kOffSync = kOffTabM + kMaxClasses * kMaxOffsets * sizeof(double);
 constexpr size_t kOffWords = kOffSync + 256;              // status, refine, ring[1], step

@@ -83,9 +83,19 @@ def test_tt06_3d_rush_larsen_parity(N, oracle):
     assert np.abs(its_g - its_o).max() <= 1
 
 
-def test_mixed_precision_against_fp64(N):
-    """Mixed mode (FP32 states, FP32 inner CG, FP64 refinement) within 0.5 mV of FP64 and activation within 1 ms."""
+@pytest.mark.parametrize("variant", ["slab", "csr", "slab_two_nodes_per_thread"])
+def test_mixed_precision_against_fp64(N, variant):
+    """Mixed mode (FP32 states, FP32 inner CG, FP64 refinement) within 0.5 mV of FP64 and activation within 1 ms.
+
+    slab: the pipelined inner solve with one node per thread; csr: the assembled
+    operator (two-reduction inner PCG); slab_two_nodes_per_thread: a slab of
+    159,681 nodes, more than the co-resident grid has threads, so each thread
+    keeps two nodes' inner vectors in registers."""
     case = dict(TC.TT06_3D)
+    if variant == "csr":
+        case["use_csr"] = True
+    elif variant == "slab_two_nodes_per_thread":
+        case.update(size=(1.0, 0.5, 0.3), box_hi=(0.1, 0.1, 0.1))
     a, _ = TC.make_gpu(N, precision=0, **case)
     b, _ = TC.make_gpu(N, precision=1, **case)
     worst = 0.0
