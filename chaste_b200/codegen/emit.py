@@ -713,7 +713,7 @@ def _emit_vjp(self, fname, outputs, wdoc, stim_zero=False):
     L.append("                                const T* __restrict__ w, T* __restrict__ gy, T* __restrict__ gp) {")
     L.append("        (void)stim; (void)cm; (void)p; (void)w; (void)gy; (void)gp;")
     if stim_zero:
-        L.append("        stim = T(0.0);")
+        L.append("        stim = T(0.0); (void)stim;")
     body, adj = _vjp_body(self, outputs, pr, stim_zero)
     L.extend(body)
     for i, st in enumerate(self.states):

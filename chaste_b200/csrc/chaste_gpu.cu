@@ -83,6 +83,8 @@ struct cg_ctx {
     int ode_blocks = 0;
     int cg_blocks = 0;
     int pipe_nodes = 0;   // > 0: mixed slab solve by cg_mixed_pipe_kernel with this many nodes per thread
+    StageArgs stage{};    // its shared-memory staging of the operator input
+    size_t pipe_smem = 0; // dynamic shared memory of that launch
     int diag_slot = 0;
     // stats
     long long steps = 0;
@@ -332,6 +334,46 @@ CgKernel pick_cg_kernel(const cg_ctx* c) {
     return c->mixed() ? pick_cg_kernel_t<true>(c) : pick_cg_kernel_t<false>(c);
 }
 
+// Bands of the slab offsets for the pipelined solve's window copies: offsets
+// closer than 1024 share a band (3D: one band per z plane).  False when the
+// offsets need more than kMaxBands bands.
+bool plan_stage(cg_ctx* c) {
+    StageArgs& g = c->stage;
+    g = StageArgs{};
+    const SlabStencil& st = c->stencil;
+    std::vector<int> offs(st.offsets, st.offsets + st.n_offsets);
+    std::sort(offs.begin(), offs.end());
+    int lo[kMaxBands], hi[kMaxBands], nb = 0;
+    for (size_t i = 0; i < offs.size(); ++i) {
+        if (nb == 0 || offs[i] - hi[nb - 1] > 1024) {
+            if (nb == kMaxBands) return false;
+            lo[nb] = hi[nb] = offs[i];
+            nb++;
+        } else {
+            hi[nb - 1] = offs[i];
+        }
+    }
+    g.n_bands = nb;
+    g.halo = (int)c->halo;
+    int base = 0;
+    for (int b = 0; b < nb; ++b) {
+        const int delta = ((lo[b] + g.halo) % 4 + 4) % 4;
+        g.lo[b] = lo[b];
+        g.len[b] = (delta + 512 + (hi[b] - lo[b]) + 3) / 4 * 4;
+        g.base[b] = base;
+        base += g.len[b];
+    }
+    g.cap = base;
+    g.alloc_len = ((long long)c->n + 2 * c->halo) / 4 * 4;
+    for (int o = 0; o < st.n_offsets; ++o) {
+        int b = 0;
+        while (b + 1 < nb && st.offsets[o] > hi[b]) ++b;
+        const int delta = ((lo[b] + g.halo) % 4 + 4) % 4;
+        g.rel[o] = g.base[b] + delta + (st.offsets[o] - lo[b]);
+    }
+    return true;
+}
+
 int alloc_vectors(cg_ctx* c) {
     const size_t n = (size_t)c->n;
     CG_TRY(dalloc_haloed(c, &c->d_V, n));
@@ -375,9 +417,12 @@ int alloc_vectors(cg_ctx* c) {
     if (c->mixed() && c->slab && pick_pipe(c, 1)) {
         const long long threads = (long long)c->cg_blocks * 512;
         const long long k = ((long long)n + threads - 1) / threads;
-        int per_sm_pipe = 0;
-        if (k <= 4) {
-            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, pick_pipe(c, (int)k), 512, 0));
+        if (k <= 4 && plan_stage(c)) {
+            c->pipe_smem = (size_t)k * c->stage.cap * sizeof(float);
+            CgKernel kern = pick_pipe(c, (int)k);
+            CG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->pipe_smem));
+            int per_sm_pipe = 0;
+            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, kern, 512, c->pipe_smem));
             if ((long long)per_sm_pipe * sms >= c->cg_blocks) c->pipe_nodes = (int)k;
         }
     }
@@ -412,8 +457,11 @@ int upload_operator(cg_ctx* c) {
                     count[cl]++;
                 }
         c->interior_cls = (int)(std::max_element(count.begin(), count.end()) - count.begin());
-        c->halo = 0;
-        for (int o = 0; o < st.n_offsets; ++o) c->halo = std::max<long long>(c->halo, std::abs(st.offsets[o]));
+        // zero halo of the stencil-read vectors: the largest offset, plus slack for
+        // the float4-aligned window copies of the pipelined solve, a multiple of 4
+        long long far = 0;
+        for (int o = 0; o < st.n_offsets; ++o) far = std::max<long long>(far, std::abs(st.offsets[o]));
+        c->halo = (far + 8 + 3) / 4 * 4;
         CG_TRY(dalloc(c, &c->d_cls8, cls.size()));
         CG_CUDA(cudaMemcpyAsync(c->d_cls8, cls.data(), cls.size(), cudaMemcpyHostToDevice, s));
         c->diag_slot = -1;
@@ -658,6 +706,7 @@ CgArgs make_cg_args(cg_ctx* c) {
     a.e32 = c->d_e32;
     a.m32a = c->d_m32a;
     a.m32b = c->d_m32b;
+    a.stage = c->stage;
     a.partials = c->d_partials;
     a.gs = c->d_gs;
     a.status = c->d_status;
@@ -681,7 +730,7 @@ cudaError_t launch_cg(cg_ctx* c) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->cg_blocks);
     cfg.blockDim = dim3(512);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = c->pipe_nodes > 0 ? c->pipe_smem : 0;
     cfg.stream = c->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;

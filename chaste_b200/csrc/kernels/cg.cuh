@@ -18,8 +18,26 @@
 
 namespace chb {
 
+// Shared-memory staging of the pipelined solve's operator input (slab stencils):
+// the offsets fall into n_bands contiguous bands (3 planes in 3D, 1 band in 1D
+// and 2D); for each 512-node group of a block, band b's window of the input
+// vector is copied with aligned float4 loads to stage[group * cap + base[b] ..],
+// and offset o of the node with thread index t is then stage[group * cap + t + rel[o]].
+constexpr int kMaxBands = 4;
+struct StageArgs {
+    int n_bands;
+    int lo[kMaxBands];      // smallest offset of the band
+    int len[kMaxBands];     // floats copied per group (multiple of 4)
+    int base[kMaxBands];    // start of the band in the group's stage (multiple of 4)
+    int cap;                // floats per group (multiple of 4)
+    int halo;               // entries before entry 0 of a haloed vector (multiple of 4)
+    long long alloc_len;    // floats of a haloed allocation, rounded down to a multiple of 4
+    int rel[kMaxOffsets];
+};
+
 struct CgArgs {
     SlabOp slab;
+    StageArgs stage;
     CsrOp csr;
     int n;
     double* x;                  // V: initial guess in, solution out (haloed)

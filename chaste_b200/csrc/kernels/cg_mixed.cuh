@@ -233,12 +233,106 @@ __device__ __forceinline__ double apply_a64_l2(const CgArgs& a, const SlabShared
     return slab_row_l2<NOFF, double>(&sh.a[c * NOFF], a.slab.off, i, x);
 }
 
+// 1D bulk copies (TMA, cp.async.bulk global -> shared, no multicast) completing
+// on an mbarrier.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Wait (bounded by 2 s of %globaltimer) for the phase with this parity.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > kBarrierTimeoutNs) return false;
+    return true;
+}
+
+// Thread 0 starts the copies of the band windows of x (a haloed vector) that the
+// groups of this block read; x was published by other blocks before the grid
+// reduction this thread has just acquired, and the stage was last read before
+// the block barrier that ended that reduction, hence the two proxy fences.
+template <int KMAX>
+__device__ __forceinline__ void stage_windows_start(const CgArgs& a, const float* x, float* stage,
+                                                    unsigned long long* bar) {
+    if (threadIdx.x != 0) return;
+    const StageArgs& g = a.stage;
+    const float* xa = x - g.halo;   // allocation start, 256-byte aligned
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    unsigned total = 0;
+    long long s0[KMAX][kMaxBands];
+    unsigned bytes[KMAX][kMaxBands];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        const long long gb = (long long)blockIdx.x * blockDim.x + k * stride;
+        for (int b = 0; b < g.n_bands; ++b) {
+            const int delta = (g.lo[b] + g.halo) & 3;
+            s0[k][b] = gb + g.lo[b] + g.halo - delta;   // multiple of 4 floats: 16-byte aligned
+            const long long len = gb < a.n ? min((long long)g.len[b], g.alloc_len - s0[k][b]) : 0;
+            bytes[k][b] = (unsigned)(len * 4);
+            total += bytes[k][b];
+        }
+    }
+    mbar_expect_tx(bar, total);
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k)
+        for (int b = 0; b < g.n_bands; ++b)
+            if (bytes[k][b]) bulk_copy_g2s(stage + k * g.cap + g.base[b], xa + s0[k][b], bytes[k][b], bar);
+}
+
+template <int NOFF>
+__device__ __forceinline__ float apply_a32_staged(const CgArgs& a, const SlabShared<float>& s32, int c,
+                                                  const float* st) {
+    float acc = 0.0f;
+    if (c == a.slab.interior) {
+#pragma unroll
+        for (int o = 0; o < NOFF; ++o) acc += a.slab.ia32[o] * st[a.stage.rel[o]];
+    } else {
+        const float* coef = &s32.a[c * NOFF];
+#pragma unroll
+        for (int o = 0; o < NOFF; ++o) acc += coef[o] * st[a.stage.rel[o]];
+    }
+    return acc;
+}
+
 template <int NOFF, int KMAX>
 __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsigned& round) {
     __shared__ SlabShared<double> sh;
     __shared__ SlabShared<float> s32;
     __shared__ double red[32 * 4];
     __shared__ double red_out[4];
+    extern __shared__ float4 stage4[];
+    float* stage = reinterpret_cast<float*>(stage4);
+    __shared__ __align__(8) unsigned long long stage_bar;
+    unsigned stage_parity = 0;
+    if (threadIdx.x == 0) mbar_init(&stage_bar);
     slab_load_shared<double>(a.slab, sh, a.diag_slot);
     slab_load_shared<float>(a.slab, s32, a.diag_slot);
     if (*(volatile int*)a.status & ~kStatusStateRange) return;
@@ -333,16 +427,32 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
             if (!(denom > 0.0)) break;   // breakdown: the FP64 residual update decides what follows
             const double alpha = gamma / denom;
             const float af = (float)alpha, bf = (float)beta;
+            stage_windows_start<KMAX>(a, mb, stage, &stage_bar);
+            // the updates that do not need A m run while the windows are in flight
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) {
-                const float nk = on[k] ? apply_a32_l2<NOFF>(a, s32, cls[k], node[k], mb) : 0.0f;
-                zq[k] = nk + bf * zq[k];
                 q[k] = m[k] + bf * q[k];
                 sv[k] = w[k] + bf * sv[k];
                 p[k] = u[k] + bf * p[k];
                 e[k] += af * p[k];
                 r[k] -= af * sv[k];
                 u[k] -= af * q[k];
+                // published every iteration: the reduction that ends the sweep is then
+                // also the barrier the FP64 refinement pass needs
+                if (on[k]) e32[node[k]] = e[k];
+            }
+            const bool late = !mbar_wait(&stage_bar, stage_parity);
+            stage_parity ^= 1u;
+            if (__syncthreads_or(late)) {
+                if (threadIdx.x == 0) atomicOr(a.status, kStatusBarrierTimeout);
+                mbar_wait(&stage_bar, stage_parity ^ 1u);   // let copies still in flight land first
+                return;
+            }
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) {
+                const float nk =
+                    on[k] ? apply_a32_staged<NOFF>(a, s32, cls[k], stage + k * a.stage.cap + threadIdx.x) : 0.0f;
+                zq[k] = nk + bf * zq[k];
                 w[k] -= af * zq[k];
             }
             gamma_old = gamma;
@@ -353,15 +463,8 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
             if (blockIdx.x == 0 && threadIdx.x == 0) *a.refine_out = sweeps;
             return cg_finish(a, step, total_its, kStatusCgDiverged);
         }
-        // ---- publish e, then x += e and r -= A e in FP64 (e of the neighbours complete)
-        {
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k)
-                if (on[k]) e32[node[k]] = e[k];
-            double v[1] = {0};
-            block_reduce<1>(v, red, red_out);
-            if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
-        }
+        // ---- x += e and r -= A e in FP64 (e of every node was published before the
+        // reduction that ended the sweep)
         {
             double v[1] = {0};
 #pragma unroll

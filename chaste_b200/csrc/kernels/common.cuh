@@ -161,9 +161,11 @@ __device__ bool grid_reduce(GridSync* gs, double* partials, const double* block_
     }
     __syncthreads();
     if (!s_ok) return false;
+    // thread 0's acquire load and the block barrier order these loads after every
+    // block's release (the pattern of a cooperative-groups grid sync), so the
+    // reading warps need no fence of their own
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp < kReduceWarps) {
-        __threadfence();
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             double vals[kLoads];

@@ -303,7 +303,7 @@ struct LuoRudy1991 {
     CHB_HD static void vjp_iionic(const T* __restrict__ y, T stim, T cm, const T* __restrict__ p,
                                 const T* __restrict__ w, T* __restrict__ gy, T* __restrict__ gp) {
         (void)stim; (void)cm; (void)p; (void)w; (void)gy; (void)gp;
-        stim = T(0.0);
+        stim = T(0.0); (void)stim;
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
         const T v_fast_sodium_current__i_Na = ((T(23.0)*p[0])*(y[1]*y[1]*y[1])*y[2]*y[3]*(y[0] - T(54.79446393509185)));
         const T v_plateau_potassium_current__Kp = (T(1.0)/(T(1.0) + m_exp(((T(7.488) - y[0])/T(5.98)))));

@@ -129,6 +129,12 @@ typedef struct {
 int orc_cable_run(const orc_cable_config* c, const double* params, const int* probes, int n_probes,
                   const double* targets, double* loss, double* traces, double* grad);
 
+/* The same gradient by forward mode: one tangent-linear run per parameter
+ * (dual numbers through the cell model, A dV' = M dz - dA V' for the voltage),
+ * `threads` runs at a time.  Independent of the adjoint's reverse products. */
+int orc_cable_tangent_gradient(const orc_cable_config* c, const double* params, const int* probes, int n_probes,
+                               const double* targets, double* grad, int threads);
+
 #ifdef __cplusplus
 }
 #endif

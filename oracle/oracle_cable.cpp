@@ -18,7 +18,55 @@
 #include <cmath>
 #include <vector>
 
+#include <thread>
+
 #include "oracle_internal.h"
+
+// Dual numbers (value, derivative along one direction) for the tangent-linear
+// run: the cell-model templates instantiated on Dual give exact directional
+// derivatives of the same discrete step (branches follow the values).
+namespace chb {
+struct Dual {
+    double v, d;
+    constexpr Dual() : v(0.0), d(0.0) {}
+    constexpr Dual(double x) : v(x), d(0.0) {}
+    constexpr Dual(double x, double dx) : v(x), d(dx) {}
+};
+inline Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(Dual a, Dual b) {
+    const double q = a.v / b.v;
+    return Dual(q, (a.d - q * b.d) / b.v);
+}
+inline Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+inline Dual& operator+=(Dual& a, Dual b) { return a = a + b; }
+inline Dual& operator-=(Dual& a, Dual b) { return a = a - b; }
+inline Dual& operator*=(Dual& a, Dual b) { return a = a * b; }
+inline Dual& operator/=(Dual& a, Dual b) { return a = a / b; }
+inline bool operator<(Dual a, Dual b) { return a.v < b.v; }
+inline bool operator>(Dual a, Dual b) { return a.v > b.v; }
+inline bool operator<=(Dual a, Dual b) { return a.v <= b.v; }
+inline bool operator>=(Dual a, Dual b) { return a.v >= b.v; }
+inline Dual m_exp(Dual a) {
+    const double e = std::exp(a.v);
+    return Dual(e, e * a.d);
+}
+inline Dual m_log(Dual a) { return Dual(std::log(a.v), a.d / a.v); }
+inline Dual m_sqrt(Dual a) {
+    const double r = std::sqrt(a.v);
+    return Dual(r, a.d / (2.0 * r));
+}
+inline Dual m_pow(Dual a, Dual b) {
+    const double p = std::pow(a.v, b.v);
+    double d = a.d != 0.0 ? b.v * std::pow(a.v, b.v - 1.0) * a.d : 0.0;
+    if (b.d != 0.0) d += p * std::log(a.v) * b.d;
+    return Dual(p, d);
+}
+inline Dual fabs(Dual a) { return a.v < 0.0 ? -a : a; }
+template <>
+constexpr Dual singularity_offset<Dual>() { return Dual(1e-7); }
+}  // namespace chb
 
 namespace {
 
@@ -226,7 +274,99 @@ int run(const orc_cable_config& c, const double* prm, const int* probes, int np,
     return 0;
 }
 
+// Directional derivative of the loss along dir (R x W) by a tangent-linear
+// run: the ODE step and Iion on Dual numbers, then A dV' = M dz - dA V' for
+// the new voltage's derivative (dA = dK along dir; CG to rtol from the last
+// derivative).  The primal values follow the same arithmetic as run().
+template <class M>
+int tangent(const orc_cable_config& c, const double* prm, const double* dir, const int* probes, int np,
+            const double* targets, double* dloss) {
+    using Run = CableRun<M>;
+    using chb::Dual;
+    constexpr int S = Run::S, P = Run::P, W = Run::W;
+    const int n = c.n_nodes, R = c.n_regions, T = c.n_steps;
+    Run run_(c, prm);
+    Tri dA;
+    dA.d.assign(n, 0.0);
+    dA.o.assign(n, 0.0);
+    for (int e = 0; e < n - 1; ++e) {
+        const double k = c.sigma * dir[elem_region(e, n, R) * W + P] / c.h;
+        dA.d[e] += k;
+        dA.d[e + 1] += k;
+        dA.o[e] = -k;
+    }
+    std::vector<double> y((size_t)n * S), yd((size_t)n * S, 0.0), V(n), Vd(n, 0.0), z(n), zd(n), b(n), bd(n), t(n);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < S; ++k) y[(size_t)i * S + k] = M::kInitialStates[k];
+    for (int i = 0; i < n; ++i) V[i] = y[(size_t)i * S];
+    double acc = 0.0;
+    for (int s = 0; s < T; ++s) {
+        const double t0 = s * c.dt, t1 = t0 + c.dt;
+        for (int i = 0; i < n; ++i) {
+            const int r = node_region(i, n, R);
+            Dual yy[S], pp[P], dy[S];
+            for (int k = 0; k < S; ++k) yy[k] = Dual(y[(size_t)i * S + k], yd[(size_t)i * S + k]);
+            yy[0] = Dual(V[i], Vd[i]);
+            for (int k = 0; k < P; ++k) pp[k] = Dual(prm[r * W + k], dir[r * W + k]);
+            M::template rhs<Dual>(yy, Dual(run_.stim(i, t0) / c.am), Dual(c.cm), pp, dy);
+            for (int k = 1; k < S; ++k) yy[k] += Dual(c.dt) * dy[k];
+            const Dual ii = M::template iionic<Dual>(yy, Dual(c.cm), pp);
+            const Dual zz = Dual(run_.ms) * yy[0] + (Dual(-c.am) * ii - Dual(run_.stim(i, t1)));
+            for (int k = 1; k < S; ++k) {
+                y[(size_t)i * S + k] = yy[k].v;
+                yd[(size_t)i * S + k] = yy[k].d;
+            }
+            z[i] = zz.v;
+            zd[i] = zz.d;
+        }
+        run_.Mm.mul(z, b);
+        if (cg(run_.A, b, V, c.rtol, c.max_iterations, true) < 0) return -1;
+        run_.Mm.mul(zd, bd);
+        dA.mul(V, t);
+        for (int i = 0; i < n; ++i) bd[i] -= t[i];
+        if (cg(run_.A, bd, Vd, c.rtol, c.max_iterations, true) < 0) return -1;
+        for (int k = 0; k < np; ++k)
+            acc += 2.0 * (V[probes[k]] - targets[(size_t)s * np + k]) * Vd[probes[k]];
+    }
+    *dloss = acc / ((double)T * np);
+    return 0;
+}
+
+template <class M>
+int tangent_gradient(const orc_cable_config& c, const double* prm, const int* probes, int np,
+                     const double* targets, double* grad, int threads) {
+    constexpr int W = M::kNumParams + 1;
+    const int m = c.n_regions * W;
+    std::vector<int> rc(m, 0);
+    std::vector<std::thread> pool;
+    const int nt = std::max(1, std::min(threads, m));
+    for (int w = 0; w < nt; ++w) {
+        pool.emplace_back([&, w]() {
+            std::vector<double> dir(m);
+            for (int k = w; k < m; k += nt) {
+                std::fill(dir.begin(), dir.end(), 0.0);
+                dir[k] = 1.0;
+                rc[k] = tangent<M>(c, prm, dir.data(), probes, np, targets, &grad[k]);
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
+    for (int k = 0; k < m; ++k)
+        if (rc[k]) return rc[k];
+    return 0;
+}
+
 }  // namespace
+
+extern "C" int orc_cable_tangent_gradient(const orc_cable_config* c, const double* params, const int* probes,
+                                          int n_probes, const double* targets, double* grad, int threads) {
+    if (!c || !params || !probes || n_probes < 1 || !targets || !grad || c->n_nodes < 2 || c->n_regions < 1 ||
+        c->n_steps < 1)
+        return -4;
+    if (c->model == ORC_LR91)
+        return tangent_gradient<chb::LuoRudy1991>(*c, params, probes, n_probes, targets, grad, threads);
+    return tangent_gradient<chb::TenTusscher2006Epi>(*c, params, probes, n_probes, targets, grad, threads);
+}
 
 extern "C" int orc_cable_run(const orc_cable_config* c, const double* params, const int* probes, int n_probes,
                              const double* targets, double* loss, double* traces, double* grad) {

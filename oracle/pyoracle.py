@@ -114,6 +114,8 @@ def lib():
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_cable_run.restype = C.c_int
         L.orc_cable_run.argtypes = [C.POINTER(CableConfig), dp, ip, C.c_int, dp, dp, dp, dp]
+        L.orc_cable_tangent_gradient.restype = C.c_int
+        L.orc_cable_tangent_gradient.argtypes = [C.POINTER(CableConfig), dp, ip, C.c_int, dp, dp, C.c_int]
         _lib = L
     return _lib
 
@@ -251,3 +253,16 @@ def cable_run(cfg: CableConfig, params, probes, targets=None, traces=False, grad
     if rc != 0:
         raise RuntimeError(f"orc_cable_run failed with code {rc}")
     return dict(loss=loss.value if tg is not None else None, traces=tr, grad=g)
+
+
+def cable_tangent_gradient(cfg: CableConfig, params, probes, targets, threads=None):
+    """orc_cable_tangent_gradient: dL/dparams by forward mode, one tangent run per parameter."""
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    probes = np.ascontiguousarray(probes, dtype=np.int32)
+    tg = np.ascontiguousarray(targets, dtype=np.float64)
+    g = np.zeros_like(params)
+    rc = lib().orc_cable_tangent_gradient(C.byref(cfg), _dp(params), _ip(probes), probes.size, _dp(tg), _dp(g),
+                                          int(threads or os.cpu_count() or 1))
+    if rc != 0:
+        raise RuntimeError(f"orc_cable_tangent_gradient failed with code {rc}")
+    return g

@@ -96,6 +96,10 @@ def test_adjoint_matches_oracle_gradient(env):
     assert abs(loss - ref["loss"]) <= 1e-9 * abs(ref["loss"])
     err = _rel_err(g, ref["grad"])
     assert err.max() <= 1e-6, (err.max(), g, ref["grad"])
+    # and against forward mode (tangent-linear runs on the CPU, no reverse products)
+    gt = O.cable_tangent_gradient(CC.oracle_config(O, cfg), p0[0], probes, targets.cpu().numpy())
+    err = _rel_err(g, gt)
+    assert err.max() <= 1e-6, (err.max(), g, gt)
 
 
 def test_autograd_function_and_batched_adjoint(env):

@@ -50,3 +50,20 @@ def test_cable_adjoint_matches_central_differences(O):
     err = np.abs(g - fd) / np.maximum(np.abs(fd), 1e-3 * scale)
     assert res["loss"] > 0
     assert err.max() <= 1e-4, (err.max(), g, fd)
+
+
+def test_cable_adjoint_matches_forward_mode(O):
+    """The reverse sweep (generated reverse products) against a tangent-linear run per
+    parameter (the primal cell-model templates on dual numbers): no finite-difference
+    step, so it also holds where a perturbation would move a node across one of
+    LR91's discontinuous gate-rate switches at -40 mV."""
+    cfg = CC.PlainCableConfig(n_nodes=120, n_steps=2000, n_regions=3, rtol=1e-12, checkpoint_every=128)
+    probes = CC.even_probes(cfg.n_nodes, 6)
+    oc = CC.oracle_config(O, cfg)
+    truth = CC.lognormal_params(np.random.default_rng(8), 1, 3, 7, 0.3)[0]
+    targets = O.cable_run(oc, truth, probes, traces=True)["traces"]
+    p0 = CC.lognormal_params(np.random.default_rng(9), 1, 3, 7, 0.1)[0]
+    g = O.cable_run(oc, p0, probes, targets, gradient=True)["grad"]
+    gt = O.cable_tangent_gradient(oc, p0, probes, targets)
+    err = np.abs(g - gt) / np.maximum(np.abs(gt), 1e-3 * np.max(np.abs(gt)))
+    assert err.max() <= 1e-6, (err.max(), g, gt)
