@@ -323,8 +323,25 @@ def main():
     ap.add_argument("--workload", default="tt06_slab_3d", choices=sorted(WORKLOADS) + ["tt06_population"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["fp64", "mixed"],
+                    help="only build the workload's tissue in this precision and take --steps steps "
+                         "(the program the ncu captures in profiles/ run)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.profile:
+        import torch
+
+        from chaste_b200 import _native as N
+        from chaste_b200.build import build_native
+
+        build_native()
+        t = build_tissue(N, WORKLOADS[args.workload], 0 if args.profile == "fp64" else 1, 0)
+        t.step(args.steps)
+        torch.cuda.synchronize()
+        st = t.stats()
+        print(json.dumps({"profile": args.profile, "workload": args.workload, "steps": int(st.steps),
+                          "last_cg_iterations": st.last_cg_iterations}), flush=True)
+        return
     if args.workload == "tt06_population":
         print(json.dumps(run_population(args)), flush=True)
         return

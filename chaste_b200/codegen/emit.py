@@ -134,11 +134,11 @@ class Printer:
             if len(num) >= 1 and num[0].is_Number and float(num[0]) == -1:
                 rest = num[1:]
                 ns = "T(1.0)" if not rest else "*".join(self._fac(f) for f in rest)
-                s = f"-{ns}" if not den else f"-({ns}/{self._den(den)})"
+                s = f"-{ns}" if not den else f"-{self._div(ns, den)}"
                 return f"({s})"
             ns = "T(1.0)" if not num else "*".join(self._fac(f) for f in num)
             if den:
-                return f"({ns}/{self._den(den)})"
+                return f"({self._div(ns, den)})"
             return f"({ns})" if len(num) > 1 else ns
         if isinstance(e, sp.Pow):
             b, x = e.base, e.exp
@@ -153,7 +153,7 @@ class Printer:
                 if xv == 0.5:
                     return f"m_sqrt({self.p(b)})"
                 if xv == -1:
-                    return f"(T(1.0)/{self.p(b)})"
+                    return f"({self._div('T(1.0)', [b])})"
                 if xv == int(xv) and 4 <= xv <= 8:
                     bs = self.p(b)
                     return "(" + "*".join([bs] * int(xv)) + ")"
@@ -162,7 +162,7 @@ class Printer:
             return f"m_exp({self.p(e.args[0])})"
         if isinstance(e, sp.log):
             if len(e.args) == 2:
-                return f"(m_log({self.p(e.args[0])})/m_log({self.p(e.args[1])}))"
+                return f"m_div(m_log({self.p(e.args[0])}), m_log({self.p(e.args[1])}))"
             return f"m_log({self.p(e.args[0])})"
         if isinstance(e, sp.floor):
             return f"floor({self.p(e.args[0])})"
@@ -177,6 +177,14 @@ class Printer:
                     out = f"(({self.cond(cond)}) ? {self.p(expr)} : {out if out is not None else 'T(NAN)'})"
             return out
         raise ValueError(f"cannot print {type(e)}: {e}")
+
+    def _div(self, ns, den):
+        """Quotient: m_divk for a numeric denominator (exact in double, multiply by the
+        reciprocal in float), m_div otherwise (a / b, or the fast quotient in float)."""
+        if len(den) == 1 and den[0].is_Number:
+            c = float(den[0])
+            return f"m_divk({ns}, {self.p(den[0])}, T({_lit(1.0 / c)}))"
+        return f"m_div({ns}, {self._den(den)})"
 
     def _split_neg(self, t):
         if isinstance(t, sp.Mul) and t.args[0].is_Number and float(t.args[0]) < 0:

@@ -60,6 +60,32 @@ CHB_HD float m_pow(float x, float y) {
 #endif
 }
 
+// Quotients.  m_div(a, b) is a / b, except in single precision on the device
+// (CHB_FAST_FP32) where it is __fdividef (the SFU reciprocal, 2 ulp).
+// m_divk(x, k, kinv) divides by the literal k: exactly in double, by
+// multiplication with the rounded reciprocal kinv in float.
+CHB_HD double m_div(double a, double b) { return a / b; }
+CHB_HD double m_divk(double x, double k, double kinv) {
+    (void)kinv;
+    return x / k;
+}
+CHB_HD float m_div(float a, float b) {
+#if defined(__CUDA_ARCH__) && CHB_FAST_FP32
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+CHB_HD float m_divk(float x, float k, float kinv) {
+#if defined(__CUDA_ARCH__) && CHB_FAST_FP32
+    (void)k;
+    return x * kinv;
+#else
+    (void)kinv;
+    return x / k;
+#endif
+}
+
 // Half-width, in units of the exponent argument U, of the window around a
 // removable singularity of a GHK-type term within which the emitted code
 // interpolates linearly (as chaste_codegen's singularity fixes do).  FP32 needs

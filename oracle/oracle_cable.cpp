@@ -64,6 +64,8 @@ inline Dual m_pow(Dual a, Dual b) {
     return Dual(p, d);
 }
 inline Dual fabs(Dual a) { return a.v < 0.0 ? -a : a; }
+inline Dual m_div(Dual a, Dual b) { return a / b; }
+inline Dual m_divk(Dual x, Dual k, Dual) { return x / k; }
 template <>
 constexpr Dual singularity_offset<Dual>() { return Dual(1e-7); }
 }  // namespace chb
