@@ -51,6 +51,7 @@ struct cg_ctx {
     HostCsr csr;
     // device arrays
     double* d_V = nullptr;
+    double* d_Vprev = nullptr;    // mixed precision: V of the previous step (extrapolated CG guess)
     void* d_states = nullptr;     // (S-1) x n of T
     void* d_iion = nullptr;
     void* d_z = nullptr;
@@ -387,6 +388,7 @@ int alloc_vectors(cg_ctx* c) {
         CG_TRY(dalloc(c, &c->d_p32, n * sizeof(float)));
         CG_TRY(dalloc(c, &c->d_q32, n * sizeof(float)));
         CG_TRY(dalloc_haloed(c, &c->d_e32, n));
+        CG_TRY(dalloc(c, &c->d_Vprev, n * sizeof(double)));
         CG_TRY(dalloc_haloed(c, &c->d_m32a, n));
         CG_TRY(dalloc_haloed(c, &c->d_m32b, n));
     }
@@ -602,6 +604,7 @@ int upload_cells_t(cg_ctx* c, const double* init, const int* pset, const double*
     cudaStream_t s = c->stream;
     CG_CUDA(cudaMemcpyAsync(c->d_states, soa.data(), soa.size() * sizeof(T), cudaMemcpyHostToDevice, s));
     CG_CUDA(cudaMemcpyAsync(c->d_V, v.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (c->d_Vprev) CG_CUDA(cudaMemcpyAsync(c->d_Vprev, c->d_V, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     CG_CUDA(cudaMemsetAsync(c->d_iion, 0, n * sizeof(T), s));
     CG_CUDA(cudaMemsetAsync(c->d_z, 0, n * sizeof(T), s));
     std::vector<uint8_t> ps;
@@ -641,6 +644,7 @@ void launch_ode(cg_ctx* c) {
     OdeArgs<T> a;
     a.n = c->n;
     a.V = c->d_V;
+    a.vprev = c->d_Vprev;
     a.states = (T*)c->d_states;
     a.iion = (T*)c->d_iion;
     a.zrhs = (T*)c->d_z;
@@ -930,6 +934,8 @@ int cg_set_voltage(cg_ctx* c, const double* v) {
     if (!c->have_cells) return CG_ERR_ORDER;
     CG_CUDA(cudaSetDevice(c->device));
     CG_CUDA(cudaMemcpy(c->d_V, v, (size_t)c->n * sizeof(double), cudaMemcpyHostToDevice));
+    // a voltage set from outside has no history: the next guess is V itself
+    if (c->d_Vprev) CG_CUDA(cudaMemcpy(c->d_Vprev, c->d_V, (size_t)c->n * sizeof(double), cudaMemcpyDeviceToDevice));
     return CG_OK;
 }
 
@@ -1063,6 +1069,7 @@ int cg_restore(cg_ctx* c, const void* buf, size_t bytes) {
     const size_t n = (size_t)c->n, w = c->real_size();
     const char* p = (const char*)buf + sizeof(h);
     CG_CUDA(cudaMemcpy(c->d_V, p, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (c->d_Vprev) CG_CUDA(cudaMemcpy(c->d_Vprev, c->d_V, n * sizeof(double), cudaMemcpyDeviceToDevice));
     p += n * sizeof(double);
     CG_CUDA(cudaMemcpy(c->d_act, p, n * sizeof(double), cudaMemcpyHostToDevice));
     p += n * sizeof(double);

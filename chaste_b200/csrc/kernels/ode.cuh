@@ -17,7 +17,8 @@ namespace chb {
 template <typename T>
 struct OdeArgs {
     int n;
-    const double* __restrict__ V;
+    double* __restrict__ V;             // V^n in; with vprev, the CG initial guess out
+    double* __restrict__ vprev;         // V^{n-1} (mixed precision), or null
     T* __restrict__ states;             // (S-1) x n
     T* __restrict__ iion;               // n
     T* __restrict__ zrhs;               // n
@@ -53,6 +54,14 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         T y[S];
         const double v = a.V[i];
+        // mixed precision: the diffusion solve starts from the linear extrapolation
+        // 2 V^n - V^{n-1} (FP64 mode keeps Chaste's guess V^n, LinearSystem.cpp:833-837);
+        // the right-hand side below still uses V^n
+        if (a.vprev) {
+            const double vp = a.vprev[i];
+            a.vprev[i] = v;
+            a.V[i] = 2.0 * v - vp;
+        }
         // activation bookkeeping of the previous step's solution (time t0)
         if (v > a.act_threshold && a.act[i] < 0.0) a.act[i] = t0;
         y[0] = (T)v;
