@@ -201,12 +201,16 @@ def run_ours(args, rank, world, device):
     # end-to-end through the C-ABI with host buffers: V in, step, V out every step
     head = "mixed" if vm_err <= 0.5 else "fp64"
     te = results[head]["tissue"]
-    vh = te.voltage()
+    # page-locked host buffers (the copies are then DMA transfers, no staging copy)
+    vin = torch.empty(te.n, dtype=torch.float64, pin_memory=True).numpy()
+    vout = torch.empty(te.n, dtype=torch.float64, pin_memory=True).numpy()
+    te.voltage(out=vin)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        te.set_voltage(vh)
+        te.set_voltage(vin)
         te.step(1)
-        vh = te.voltage()
+        te.voltage(out=vout)
+        vin, vout = vout, vin
     e2e_s = time.perf_counter() - t0
     out = {}
     for label, r in results.items():
@@ -297,6 +301,78 @@ def run_population(args):
             "per_beat_max_vm_error_mv": {"max": max(dv), "median": float(np.median(dv))}}
 
 
+def run_cable(args):
+    """LR91 cable of 1000 nodes, h 0.01 cm, dt 0.01 ms, 400 ms, stimulus at x = 0,
+    20 evenly spaced probes, targets from scale factors drawn from lognormal(0, 0.3) over 4 regions x 7
+    (six LR91 conductances + the region's tissue conductivity), loss = MSE of the probe traces, gradient by
+    the adjoint with checkpoints every 200 steps; central differences (eps 1e-6) of all 28 parameters run
+    as 56 cables in one launch.  Metric: gradient evaluations/s (forward with checkpoints + adjoint)."""
+    import torch
+
+    from chaste_b200 import fitting as F
+    from chaste_b200.build import build_native
+
+    build_native()
+    cfg = F.default_cable_config()
+    probes = F.even_probes(cfg.n_nodes, 20)
+    cable = F.Cable(cfg, probes)
+    rng = np.random.default_rng(20261203)
+    truth = torch.tensor(np.exp(rng.normal(0.0, 0.3, size=(1, 4, cable.stride))), device="cuda")
+    targets = cable.forward(truth, traces=True)["traces"][0].contiguous()
+    p0 = torch.ones((1, 4, cable.stride), dtype=torch.float64, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    cable.forward(p0, targets, keep_checkpoints=True)   # warm-up
+    torch.cuda.synchronize()
+    ev[0].record()
+    out = cable.forward(p0, targets, keep_checkpoints=True, iterations=True)
+    ev[1].record()
+    grad = cable.backward(p0, targets)
+    ev[2].record()
+    sets = np.repeat(np.ones((1, 4, cable.stride)), 2 * 4 * cable.stride, axis=0)
+    for k in range(4 * cable.stride):
+        sets[2 * k].flat[k] += 1e-6
+        sets[2 * k + 1].flat[k] -= 1e-6
+    d_sets = torch.tensor(sets, device="cuda")
+    ev[3].record()
+    fd_loss = cable.forward(d_sets, targets)["loss"]
+    ev[4].record()
+    torch.cuda.synchronize()
+    t_fwd, t_adj, t_fd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[3].elapsed_time(ev[4])
+    g = grad.cpu().numpy()[0]
+    fl = fd_loss.cpu().numpy()
+    fd = ((fl[0::2] - fl[1::2]) / 2e-6).reshape(g.shape)
+    rel = np.abs(g - fd) / np.maximum(np.abs(fd), 1e-3 * np.abs(fd).max())
+    node_steps = cfg.n_nodes * cfg.n_steps
+    line = {"metric": "cable gradient evaluations/s (forward with checkpoints + adjoint, 28 parameters)",
+            "value": 1e3 / (t_fwd + t_adj), "unit": "gradients/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "LR91 cable 1000 nodes h=0.01 cm, dt 0.01 ms, 400 ms, 4 regions x 7 scales, "
+                                   "20 probes, checkpoints every 200 steps, CG+Jacobi rtol 1e-8"},
+            "ms_forward": t_fwd, "ms_adjoint": t_adj, "ms_fd_56_cables_one_launch": t_fd,
+            "forward_node_steps_per_s": node_steps / (t_fwd / 1e3),
+            "fd_cable_node_steps_per_s": 56 * node_steps / (t_fd / 1e3),
+            "loss": float(out["loss"][0]), "cg_iterations_forward": int(out["iterations"][0]),
+            "adjoint_vs_central_differences": {
+                "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
+                "within_1e-4": int((rel <= 1e-4).sum()), "of": int(rel.size),
+                "note": "LR91's h/j gate rates jump at V = -40 mV, so a 1e-6 change of a parameter that moves "
+                        "activation times (g_Na, g_K1, g_b, sigma) crosses branch switches somewhere in the "
+                        "cable; the forward-mode check of tests/test_gpu_cable.py covers those"}}
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+
+        from tests import cable_cases as CC
+
+        k = max(200, int(4000 * min(1.0, args.cpu_seconds / 15.0)))
+        cc = CC.PlainCableConfig(n_nodes=cfg.n_nodes, n_steps=k, n_regions=4)
+        t0 = time.perf_counter()
+        O.cable_run(CC.oracle_config(O, cc), np.ones((4, cable.stride)), probes, traces=True)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": cfg.n_nodes * k / dt, "unit": "node-steps/s (forward)", "cores": 1,
+                                "kind": "port", "sample": f"{k} steps of the 1000-node cable forward, {dt:.1f} s"}
+    return line
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -320,7 +396,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tt06_slab_3d", choices=sorted(WORKLOADS) + ["tt06_population"])
+    ap.add_argument("--workload", default="tt06_slab_3d",
+                    choices=sorted(WORKLOADS) + ["tt06_population", "lr91_cable_adjoint"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", choices=["fp64", "mixed"],
@@ -344,6 +421,9 @@ def main():
         return
     if args.workload == "tt06_population":
         print(json.dumps(run_population(args)), flush=True)
+        return
+    if args.workload == "lr91_cable_adjoint":
+        print(json.dumps(run_cable(args)), flush=True)
         return
     rank, world, local, dist = dist_setup(args)
     wl = WORKLOADS[args.workload]

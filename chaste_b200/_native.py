@@ -224,8 +224,11 @@ class Tissue:
         return a.value, b.value
 
     # -- views
-    def voltage(self):
-        v = np.empty(self.n)
+    def voltage(self, out=None):
+        """V (FP64, n values); `out` may be a caller buffer (e.g. page-locked) to fill."""
+        v = np.empty(self.n) if out is None else out
+        if v.dtype != np.float64 or v.size != self.n or not v.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of n values")
         check(lib().cg_get_voltage(self.h, dptr(v)), "cg_get_voltage")
         return v
 
