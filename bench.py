@@ -222,6 +222,17 @@ def run_ours(args, rank, world, device):
     return dict(n=n, out=out, vm_err=vm_err, head=head, e2e_s=e2e_s, wl=wl)
 
 
+# DRAM bytes (read + write) per launch from one ncu capture of each kernel on the
+# 442,401-node slab (profiles/cg_kernels_tt06_slab_3d.md, profiles/ode_kernel_tt06_slab_3d.md;
+# `bench.py --profile <precision> --steps 30`, 26th launch)
+NCU_TRAFFIC = {
+    ("tt06_slab_3d", "mixed", "cg_kernel"): 8.03e6,
+    ("tt06_slab_3d", "mixed", "ode_kernel"): 39.7e6,
+    ("tt06_slab_3d", "fp64", "cg_kernel"): 8.70e6,
+    ("tt06_slab_3d", "fp64", "ode_kernel"): 127.2e6,
+}
+
+
 def roofline(res, args):
     peak, kind = hbm_peak()
     head = res["head"]
@@ -235,8 +246,10 @@ def roofline(res, args):
     ach_cg = b_cg / (o["ms_cg"] / 1e3) / 1e9
     dom = "ode" if o["ms_ode"] >= o["ms_cg"] else "cg"
     ach = ach_ode if dom == "ode" else ach_cg
-    return {"bound": "hbm", "kernel": "ode_kernel" if dom == "ode" else "cg_kernel", "achieved": round(ach, 1),
-            "peak": peak, "peak_kind": kind, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+    kern = "ode_kernel" if dom == "ode" else "cg_kernel"
+    traffic = NCU_TRAFFIC.get((args.workload, head, kern))
+    return {"bound": "hbm", "kernel": kern, "achieved": round(ach, 1),
+            "peak": peak, "peak_kind": kind, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": traffic,
             "per_kernel": {"ode_kernel": {"ms": round(o["ms_ode"], 4), "algorithmic_bytes": b_ode,
                                           "achieved_gbs": round(ach_ode, 1)},
                            "cg_kernel": {"ms": round(o["ms_cg"], 4), "algorithmic_bytes": int(b_cg),
@@ -363,7 +376,9 @@ def run_cable(args):
 
         from tests import cable_cases as CC
 
-        k = max(200, int(4000 * min(1.0, args.cpu_seconds / 15.0)))
+        # about one oracle forward of the whole cable (~8 s on one host core), fewer steps for a
+        # smaller --cpu-seconds
+        k = max(2000, min(cfg.n_steps, int(cfg.n_steps * args.cpu_seconds / 8.0)))
         cc = CC.PlainCableConfig(n_nodes=cfg.n_nodes, n_steps=k, n_regions=4)
         t0 = time.perf_counter()
         O.cable_run(CC.oracle_config(O, cc), np.ones((4, cable.stride)), probes, traces=True)

@@ -110,7 +110,6 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
     __shared__ SlabShared<double> sh;
     __shared__ int soff[kMaxOffsets];
     __shared__ double red[32 * 4];
-    __shared__ double red_out[4];
     if constexpr (SLAB) {
         for (int k = threadIdx.x; k < a.slab.n_off; k += blockDim.x) soff[k] = a.slab.off[k];
         slab_load_shared<double>(a.slab, sh, a.diag_slot);
@@ -143,8 +142,7 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
             r[i] = rr;
             zp[i] = zz;
         }
-        block_reduce<4>(v, red, red_out);
-        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status, round)) return;
+        if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
     }
     double rnorm0 = sqrt(res[1]);
     double dp = sqrt(res[2]);
@@ -163,8 +161,7 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
             v[1] += b * zz;
         }
         double o2[2];
-        block_reduce<2>(v, red, red_out);
-        if (!grid_reduce<2>(a.gs, a.partials, red_out, o2, a.status, round)) return;
+        if (!grid_reduce<2>(v, red, a.gs, a.partials, o2, a.status, round)) return;
         dp = sqrt(o2[0]);
         beta = o2[1];
         rnorm0 = dp;
@@ -194,8 +191,7 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
                 p[i] = pi;
                 v[0] += pi * qi;
             }
-            block_reduce<1>(v, red, red_out);
-            if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
+            if (!grid_reduce<1>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }
         const double dpi = res[0];
         if (!(dpi > 0.0)) return cg_finish(a, step, it + 1, isfinite(dpi) ? kStatusCgDiverged : kStatusNaN);
@@ -213,8 +209,7 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
                 v[0] += zz * zz;
                 v[1] += zz * rr;
             }
-            block_reduce<2>(v, red, red_out);
-            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
+            if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }
         dp = sqrt(res[0]);
         if (!isfinite(dp)) return cg_finish(a, step, it + 1, kStatusNaN);

@@ -51,7 +51,6 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
     __shared__ SlabShared<float> s32;
     __shared__ int soff[kMaxOffsets];
     __shared__ double red[32 * 4];
-    __shared__ double red_out[4];
     if constexpr (SLAB) {
         for (int k = threadIdx.x; k < a.slab.n_off; k += blockDim.x) soff[k] = a.slab.off[k];
         slab_load_shared<double>(a.slab, sh, a.diag_slot);
@@ -94,8 +93,7 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
             z32[i] = zf;
             v[3] += (double)rf * (double)zf;
         }
-        block_reduce<4>(v, red, red_out);
-        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status, round)) return;
+        if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
     }
     rnorm0 = sqrt(res[1]);
     dp = sqrt(res[2]);
@@ -137,8 +135,7 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
                     p32[i] = pi;
                     v[0] += (double)pi * (double)qi;
                 }
-                block_reduce<1>(v, red, red_out);
-                if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
+                if (!grid_reduce<1>(v, red, a.gs, a.partials, res, a.status, round)) return;
             }
             const double dpi = res[0];
             if (!(dpi > 0.0)) break;   // the FP64 residual update decides what happens next
@@ -155,8 +152,7 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
                     v[0] += (double)zz * (double)zz;
                     v[1] += (double)zz * (double)rr;
                 }
-                block_reduce<2>(v, red, red_out);
-                if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
+                if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
             }
             const double dp_in = sqrt(res[0]);
             betaold = beta;
@@ -186,8 +182,7 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
                 v[0] += zz * zz;
                 v[1] += (double)rf * (double)zf;
             }
-            block_reduce<2>(v, red, red_out);
-            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
+            if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }
         dp = sqrt(res[0]);
         rz = res[1];
@@ -337,7 +332,6 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
     __shared__ SlabShared<double> sh;
     __shared__ SlabShared<float> s32;
     __shared__ double red[32 * 4];
-    __shared__ double red_out[4];
     extern __shared__ float4 stage4[];
     float* stage = reinterpret_cast<float*>(stage4);
     __shared__ __align__(8) unsigned long long stage_bar;
@@ -388,8 +382,7 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
             u[k] = dinv[k] * r[k];
             z32[i] = u[k];
         }
-        block_reduce<4>(v, red, red_out);
-        if (!grid_reduce<4>(a.gs, a.partials, red_out, res, a.status, round)) return;
+        if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
     }
     double rnorm0 = sqrt(res[1]);
     double dp = sqrt(res[2]);
@@ -427,8 +420,7 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
                 m[k] = dinv[k] * w[k];
                 if (on[k]) mb[node[k]] = m[k];
             }
-            block_reduce<2>(v, red, red_out);
-            if (!grid_reduce<2>(a.gs, a.partials, red_out, res, a.status, round)) return;
+            if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
             const double gamma = res[0], delta = res[1];
             if (it == 0) g0 = gamma;
             if (!(gamma > 0.0) || !(gamma > target * target * g0) || it >= a.maxit) break;
@@ -492,8 +484,7 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
                 u[k] = dinv[k] * r[k];
                 z32[i] = u[k];
             }
-            block_reduce<1>(v, red, red_out);
-            if (!grid_reduce<1>(a.gs, a.partials, red_out, res, a.status, round)) return;
+            if (!grid_reduce<1>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }
         dp = sqrt(res[0]);
     }

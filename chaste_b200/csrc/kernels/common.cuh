@@ -100,96 +100,90 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Reduce NV per-thread values over the block into smem_out[NV].
-template <int NV>
-__device__ __forceinline__ void block_reduce(double (&v)[NV], double* smem /* 32*NV */, double* smem_out) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) smem[warp * NV + k] = v[k];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double s = lane < nw ? smem[lane * NV + k] : 0.0;
-            s = warp_sum(s);
-            if (lane == 0) smem_out[k] = s;
-        }
-    }
-    __syncthreads();
-}
-
-// All blocks contribute NV partial sums (partials: 2 x gridDim x kPartialStride
-// doubles); out[] receives the grid totals, identical in every block.  `round`
-// counts this block's reductions in the launch (start at 0; same sequence in
-// every block).  The partials are read by the first kReduceWarps warps, thread
-// t taking blocks t, t + 32 kReduceWarps, ... (at most 4 loads, issued together),
-// then each warp's shuffle tree and the warps in order; the order is fixed, so
-// every block gets bitwise the same sums.  Needs blockDim >= 32 * kReduceWarps.
+// Block and grid reduction in one: every thread contributes v[NV]; out[] receives
+// the grid totals, identical in every block.  The block's sum is formed by each
+// warp's shuffle tree and then warp 0's over the warps (so thread 0 holds it and
+// arrives without a further block barrier); partials: 2 x gridDim x
+// kPartialStride doubles; `round` counts this block's reductions in the launch
+// (start at 0; same sequence in every block).  The partials are read back by the
+// first kReduceWarps warps, thread t taking blocks t, t + 32 kReduceWarps, ... (at
+// most 4 loads, issued together), then each warp's shuffle tree and the warps in
+// order: the order is fixed, so every block gets bitwise the same sums.
+// Needs blockDim >= 32 * kReduceWarps; red holds 32 * NV doubles.
 constexpr int kReduceWarps = 4;
 
 template <int NV>
-__device__ bool grid_reduce(GridSync* gs, double* partials, const double* block_vals, double* out, int* status,
+__device__ bool grid_reduce(double (&v)[NV], double* red, GridSync* gs, double* partials, double* out, int* status,
                             unsigned& round) {
     static_assert(NV >= 1 && NV <= kPartialStride, "at most four sums per reduction");
     constexpr int kLoads = kMaxGridBlocks / (32 * kReduceWarps);
     __shared__ int s_ok;
     __shared__ double s_part[kReduceWarps][kPartialStride];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp * NV + k] = v[k];
+    __syncthreads();
     double* buf = partials + (size_t)(round & 1u) * gridDim.x * kPartialStride;
     const unsigned target = (round + 1u) * gridDim.x;
     round++;
-    if (threadIdx.x == 0) {
-        int ok = 1;
+    if (warp == 0) {
+        double b[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) buf[blockIdx.x * kPartialStride + k] = block_vals[k];
-        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count);
-        cnt.fetch_add(1u, cuda::memory_order_release);
-        if (cnt.load(cuda::memory_order_acquire) < target) {
-            const unsigned long long t0 = global_ns();
-            while (cnt.load(cuda::memory_order_acquire) < target) {
-                if ((*(volatile int*)status & kStatusBarrierTimeout) || global_ns() - t0 > kBarrierTimeoutNs) {
-                    atomicOr(status, kStatusBarrierTimeout);
-                    ok = 0;
-                    break;
+        for (int k = 0; k < NV; ++k) b[k] = warp_sum(lane < nw ? red[lane * NV + k] : 0.0);
+        if (lane == 0) {
+            int ok = 1;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) buf[blockIdx.x * kPartialStride + k] = b[k];
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count);
+            cnt.fetch_add(1u, cuda::memory_order_release);
+            if (cnt.load(cuda::memory_order_acquire) < target) {
+                const unsigned long long t0 = global_ns();
+                while (cnt.load(cuda::memory_order_acquire) < target) {
+                    if ((*(volatile int*)status & kStatusBarrierTimeout) || global_ns() - t0 > kBarrierTimeoutNs) {
+                        atomicOr(status, kStatusBarrierTimeout);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(32);
                 }
-                __nanosleep(32);
             }
+            s_ok = ok;
         }
-        s_ok = ok;
     }
     __syncthreads();
     if (!s_ok) return false;
     // thread 0's acquire load and the block barrier order these loads after every
     // block's release (the pattern of a cooperative-groups grid sync), so the
     // reading warps need no fence of their own
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp < kReduceWarps) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             double vals[kLoads];
 #pragma unroll
             for (int m = 0; m < kLoads; ++m) {
-                const unsigned b = threadIdx.x + 32u * kReduceWarps * m;
-                vals[m] = b < gridDim.x ? __ldcg(&buf[b * kPartialStride + k]) : 0.0;
+                const unsigned bb = threadIdx.x + 32u * kReduceWarps * m;
+                vals[m] = bb < gridDim.x ? __ldcg(&buf[bb * kPartialStride + k]) : 0.0;
             }
-            double s = 0.0;
+            double sum = 0.0;
 #pragma unroll
-            for (int m = 0; m < kLoads; ++m) s += vals[m];
-            s = warp_sum(s);
-            if (lane == 0) s_part[warp][k] = s;
+            for (int m = 0; m < kLoads; ++m) sum += vals[m];
+            sum = warp_sum(sum);
+            if (lane == 0) s_part[warp][k] = sum;
         }
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-        double s = s_part[0][k];
+        double sum = s_part[0][k];
 #pragma unroll
-        for (int w = 1; w < kReduceWarps; ++w) s += s_part[w][k];
-        out[k] = s;
+        for (int w = 1; w < kReduceWarps; ++w) sum += s_part[w][k];
+        out[k] = sum;
     }
-    __syncthreads();   // s_part / s_ok are rewritten by the next reduction
+    // no trailing barrier: the next reduction writes s_part / s_ok / red only after
+    // its own block barrier, which every thread reaches after reading these
     return true;
 }
 
