@@ -83,6 +83,7 @@ struct cg_ctx {
     // launch shapes
     int ode_blocks = 0;
     int cg_blocks = 0;
+    int cg_threads = 512;   // threads per block of the persistent CG kernel
     int pipe_nodes = 0;   // > 0: mixed slab solve by cg_mixed_pipe_kernel with this many nodes per thread
     StageArgs stage{};    // its shared-memory staging of the operator input
     size_t pipe_smem = 0; // dynamic shared memory of that launch
@@ -338,7 +339,7 @@ CgKernel pick_cg_kernel(const cg_ctx* c) {
 // Bands of the slab offsets for the pipelined solve's window copies: offsets
 // closer than 1024 share a band (3D: one band per z plane).  False when the
 // offsets need more than kMaxBands bands.
-bool plan_stage(cg_ctx* c) {
+bool plan_stage(cg_ctx* c, int threads) {
     StageArgs& g = c->stage;
     g = StageArgs{};
     const SlabStencil& st = c->stencil;
@@ -360,7 +361,7 @@ bool plan_stage(cg_ctx* c) {
     for (int b = 0; b < nb; ++b) {
         const int delta = ((lo[b] + g.halo) % 4 + 4) % 4;
         g.lo[b] = lo[b];
-        g.len[b] = (delta + 512 + (hi[b] - lo[b]) + 3) / 4 * 4;
+        g.len[b] = (delta + threads + (hi[b] - lo[b]) + 3) / 4 * 4;
         g.base[b] = base;
         base += g.len[b];
     }
@@ -415,20 +416,36 @@ int alloc_vectors(cg_ctx* c) {
     if (per_sm < 1) return CG_ERR_UNSUPPORTED;
     const long long want = ((long long)n + 511) / 512;
     c->cg_blocks = (int)std::max(1LL, std::min({want, (long long)per_sm * sms, (long long)kMaxGridBlocks}));
+    c->cg_threads = 512;
+    const int blocks_512 = c->cg_blocks;
     c->pipe_nodes = 0;
     if (c->mixed() && c->slab && pick_pipe(c, 1)) {
-        const long long threads = (long long)c->cg_blocks * 512;
-        const long long k = ((long long)n + threads - 1) / threads;
-        if (k <= 4 && plan_stage(c)) {
-            c->pipe_smem = (size_t)k * c->stage.cap * sizeof(float);
-            CgKernel kern = pick_pipe(c, (int)k);
-            CG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->pipe_smem));
+        // one block of kPipeThreads per SM; nodes per thread as that grid gives
+        const long long k0 = ((long long)n + (long long)sms * kPipeThreads - 1) / ((long long)sms * kPipeThreads);
+        if (k0 <= 4 && plan_stage(c, kPipeThreads)) {
+            CgKernel kern0 = pick_pipe(c, (int)k0);
+            const size_t smem0 = (size_t)k0 * c->stage.cap * sizeof(float);
+            CG_CUDA(cudaFuncSetAttribute(kern0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
             int per_sm_pipe = 0;
-            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, kern, 512, c->pipe_smem));
-            if ((long long)per_sm_pipe * sms >= c->cg_blocks) c->pipe_nodes = (int)k;
+            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, kern0, kPipeThreads, smem0));
+            if (per_sm_pipe >= 1) {
+                const long long blocks = std::max(1LL, std::min({((long long)n + kPipeThreads - 1) / kPipeThreads,
+                                                                  (long long)per_sm_pipe * sms,
+                                                                  (long long)kMaxGridBlocks}));
+                const long long k = ((long long)n + blocks * kPipeThreads - 1) / (blocks * kPipeThreads);
+                if (k <= k0) {
+                    c->pipe_nodes = (int)k;
+                    c->pipe_smem = (size_t)k * c->stage.cap * sizeof(float);
+                    CG_CUDA(cudaFuncSetAttribute(pick_pipe(c, (int)k), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)c->pipe_smem));
+                    c->cg_blocks = (int)blocks;
+                    c->cg_threads = kPipeThreads;
+                }
+            }
         }
     }
-    CG_TRY(dalloc(c, &c->d_partials, (size_t)2 * c->cg_blocks * kPartialStride * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_partials,
+                  (size_t)2 * std::max(blocks_512, c->cg_blocks) * kPartialStride * sizeof(double)));
     c->ode_blocks = (int)std::max(1LL, std::min(((long long)n + 255) / 256, (long long)sms * 16));
     CG_CUDA(cudaStreamSynchronize(s));
     return CG_OK;
@@ -733,7 +750,7 @@ cudaError_t launch_cg(cg_ctx* c) {
     CgArgs a = make_cg_args(c);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->cg_blocks);
-    cfg.blockDim = dim3(512);
+    cfg.blockDim = dim3(c->cg_threads);
     cfg.dynamicSmemBytes = c->pipe_nodes > 0 ? c->pipe_smem : 0;
     cfg.stream = c->stream;
     cudaLaunchAttribute attr[1];

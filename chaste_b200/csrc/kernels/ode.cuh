@@ -82,8 +82,10 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
         const T cm = (T)a.cm;
         DevTimeStepper ts(t0, t1, a.dt_ode);
         while (!ts.at_end()) {
-            // cell stimulus in uA/cm^2 = tissue stimulus / Am (GetIntracellularAreaStimulus)
-            const T s = (T)(stimulus_value(st, ts.time) / a.am);
+            // cell stimulus in uA/cm^2 = tissue stimulus / Am (GetIntracellularAreaStimulus);
+            // most nodes have none, and 0 / Am = +0 needs no division
+            const double sv = stimulus_value(st, ts.time);
+            const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
             if (METHOD == 1) {
                 rl_step_except_voltage<M, T>(y, s, cm, p, (T)a.dt_ode);
             } else {

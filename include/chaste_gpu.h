@@ -94,7 +94,8 @@ typedef struct {
     double ms_last_call;           /* device time of the last cg_step call */
     int pipelined_nodes_per_thread; /* mixed slab solve: > 0 when the single-reduction (pipelined)
                                        inner solve runs, keeping this many nodes per thread in registers */
-    int cg_blocks;                 /* blocks of the persistent CG kernel (512 threads each) */
+    int cg_blocks;                 /* blocks of the persistent CG kernel (512 threads each; 1024 when
+                                      pipelined_nodes_per_thread > 0) */
 } cg_stats;
 
 /* Fill cfg with Chaste's defaults (LR91, FE, dt 0.01, Am 1400, Cm 1, Jacobi, atol 2e-4). */
