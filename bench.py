@@ -226,7 +226,7 @@ def run_ours(args, rank, world, device):
 # 442,401-node slab (profiles/cg_kernels_tt06_slab_3d.md, profiles/ode_kernel_tt06_slab_3d.md;
 # `bench.py --profile <precision> --steps 30`, 26th launch)
 NCU_TRAFFIC = {
-    ("tt06_slab_3d", "mixed", "cg_kernel"): 8.03e6,
+    ("tt06_slab_3d", "mixed", "cg_kernel"): 7.24e6,
     ("tt06_slab_3d", "mixed", "ode_kernel"): 39.7e6,
     ("tt06_slab_3d", "fp64", "cg_kernel"): 8.70e6,
     ("tt06_slab_3d", "fp64", "ode_kernel"): 127.2e6,
@@ -388,6 +388,19 @@ def run_cable(args):
     return line
 
 
+def aggregate(dist, device, ms_step, e2e_s, n, steps, world):
+    """Whole-job figures of N replicas: the max over ranks of the device step time and of
+    the end-to-end time (a collective on `device`: cuda for NCCL, cpu for gloo), then
+    throughput = all ranks' node-steps over that time."""
+    if dist is not None and world > 1:
+        import torch
+
+        tt = torch.tensor([ms_step, e2e_s], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_step, e2e_s = tt.tolist()
+    return {"ms_step": ms_step, "value": world * n / (ms_step / 1e3), "e2e_rate": world * n * steps / e2e_s}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -468,14 +481,8 @@ def main():
     res = run_ours(args, rank, world, local)
     head = res["head"]
     o = res["out"][head]
-    ms_step = o["ms_per_step"]
-    e2e_rate = res["n"] * args.steps / res["e2e_s"]
-    if dist:
-        tt = torch.tensor([ms_step, res["e2e_s"]], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms_step, e2e_s = tt.tolist()
-        e2e_rate = world * res["n"] * args.steps / e2e_s
-    value = world * res["n"] / (ms_step / 1e3)
+    agg = aggregate(dist, f"cuda:{local}", o["ms_per_step"], res["e2e_s"], res["n"], args.steps, world)
+    ms_step, value, e2e_rate = agg["ms_step"], agg["value"], agg["e2e_rate"]
     if rank == 0:
         line = {
             "metric": metric, "value": value, "unit": "node-steps/s", "n_gpus": world,

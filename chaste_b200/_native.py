@@ -25,6 +25,7 @@ ODE_FORWARD_EULER, ODE_RUSH_LARSEN = 0, 1
 PC_NONE, PC_JACOBI, PC_BJACOBI = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 STIM_NONE, STIM_SIMPLE, STIM_REGULAR = 0, 1, 2
+SOLVER_MONODOMAIN, SOLVER_OPERATOR_SPLITTING = 0, 1
 
 
 class ChasteGpuError(RuntimeError):
@@ -47,6 +48,7 @@ class Config(C.Structure):
         ("use_absolute_tolerance", C.c_int), ("ksp_tolerance", C.c_double),
         ("use_mass_lumping", C.c_int), ("max_iterations", C.c_int), ("precision", C.c_int),
         ("device", C.c_int), ("check_state_ranges", C.c_int), ("activation_threshold", C.c_double),
+        ("solver", C.c_int),
     ]
 
 
@@ -115,6 +117,7 @@ SIGNATURES = {
     "cg_cable_forward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp]),
     "cg_cable_backward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
     "cg_cable_destroy": (C.c_int, [_vp]),
+    "cg_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_double, _ip, _dp]),
     "cg_slab_solve_noalloc": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, _dp, _vp, _vp, _vp, _ip]),
 }

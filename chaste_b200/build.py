@@ -12,7 +12,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 
-SOURCES = ["chaste_gpu.cu", "noalloc.cu", "batch.cu", "cable.cu", "host/assemble.cpp"]
+SOURCES = ["chaste_gpu.cu", "noalloc.cu", "batch.cu", "cable.cu", "selftest.cu", "host/assemble.cpp"]
 DEPS = SOURCES + [
     "kernels/common.cuh", "kernels/ops.cuh", "kernels/cg.cuh", "kernels/cg_mixed.cuh",
     "kernels/ode.cuh", "kernels/batch.cuh", "kernels/cable.cuh", "models/cellmodel_common.h", "models/lr91.h", "models/tt06.h",

@@ -251,6 +251,7 @@ int cg_create(const cg_config* cfg, cg_ctx** out) {
     if (cfg->ksp_preconditioner == CG_PC_BJACOBI) return CG_ERR_UNSUPPORTED;
     if (cfg->ksp_preconditioner != CG_PC_NONE && cfg->ksp_preconditioner != CG_PC_JACOBI) return CG_ERR_ARG;
     if (cfg->precision != CG_PRECISION_FP64 && cfg->precision != CG_PRECISION_MIXED) return CG_ERR_ARG;
+    if (cfg->solver != CG_SOLVER_MONODOMAIN && cfg->solver != CG_SOLVER_OPERATOR_SPLITTING) return CG_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -420,26 +421,30 @@ int alloc_vectors(cg_ctx* c) {
     const int blocks_512 = c->cg_blocks;
     c->pipe_nodes = 0;
     if (c->mixed() && c->slab && pick_pipe(c, 1)) {
-        // one block of kPipeThreads per SM; nodes per thread as that grid gives
-        const long long k0 = ((long long)n + (long long)sms * kPipeThreads - 1) / ((long long)sms * kPipeThreads);
-        if (k0 <= 4 && plan_stage(c, kPipeThreads)) {
+        // one block of kPipeThreads per SM when the slab fills every SM with them (fewer
+        // arrivals per grid reduction), else blocks of 512 so small slabs still spread
+        // over many SMs; nodes per thread as that grid gives
+        const int pt = (long long)n >= (long long)sms * kPipeThreads ? kPipeThreads : 512;
+        const long long per_sm_guess = kPipeThreads / pt;
+        const long long k0 = ((long long)n + sms * per_sm_guess * pt - 1) / (sms * per_sm_guess * pt);
+        if (k0 <= 4 && plan_stage(c, pt)) {
             CgKernel kern0 = pick_pipe(c, (int)k0);
             const size_t smem0 = (size_t)k0 * c->stage.cap * sizeof(float);
             CG_CUDA(cudaFuncSetAttribute(kern0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
             int per_sm_pipe = 0;
-            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, kern0, kPipeThreads, smem0));
+            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, kern0, pt, smem0));
             if (per_sm_pipe >= 1) {
-                const long long blocks = std::max(1LL, std::min({((long long)n + kPipeThreads - 1) / kPipeThreads,
+                const long long blocks = std::max(1LL, std::min({((long long)n + pt - 1) / pt,
                                                                   (long long)per_sm_pipe * sms,
                                                                   (long long)kMaxGridBlocks}));
-                const long long k = ((long long)n + blocks * kPipeThreads - 1) / (blocks * kPipeThreads);
+                const long long k = ((long long)n + blocks * pt - 1) / (blocks * pt);
                 if (k <= k0) {
                     c->pipe_nodes = (int)k;
                     c->pipe_smem = (size_t)k * c->stage.cap * sizeof(float);
                     CG_CUDA(cudaFuncSetAttribute(pick_pipe(c, (int)k), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)c->pipe_smem));
                     c->cg_blocks = (int)blocks;
-                    c->cg_threads = kPipeThreads;
+                    c->cg_threads = pt;
                 }
             }
         }
@@ -657,11 +662,12 @@ int upload_cells_t(cg_ctx* c, const double* init, const int* pset, const double*
 }
 
 template <class M, typename T>
-void launch_ode(cg_ctx* c) {
+void launch_ode(cg_ctx* c, int half = 0) {
     OdeArgs<T> a;
     a.n = c->n;
     a.V = c->d_V;
-    a.vprev = c->d_Vprev;
+    a.vprev = c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING ? nullptr : c->d_Vprev;
+    a.half = half;
     a.states = (T*)c->d_states;
     a.iion = (T*)c->d_iion;
     a.zrhs = (T*)c->d_z;
@@ -761,18 +767,29 @@ cudaError_t launch_cg(cg_ctx* c) {
     return cudaLaunchKernelEx(&cfg, pick_cg_kernel(c), a);
 }
 
-cudaError_t launch_step(cg_ctx* c) {
+// The ODE launch of a step: the whole step with V clamped (half 0), or one half of
+// the operator-splitting step including V (half 1, 2).
+void launch_odes(cg_ctx* c, int half) {
     const bool tt = c->cfg.model == CG_MODEL_TT06;
     if (c->mixed()) {
-        if (tt) launch_ode<TenTusscher2006Epi, float>(c);
-        else launch_ode<LuoRudy1991, float>(c);
+        if (tt) launch_ode<TenTusscher2006Epi, float>(c, half);
+        else launch_ode<LuoRudy1991, float>(c, half);
     } else {
-        if (tt) launch_ode<TenTusscher2006Epi, double>(c);
-        else launch_ode<LuoRudy1991, double>(c);
+        if (tt) launch_ode<TenTusscher2006Epi, double>(c, half);
+        else launch_ode<LuoRudy1991, double>(c, half);
     }
+}
+
+bool split(const cg_ctx* c) { return c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING; }
+
+cudaError_t launch_step(cg_ctx* c) {
+    launch_odes(c, split(c) ? 1 : 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    return launch_cg(c);
+    e = launch_cg(c);
+    if (e != cudaSuccess || !split(c)) return e;
+    launch_odes(c, 2);
+    return cudaGetLastError();
 }
 
 int build_graph(cg_ctx* c) {
@@ -1107,7 +1124,7 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
     if (!c || n_steps < 0) return CG_ERR_ARG;
     if (!c->have_mesh || !c->have_cells) return CG_ERR_ORDER;
     CG_CUDA(cudaSetDevice(c->device));
-    cudaEvent_t e[3];
+    cudaEvent_t e[4];
     for (auto& x : e)
         if (cudaEventCreate(&x) != cudaSuccess) {
             cudaGetLastError();
@@ -1115,24 +1132,20 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
         }
     double t_ode = 0.0, t_cg = 0.0;
     int rc = CG_OK;
-    const bool tt = c->cfg.model == CG_MODEL_TT06;
     for (int k = 0; k < n_steps && rc == CG_OK; ++k) {
         cudaEventRecord(e[0], c->stream);
-        if (c->mixed()) {
-            if (tt) launch_ode<TenTusscher2006Epi, float>(c);
-            else launch_ode<LuoRudy1991, float>(c);
-        } else {
-            if (tt) launch_ode<TenTusscher2006Epi, double>(c);
-            else launch_ode<LuoRudy1991, double>(c);
-        }
+        launch_odes(c, split(c) ? 1 : 0);
         cudaEventRecord(e[1], c->stream);
         if (cudaGetLastError() != cudaSuccess || launch_cg(c) != cudaSuccess) rc = CG_ERR_CUDA;
         cudaEventRecord(e[2], c->stream);
-        if (cudaEventSynchronize(e[2]) != cudaSuccess) rc = CG_ERR_CUDA;
-        float a = 0.f, b = 0.f;
+        if (split(c)) launch_odes(c, 2);
+        cudaEventRecord(e[3], c->stream);
+        if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e[3]) != cudaSuccess) rc = CG_ERR_CUDA;
+        float a = 0.f, b = 0.f, d = 0.f;
         cudaEventElapsedTime(&a, e[0], e[1]);
         cudaEventElapsedTime(&b, e[1], e[2]);
-        t_ode += a;
+        cudaEventElapsedTime(&d, e[2], e[3]);
+        t_ode += a + d;
         t_cg += b;
     }
     for (auto& x : e) cudaEventDestroy(x);

@@ -21,9 +21,10 @@ namespace chb {
 // convergence either way).  Measured on the 442,401-node TT06 slab: (1e-5, 0.8)
 // took 19.7 inner iterations per solve against 22.4 for (3e-5, 0.1), both in 2
 // sweeps, at the same 0.004 mV difference from the FP64 solve.
-// The pipelined solve runs one block of 1024 threads per SM: the same threads (and
-// registers) as two blocks of 512, with half the arrivals and partial sums per grid
-// reduction (measured 2.6 us per reduction against 2.9 us for 296 x 512).
+// The pipelined solve runs one block of 1024 threads per SM when the slab fills every
+// SM with such blocks: the same threads (and registers) as two blocks of 512, with
+// half the arrivals and partial sums per grid reduction (measured 2.6 us per
+// reduction against 2.9 us for 296 x 512).  Smaller slabs use blocks of 512.
 constexpr int kPipeThreads = 1024;
 
 constexpr double kInnerFloor = 1e-5;

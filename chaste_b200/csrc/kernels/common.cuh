@@ -100,6 +100,24 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// One thread waits until *counter >= target (acquire), for at most limit_ns of
+// %globaltimer.  On timeout, or when another waiter has already timed out, it sets
+// kStatusBarrierTimeout and returns false: every wait of a kernel ends.
+__device__ __forceinline__ bool wait_count(unsigned* counter, unsigned target, int* status,
+                                           unsigned long long limit_ns = kBarrierTimeoutNs) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(*counter);
+    if (cnt.load(cuda::memory_order_acquire) >= target) return true;
+    const unsigned long long t0 = global_ns();
+    while (cnt.load(cuda::memory_order_acquire) < target) {
+        if ((*(volatile int*)status & kStatusBarrierTimeout) || global_ns() - t0 > limit_ns) {
+            atomicOr(status, kStatusBarrierTimeout);
+            return false;
+        }
+        __nanosleep(32);
+    }
+    return true;
+}
+
 // Block and grid reduction in one: every thread contributes v[NV]; out[] receives
 // the grid totals, identical in every block.  The block's sum is formed by each
 // warp's shuffle tree and then warp 0's over the warps (so thread 0 holds it and
@@ -139,17 +157,7 @@ __device__ bool grid_reduce(double (&v)[NV], double* red, GridSync* gs, double* 
             for (int k = 0; k < NV; ++k) buf[blockIdx.x * kPartialStride + k] = b[k];
             cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count);
             cnt.fetch_add(1u, cuda::memory_order_release);
-            if (cnt.load(cuda::memory_order_acquire) < target) {
-                const unsigned long long t0 = global_ns();
-                while (cnt.load(cuda::memory_order_acquire) < target) {
-                    if ((*(volatile int*)status & kStatusBarrierTimeout) || global_ns() - t0 > kBarrierTimeoutNs) {
-                        atomicOr(status, kStatusBarrierTimeout);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(32);
-                }
-            }
+            ok = wait_count(&gs->count, target, status) ? 1 : 0;
             s_ok = ok;
         }
     }

@@ -32,6 +32,8 @@ struct OdeArgs {
     int check_range;
     double* act;                        // first activation time per node (-1: none yet)
     double act_threshold;
+    int half;                           // 0: ComputeExceptVoltage over the step; 1, 2: first or second
+                                        // half step including V (operator splitting)
 };
 
 // First step with V above the threshold (ActivationOutputModifier::ProcessSolutionAtTimeStep,
@@ -42,14 +44,72 @@ __global__ void activation_kernel(int n, const double* __restrict__ V, double* _
         if (V[i] > threshold && act[i] < 0.0) act[i] = t;
 }
 
+// Half a PDE step of every cell including V, for the operator-splitting solver:
+// SolveCellSystems(..., updateVoltage = true) (AbstractCardiacTissue.cpp:531-536) --
+// SolveAndUpdateState over [t0, t0 + dt/2] or [t0 + dt/2, t1] by forward Euler
+// (AbstractOneStepIvpOdeSolver::InternalSolve) or Rush-Larsen
+// (AbstractRushLarsenCardiacCell.cpp:130-147), V written back, then UpdateCaches at
+// the end of the half; after the first half z = Am*Cm*V/dt, the diffusion-only
+// right-hand side term (OperatorSplittingMonodomainSolver.cpp:86-89).
+template <class M, typename T, int METHOD>
+__device__ __forceinline__ void ode_half_step(const OdeArgs<T>& a, double t0, double t1) {
+    constexpr int S = M::kNumStates;
+    constexpr int P = M::kNumParams;
+    const double th0 = a.half == 1 ? t0 : t0 + a.dt_pde / 2.0;
+    const double th1 = a.half == 1 ? t0 + a.dt_pde / 2.0 : t1;
+    const double dtinv = 1.0 / a.dt_pde;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        T y[S];
+        const double v = a.V[i];
+        if (a.half == 1 && v > a.act_threshold && a.act[i] < 0.0) a.act[i] = t0;
+        y[0] = (T)v;
+#pragma unroll
+        for (int k = 1; k < S; ++k) y[k] = a.states[(size_t)(k - 1) * a.n + i];
+        T p[P > 0 ? P : 1];
+        if (a.pset) {
+            const T* pp = a.params + (size_t)a.pset[i] * P;
+#pragma unroll
+            for (int k = 0; k < P; ++k) p[k] = pp[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < P; ++k) p[k] = T(1);
+        }
+        const int sid = a.stim_id[i];
+        DevStimulus st{0, 0, 0, 0, 0, 0};
+        if (sid != 0xFF) st = a.stims[sid];
+        const T cm = (T)a.cm;
+        DevTimeStepper ts(th0, th1, a.dt_ode);
+        while (!ts.at_end()) {
+            const double sv = stimulus_value(st, ts.time);
+            const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
+            if (METHOD == 1) rl_step<M, T>(y, s, cm, p, (T)a.dt_ode);
+            else fe_step<M, T>(y, s, cm, p, (T)(ts.next - ts.time));
+            ts.advance();
+        }
+        const double vn = (double)y[0];
+        a.V[i] = vn;
+#pragma unroll
+        for (int k = 1; k < S; ++k) a.states[(size_t)(k - 1) * a.n + i] = y[k];
+        a.iion[i] = M::template iionic<T>(y, cm, p);
+        if (a.half == 1) a.zrhs[i] = (T)(a.am * a.cm * vn * dtinv);
+        if (!(vn == vn)) atomicOr(a.status, kStatusNaN);
+        if (a.check_range && !states_in_range<M, T>(y)) atomicOr(a.status, kStatusStateRange);
+    }
+}
+
 template <class M, typename T, int METHOD>
 __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
     constexpr int S = M::kNumStates;
     constexpr int P = M::kNumParams;
     if (*(volatile int*)a.status & ~kStatusStateRange) return;   // a failed step stops the run
-    const long long step = *a.step;
+    // the second half step runs after the diffusion solve has advanced the step counter
+    const long long step = *a.step - (a.half == 2 ? 1 : 0);
     const double t0 = (double)step * a.dt_pde;
     const double t1 = (double)(step + 1) * a.dt_pde;
+    if (a.half) {
+        ode_half_step<M, T, METHOD>(a, t0, t1);
+        return;
+    }
     const double dtinv = 1.0 / a.dt_pde;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         T y[S];

@@ -63,6 +63,7 @@ class HeartConfig:
         self.activation_threshold = -40.0
         self.check_state_ranges = False
         self.device = 0
+        self.operator_splitting = False
 
     # HeartConfig.cpp:1581-1587, 2337
     def SetOdeTimeStep(self, dt):
@@ -126,6 +127,14 @@ class HeartConfig:
 
     def SetUseMassLumping(self, flag=True):
         self.mass_lumping = bool(flag)
+
+    # HeartConfig::SetUseReactionDiffusionOperatorSplitting (MonodomainProblem.cpp:65-69
+    # then builds an OperatorSplittingMonodomainSolver)
+    def SetUseReactionDiffusionOperatorSplitting(self, flag=True):
+        self.operator_splitting = bool(flag)
+
+    def GetUseReactionDiffusionOperatorSplitting(self):
+        return self.operator_splitting
 
     def SetFibreLength(self, length, h):
         self.space_dimension, self.slab = 1, (length, 0.0, 0.0, h)
@@ -322,6 +331,7 @@ class MonodomainProblem:
         cfg.activation_threshold = hc.activation_threshold
         cfg.check_state_ranges = 1 if hc.check_state_ranges else 0
         cfg.device = hc.device
+        cfg.solver = N.SOLVER_OPERATOR_SPLITTING if hc.operator_splitting else N.SOLVER_MONODOMAIN
         return cfg
 
     def Initialise(self):

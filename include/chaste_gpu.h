@@ -50,6 +50,11 @@ enum { CG_ODE_FORWARD_EULER = 0, CG_ODE_RUSH_LARSEN = 1 };
 enum { CG_PC_NONE = 0, CG_PC_JACOBI = 1, CG_PC_BJACOBI = 2 };
 enum { CG_PRECISION_FP64 = 0, CG_PRECISION_MIXED = 1 };
 enum { CG_STIM_NONE = 0, CG_STIM_SIMPLE = 1, CG_STIM_REGULAR = 2 };
+/* MonodomainSolver (heart/src/solver/electrics/monodomain/MonodomainSolver.cpp) or
+ * OperatorSplittingMonodomainSolver (OperatorSplittingMonodomainSolver.cpp:40-117,
+ * HeartConfig::SetUseReactionDiffusionOperatorSplitting): half a step of the cells
+ * including V, the diffusion solve with z = Am*Cm*V/dt, the second half. */
+enum { CG_SOLVER_MONODOMAIN = 0, CG_SOLVER_OPERATOR_SPLITTING = 1 };
 
 /* HeartConfig fields used by the path (heart/src/problem/HeartConfig.cpp:1581-1650,
  * 2337-2412; defaults heart/src/problem/HeartConfigDefaults.hpp:53-91). */
@@ -69,6 +74,7 @@ typedef struct {
     int device;                /* CUDA device ordinal */
     int check_state_ranges;    /* 1: device-side VerifyStateVariables analogue */
     double activation_threshold; /* mV; activation time = first step with V above it */
+    int solver;                /* CG_SOLVER_* (default CG_SOLVER_MONODOMAIN) */
 } cg_config;
 
 /* SimpleStimulus (heart/src/stimulus/SimpleStimulus.cpp:44-76) / RegularStimulus
@@ -94,8 +100,8 @@ typedef struct {
     double ms_last_call;           /* device time of the last cg_step call */
     int pipelined_nodes_per_thread; /* mixed slab solve: > 0 when the single-reduction (pipelined)
                                        inner solve runs, keeping this many nodes per thread in registers */
-    int cg_blocks;                 /* blocks of the persistent CG kernel (512 threads each; 1024 when
-                                      pipelined_nodes_per_thread > 0) */
+    int cg_blocks;                 /* blocks of the persistent CG kernel (512 threads each; 1024 for a
+                                      pipelined solve of a slab that fills every SM with them) */
 } cg_stats;
 
 /* Fill cfg with Chaste's defaults (LR91, FE, dt 0.01, Am 1400, Cm 1, Jacobi, atol 2e-4). */
@@ -242,6 +248,14 @@ int cg_cable_forward(cg_cable* c, int n_sets, const double* d_params, const doub
 int cg_cable_backward(cg_cable* c, int n_sets, const double* d_params, const double* d_targets, double* d_grad,
                       void* stream);
 int cg_cable_destroy(cg_cable* c);
+
+/* Self-test of the device-side failure path, no counterpart in the reference:
+ * launches a small kernel whose blocks wait, through the same bounded wait the
+ * CG kernels' grid reductions use, for an arrival that never comes.  The wait
+ * must end after about limit_ms (1 .. 2000) with the barrier-timeout status bit
+ * (16) in *status_bits; *waited_ms (may be NULL) receives the longest wait.  No
+ * fault, trap or hang is involved, and the device stays usable afterwards. */
+int cg_selftest_barrier_timeout(int device, double limit_ms, int* status_bits, double* waited_ms);
 
 /* Allocation-free diffusion solve of one PDE step on a regular slab.
  *

@@ -21,6 +21,8 @@ enum { ORC_LR91 = 0, ORC_TT06 = 1 };
 enum { ORC_FE = 0, ORC_RL = 1 };
 enum { ORC_PC_NONE = 0, ORC_PC_JACOBI = 1, ORC_PC_BJACOBI = 2 };
 enum { ORC_STIM_NONE = 0, ORC_STIM_SIMPLE = 1, ORC_STIM_REGULAR = 2 };
+/* MonodomainSolver (default) or OperatorSplittingMonodomainSolver */
+enum { ORC_SOLVER_MONODOMAIN = 0, ORC_SOLVER_OPERATOR_SPLITTING = 1 };
 
 /* SimpleStimulus (heart/src/stimulus/SimpleStimulus.cpp:44-76) and
  * RegularStimulus (heart/src/stimulus/RegularStimulus.cpp:43-81).  The
@@ -80,6 +82,7 @@ typedef struct {
     double tol;
     int mass_lumping;
     int max_iterations;   /* PETSc default 10000 */
+    int solver;           /* ORC_SOLVER_* */
 } orc_config;
 
 typedef struct orc_tissue orc_tissue;

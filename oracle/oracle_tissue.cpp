@@ -396,7 +396,77 @@ static void solve_cells(Tissue& T, double t0, double t1) {
     });
 }
 
+// SolveCellSystems(..., updateVoltage = true) for the operator-splitting solver
+// (AbstractCardiacTissue.cpp:531-536): every cell's SolveAndUpdateState over
+// [t0, t1] including V -- forward Euler through AbstractOneStepIvpOdeSolver's
+// InternalSolve (ode/src/solver/AbstractOneStepIvpOdeSolver.cpp:115-153), or
+// Rush-Larsen (AbstractRushLarsenCardiacCell.cpp:130-147, V by Euler first) --
+// then V from the cell and UpdateCaches at t1.
+template <class Mdl>
+static void solve_cells_with_voltage(Tissue& T, double t0, double t1) {
+    const int ns = Mdl::kNumStates;
+    const int np = Mdl::kNumParams;
+    parallel_for(T.n, [&](int b, int e) {
+        double y[Mdl::kNumStates], dy[Mdl::kNumStates];
+        double pdef[16];
+        for (int k = 0; k < np; ++k) pdef[k] = 1.0;
+        for (int i = b; i < e; ++i) {
+            double* s = &T.states[(size_t)i * ns];
+            for (int k = 0; k < ns; ++k) y[k] = s[k];
+            y[0] = T.V[i];
+            const double* p = pdef;
+            if (!T.param_id.empty() && T.param_id[i] >= 0)
+                p = &T.param_table[(size_t)T.param_id[i] * np];
+            const orc_stimulus* st = (!T.stim_id.empty() && T.stim_id[i] >= 0) ? &T.stims[T.stim_id[i]] : nullptr;
+            TimeStepper ts(t0, t1, T.cfg.dt_ode);
+            while (!ts.AtEnd()) {
+                const double sv = stimulus_value(st, ts.Time()) / T.cfg.am;   // GetIntracellularAreaStimulus
+                if (T.cfg.ode_method == ORC_RL) {
+                    chb::rl_step<Mdl, double>(y, sv, T.cfg.cm, p, T.cfg.dt_ode);
+                } else {
+                    const double h = ts.NextStep();
+                    Mdl::template rhs<double>(y, sv, T.cfg.cm, p, dy);
+                    for (int k = 0; k < ns; ++k) y[k] += h * dy[k];
+                }
+                ts.Advance();
+            }
+            T.V[i] = y[0];
+            for (int k = 0; k < ns; ++k) s[k] = y[k];
+            T.iion[i] = Mdl::template iionic<double>(y, T.cfg.cm, p);
+            T.istim[i] = stimulus_value(st, t1);
+        }
+    });
+}
+
+// OperatorSplittingMonodomainSolver (heart/src/solver/electrics/monodomain/
+// OperatorSplittingMonodomainSolver.cpp:40-117): half a step of the cells with V,
+// the diffusion solve with z = Am*Cm*V/dt (no reaction term), the second half.
+static int step_split(Tissue& T, int* iters) {
+    const double t0 = T.t;
+    const double dt = T.cfg.dt_pde;
+    const double t1 = (double)(T.steps + 1) * dt;
+    if (T.cfg.model == ORC_TT06) solve_cells_with_voltage<chb::TenTusscher2006Epi>(T, t0, t0 + dt / 2.0);
+    else solve_cells_with_voltage<chb::LuoRudy1991>(T, t0, t0 + dt / 2.0);
+    const double am = T.cfg.am, cm = T.cfg.cm;
+    const double dtinv = 1.0 / dt;
+    double* zz = T.w.data();
+    parallel_for(T.n, [&](int b, int e) {
+        for (int i = b; i < e; ++i) zz[i] = am * cm * T.V[i] * dtinv;
+    });
+    T.M.matvec(zz, T.b.data());
+    T.x = T.V;
+    const int rc = cg_solve(T, T.x.data(), T.b.data(), iters);
+    if (rc != 0) return rc;
+    T.V = T.x;
+    if (T.cfg.model == ORC_TT06) solve_cells_with_voltage<chb::TenTusscher2006Epi>(T, t0 + dt / 2.0, t1);
+    else solve_cells_with_voltage<chb::LuoRudy1991>(T, t0 + dt / 2.0, t1);
+    T.steps++;
+    T.t = t1;
+    return 0;
+}
+
 static int step_once(Tissue& T, int* iters) {
+    if (T.cfg.solver == ORC_SOLVER_OPERATOR_SPLITTING) return step_split(T, iters);
     const double t0 = T.t;
     const double t1 = (double)(T.steps + 1) * T.cfg.dt_pde;
     if (T.cfg.model == ORC_TT06) solve_cells<chb::TenTusscher2006Epi>(T, t0, t1);

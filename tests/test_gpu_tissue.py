@@ -111,6 +111,28 @@ def test_mixed_precision_against_fp64(N, variant):
     assert np.abs(ta[act] - tb[act]).max() <= 1.0
 
 
+@pytest.mark.parametrize("case_name", ["LR91_2D", "TT06_3D"])
+def test_operator_splitting_parity(N, oracle, case_name):
+    """OperatorSplittingMonodomainSolver on the GPU (FP64) against the oracle's
+    restatement: half step of the cells with V, diffusion, second half."""
+    case = dict(getattr(TC, case_name))
+    case["solver"] = 1
+    g, _ = TC.make_gpu(N, **case)
+    o, _ = TC.make_oracle(oracle, **case)
+    worst = 0.0
+    for _ in range(10):
+        g.step(5)
+        o.step(5)
+        vo = o.voltage()
+        worst = max(worst, float(np.max(np.abs(g.voltage() - vo) / np.maximum(np.abs(vo), 1.0))))
+    assert worst <= FP64_RTOL, worst
+    assert o.voltage().max() > -60.0          # the stimulus took
+    # mixed precision in the same mode, within 0.5 mV of FP64
+    m, _ = TC.make_gpu(N, precision=1, **case)
+    m.step(50)
+    assert float(np.max(np.abs(m.voltage() - g.voltage()))) <= 0.5
+
+
 def test_snapshot_restore_is_bitwise(N):
     case = dict(TC.LR91_2D)
     a, _ = TC.make_gpu(N, **case)
@@ -163,6 +185,52 @@ def test_nan_voltage_is_reported(N):
     with pytest.raises(N.ChasteGpuError) as e:
         g.step(1)
     assert e.value.status == 5
+
+
+def test_state_out_of_range_is_reported(N):
+    """VerifyStateVariables analogue (AbstractCardiacCell.cpp:100-104): a gate above 1
+    with range checking on returns CG_ERR_STATE_RANGE."""
+    case = dict(TC.LR91_2D)
+
+    def tissue(check):
+        cfg = N.default_config()
+        cfg.model, cfg.ode_method = case["model"], case["method"]
+        cfg.ode_time_step, cfg.pde_time_step = case["dt_ode"], case["dt_pde"]
+        cfg.use_absolute_tolerance, cfg.ksp_tolerance = 0, 1e-8
+        cfg.ksp_preconditioner = N.PC_JACOBI
+        cfg.check_state_ranges = check
+        t = N.Tissue(cfg)
+        t.set_slab_mesh(case["dim"], case["h"], *case["size"], sigma=case["sigma"])
+        return t
+
+    ref = tissue(0)
+    ref.set_cells()
+    init = ref.states().copy()
+    # the slow time-dependent K gate X (state 6, rates ~1e-3 /ms) of node 7 outside
+    # [0, 1]; a fast gate would be pulled back inside within the step's substeps
+    init[7, 6] = 1.5
+    t = tissue(1)
+    t.set_cells(init_states=init)
+    t.set_stimulus(np.full(t.n, -1, np.int32), [N.stimulus(N.STIM_SIMPLE, 0.0, 0.0)])
+    with pytest.raises(N.ChasteGpuError) as e:
+        t.step(1)
+    assert e.value.status == 6
+
+
+def test_bounded_device_wait_times_out_and_the_device_stays_usable(N):
+    """Failure path of the persistent kernels' grid reductions, without a fault: a
+    wait for an arrival that never comes ends after its limit with the timeout bit,
+    and a tissue step afterwards still matches."""
+    import ctypes as C
+
+    bits, waited = C.c_int(0), C.c_double(0.0)
+    rc = N.lib().cg_selftest_barrier_timeout(0, 50.0, C.byref(bits), C.byref(waited))
+    assert rc == 0
+    assert bits.value & 16
+    assert 40.0 <= waited.value <= 1000.0, waited.value
+    g, _ = TC.make_gpu(N, **dict(TC.LR91_2D))
+    g.step(3)
+    assert np.all(np.isfinite(g.voltage()))
 
 
 def test_monodomain_problem_api_on_gpu(N, kats):

@@ -17,7 +17,7 @@ def slab_stim_ids(xyz, box_hi):
 
 def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
              abs_tol=None, rel_tol=1e-8, precision=0, use_csr=False, param_set=None, param_table=None,
-             init_states=None, max_iterations=10000):
+             init_states=None, max_iterations=10000, solver=0):
     """A GPU tissue on a regular slab (stencil operator, or CSR through cg_set_mesh when use_csr)."""
     from oracle import pyoracle as O  # mesh generator only: the same node/element order as the library
 
@@ -32,6 +32,7 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
         cfg.use_absolute_tolerance, cfg.ksp_tolerance = 0, rel_tol
     cfg.precision = precision
     cfg.max_iterations = max_iterations
+    cfg.solver = solver
     t = N.Tissue(cfg)
     xyz, conn, _ = O.slab_mesh(dim, h, *size)
     if use_csr:
@@ -45,11 +46,11 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
 
 
 def make_oracle(O, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
-                abs_tol=None, rel_tol=1e-8, param_set=None, param_table=None, init_states=None, **_):
+                abs_tol=None, rel_tol=1e-8, param_set=None, param_table=None, init_states=None, solver=0, **_):
     xyz, conn, _ = O.slab_mesh(dim, h, *size)
     use_abs = abs_tol is not None
     cfg = O.Config(model, method, dt_ode, dt_pde, am, cm, O.PC_JACOBI, 1 if use_abs else 0,
-                   abs_tol if use_abs else rel_tol, 0, 10000)
+                   abs_tol if use_abs else rel_tol, 0, 10000, solver)
     sig = np.tile(np.asarray(sigma[:dim], float), (conn.shape[0], 1))
     sid = slab_stim_ids(xyz, box_hi)
     return O.Tissue(cfg, dim, xyz, conn, sig, sid, [O.simple(*stim)], param_id=param_set,
