@@ -296,7 +296,8 @@ def run_population(args):
     params[:, :6] = np.exp(rng.normal(0.0, 0.2, size=(n, 6)))
     beats = rng.integers(1, 21, size=n).astype(np.int32)
     b = N.CellBatch(N.MODEL_TT06, beats, params)
-    tpb = b.autotune(steps=2000)
+    b.autotune(steps=2000)
+    tpb, cpt = b.launch_shape()
     ms = b.run()
     r = b.results()
     steps = int(beats.sum()) * 100000
@@ -309,7 +310,8 @@ def run_population(args):
             "higher_is_better": True, "dtype": "f64+f32", "data": "synthetic",
             "config": {"workload": "8192 TT06-epi cells, lognormal(0,0.2) conductance scales, 1-20 beats at "
                                    "BCL 1000 ms, RL dt 0.01 ms", "cell_steps_per_precision": steps,
-                       "threads_per_block": tpb},
+                       "threads_per_block": tpb, "cells_per_thread": cpt,
+                       "launch_shape": "autotuned over threads per block x cells per thread"},
             "apd90_fp32_vs_fp64_ms": {"max": max(d_apd), "mean": float(np.mean(d_apd)), "n": len(d_apd)},
             "per_beat_max_vm_error_mv": {"max": max(dv), "median": float(np.median(dv))}}
 

@@ -21,7 +21,7 @@ STATUS_NAMES = {
     9: "CG_ERR_NOMEM", 10: "CG_ERR_UNSUPPORTED",
 }
 MODEL_LR91, MODEL_TT06 = 0, 1
-ODE_FORWARD_EULER, ODE_RUSH_LARSEN = 0, 1
+ODE_FORWARD_EULER, ODE_RUSH_LARSEN, ODE_BACKWARD_EULER = 0, 1, 2
 PC_NONE, PC_JACOBI, PC_BJACOBI = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 STIM_NONE, STIM_SIMPLE, STIM_REGULAR = 0, 1, 2
@@ -110,6 +110,8 @@ SIGNATURES = {
                                   C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "cg_batch_autotune": (C.c_int, [_vp, C.c_int, _ip]),
     "cg_batch_run": (C.c_int, [_vp, _dp]),
+    "cg_batch_launch_shape": (C.c_int, [_vp, _ip, _ip]),
+    "cg_batch_set_launch_shape": (C.c_int, [_vp, C.c_int, C.c_int]),
     "cg_batch_results": (C.c_int, [_vp, _dp, _dp, _ip, _ip, C.POINTER(C.c_float), _dp, _dp]),
     "cg_batch_destroy": (C.c_int, [_vp]),
     "cg_cable_default_config": (None, [C.POINTER(CableConfig)]),
@@ -310,9 +312,19 @@ class CellBatch:
         self.h = h
 
     def autotune(self, steps=2000):
+        """Pick threads per block and cells per thread; returns the threads per block."""
         tpb = C.c_int()
         check(lib().cg_batch_autotune(self.h, steps, C.byref(tpb)), "cg_batch_autotune")
         return tpb.value
+
+    def set_launch_shape(self, threads_per_block, cells_per_thread):
+        check(lib().cg_batch_set_launch_shape(self.h, threads_per_block, cells_per_thread),
+              "cg_batch_set_launch_shape")
+
+    def launch_shape(self):
+        tpb, cpt = C.c_int(), C.c_int()
+        check(lib().cg_batch_launch_shape(self.h, C.byref(tpb), C.byref(cpt)), "cg_batch_launch_shape")
+        return tpb.value, cpt.value
 
     def run(self):
         ms = C.c_double()

@@ -17,6 +17,7 @@ using namespace chb;
 struct cg_batch {
     int model = 0, n = 0, S = 0, P = 0, max_beats = 0, max_aps = 0, sample_every = 10, device = 0;
     int tpb = 64;
+    int cpt = 1;            // cells per thread
     long long steps_per_beat = 0;
     double dt = 0.01;
     DevStimulus stim{};
@@ -62,7 +63,7 @@ BatchArgs batch_args(const cg_batch* b, long long steps_override) {
     a.max_aps = b->max_aps;
     a.max_beats = b->max_beats;
     a.sample_every = b->sample_every;
-    a.blocks_per_precision = (b->n + b->tpb - 1) / b->tpb;
+    a.blocks_per_precision = (b->n + b->tpb * b->cpt - 1) / (b->tpb * b->cpt);
     a.steps_per_beat = b->steps_per_beat;
     a.dt = b->dt;
     a.cm = 1.0;
@@ -83,8 +84,14 @@ BatchArgs batch_args(const cg_batch* b, long long steps_override) {
 cudaError_t launch_beat(cg_batch* b, long long steps_override, bool with_error) {
     BatchArgs a = batch_args(b, steps_override);
     const int grid = 2 * a.blocks_per_precision;
-    if (b->model == CG_MODEL_TT06) batch_kernel<TenTusscher2006Epi><<<grid, b->tpb, 0, b->stream>>>(a);
-    else batch_kernel<LuoRudy1991><<<grid, b->tpb, 0, b->stream>>>(a);
+    const bool tt = b->model == CG_MODEL_TT06;
+    if (b->cpt == 2) {
+        if (tt) batch_kernel<TenTusscher2006Epi, 2><<<grid, b->tpb, 0, b->stream>>>(a);
+        else batch_kernel<LuoRudy1991, 2><<<grid, b->tpb, 0, b->stream>>>(a);
+    } else {
+        if (tt) batch_kernel<TenTusscher2006Epi, 1><<<grid, b->tpb, 0, b->stream>>>(a);
+        else batch_kernel<LuoRudy1991, 1><<<grid, b->tpb, 0, b->stream>>>(a);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !with_error) return e;
     batch_beat_error_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(a, b->d_maxdv);
@@ -193,12 +200,14 @@ int cg_batch_autotune(cg_batch* b, int steps, int* threads_per_block) {
     cudaSetDevice(b->device);
     const int cands[4] = {32, 64, 128, 256};
     float best = 1e30f;
-    int best_tpb = b->tpb;
+    int best_tpb = b->tpb, best_cpt = b->cpt;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int c : cands) {
+    for (int cand = 0; cand < 8; ++cand) {
+        const int c = cands[cand % 4];
         b->tpb = c;
+        b->cpt = cand < 4 ? 1 : 2;
         int rc = reset_states(b);
         if (rc != CG_OK) return rc;
         cudaEventRecord(e0, b->stream);
@@ -214,17 +223,39 @@ int cg_batch_autotune(cg_batch* b, int steps, int* threads_per_block) {
         if (ms < best) {
             best = ms;
             best_tpb = c;
+            best_cpt = b->cpt;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->tpb = best_tpb;
+    b->cpt = best_cpt;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
     if (threads_per_block) *threads_per_block = best_tpb;
     return reset_states(b);
+}
+
+int cg_batch_set_launch_shape(cg_batch* b, int threads_per_block, int cells_per_thread) {
+    if (!b || threads_per_block < 32 || threads_per_block > 1024 || threads_per_block % 32 != 0 ||
+        (cells_per_thread != 1 && cells_per_thread != 2))
+        return CG_ERR_ARG;
+    b->tpb = threads_per_block;
+    b->cpt = cells_per_thread;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return CG_OK;
+}
+
+int cg_batch_launch_shape(const cg_batch* b, int* threads_per_block, int* cells_per_thread) {
+    if (!b) return CG_ERR_ARG;
+    if (threads_per_block) *threads_per_block = b->tpb;
+    if (cells_per_thread) *cells_per_thread = b->cpt;
+    return CG_OK;
 }
 
 int cg_batch_run(cg_batch* b, double* ms) {

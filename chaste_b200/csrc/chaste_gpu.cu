@@ -244,7 +244,9 @@ int cg_create(const cg_config* cfg, cg_ctx** out) {
     if (!cfg || !out) return CG_ERR_ARG;
     *out = nullptr;
     if (cfg->model != CG_MODEL_LR91 && cfg->model != CG_MODEL_TT06) return CG_ERR_ARG;
-    if (cfg->ode_method != CG_ODE_FORWARD_EULER && cfg->ode_method != CG_ODE_RUSH_LARSEN) return CG_ERR_ARG;
+    if (cfg->ode_method != CG_ODE_FORWARD_EULER && cfg->ode_method != CG_ODE_RUSH_LARSEN &&
+        cfg->ode_method != CG_ODE_BACKWARD_EULER)
+        return CG_ERR_ARG;
     if (!(cfg->ode_time_step > 0) || !(cfg->pde_time_step > 0)) return CG_ERR_ARG;
     if (!(cfg->surface_area_to_volume_ratio > 0) || !(cfg->capacitance > 0)) return CG_ERR_ARG;
     if (!(cfg->ksp_tolerance > 0)) return CG_ERR_ARG;
@@ -686,6 +688,8 @@ void launch_ode(cg_ctx* c, int half = 0) {
     a.act_threshold = c->cfg.activation_threshold;
     if (c->cfg.ode_method == CG_ODE_RUSH_LARSEN)
         ode_kernel<M, T, 1><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+    else if (c->cfg.ode_method == CG_ODE_BACKWARD_EULER)
+        ode_kernel<M, T, 2><<<c->ode_blocks, 256, 0, c->stream>>>(a);
     else
         ode_kernel<M, T, 0><<<c->ode_blocks, 256, 0, c->stream>>>(a);
 }

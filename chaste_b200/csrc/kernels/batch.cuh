@@ -136,52 +136,79 @@ __device__ __forceinline__ void apd_sample(ApdTracker& k, double v, long long q,
     k.prev_v = v;
 }
 
-template <class M, typename T>
-__device__ __forceinline__ void batch_cell(const BatchArgs& a, int cell, int prec, T* __restrict__ ys) {
+// K cells per thread (cells c0, c0 + cstride, ...), advanced together step by step
+// so their independent updates interleave; the stimulus is evaluated once per step.
+template <class M, typename T, int K>
+__device__ __forceinline__ void batch_cells(const BatchArgs& a, int c0, int cstride, int prec, T* __restrict__ ys) {
     constexpr int S = M::kNumStates;
     constexpr int P = M::kNumParams;
     const long long beat = *a.launch;
-    const long long total = (long long)a.beats[cell] * a.steps_per_beat;
     const long long s0 = beat * a.steps_per_beat;
-    if (s0 >= total) return;
     const long long s1 = a.steps_override > 0 ? s0 + a.steps_override : s0 + a.steps_per_beat;
-    T y[S];
-    T p[P > 0 ? P : 1];
+    int cell[K];
+    bool on[K];
+    bool any = false;
 #pragma unroll
-    for (int k = 0; k < S; ++k) y[k] = ys[(size_t)k * a.n_cells + cell];
+    for (int j = 0; j < K; ++j) {
+        cell[j] = c0 + j * cstride;
+        on[j] = cell[j] < a.n_cells && s0 < (long long)a.beats[cell[j]] * a.steps_per_beat;
+        any |= on[j];
+    }
+    if (!any) return;
+    T y[K][S];
+    T p[K][P > 0 ? P : 1];
+    ApdTracker trk[K];
+    T ring[K][kApdRing];
+    T up[K][kApdRing];
+    double* apd[K];
 #pragma unroll
-    for (int k = 0; k < P; ++k) p[k] = (T)a.params[(size_t)cell * P + k];
-    ApdTracker trk = a.trk[(size_t)prec * a.n_cells + cell];
-    if (s0 == 0) apd_init(trk, (double)y[0]);
-    T ring[kApdRing];
-    T up[kApdRing];
-    ring[s0 % kApdRing] = y[0];
-    double* apd = a.apd + ((size_t)prec * a.n_cells + cell) * a.max_aps;
+    for (int j = 0; j < K; ++j) {
+        const int c = on[j] ? cell[j] : c0;
+#pragma unroll
+        for (int k = 0; k < S; ++k) y[j][k] = ys[(size_t)k * a.n_cells + c];
+#pragma unroll
+        for (int k = 0; k < P; ++k) p[j][k] = (T)a.params[(size_t)c * P + k];
+        trk[j] = a.trk[(size_t)prec * a.n_cells + c];
+        if (s0 == 0) apd_init(trk[j], (double)y[j][0]);
+        ring[j][s0 % kApdRing] = y[j][0];
+        apd[j] = a.apd + ((size_t)prec * a.n_cells + c) * a.max_aps;
+    }
     const long long nsamp = (a.steps_per_beat + a.sample_every - 1) / a.sample_every;
     float* vs = a.vsamp + (size_t)prec * nsamp * a.n_cells;
     const T dt = (T)a.dt, cm = (T)a.cm;
     for (long long s = s0; s < s1; ++s) {
-        if ((s - s0) % a.sample_every == 0) vs[(size_t)((s - s0) / a.sample_every) * a.n_cells + cell] = (float)y[0];
-        const double t = (double)s * a.dt;
-        rl_step<M, T>(y, (T)stimulus_value(a.stim, t), cm, p, dt);
-        ring[(s + 1) % kApdRing] = y[0];
-        apd_sample<T>(trk, (double)y[0], s + 1, a.dt, ring, up, s0, apd, a.max_aps);
-    }
-    if (!(y[0] == y[0])) atomicOr(a.status, kStatusNaN);
+        const T st = (T)stimulus_value(a.stim, (double)s * a.dt);
+        const bool sample = (s - s0) % a.sample_every == 0;
 #pragma unroll
-    for (int k = 0; k < S; ++k) ys[(size_t)k * a.n_cells + cell] = y[k];
-    a.trk[(size_t)prec * a.n_cells + cell] = trk;
+        for (int j = 0; j < K; ++j) {
+            if (!on[j]) continue;
+            if (sample) vs[(size_t)((s - s0) / a.sample_every) * a.n_cells + cell[j]] = (float)y[j][0];
+            rl_step<M, T>(y[j], st, cm, p[j], dt);
+            ring[j][(s + 1) % kApdRing] = y[j][0];
+            apd_sample<T>(trk[j], (double)y[j][0], s + 1, a.dt, ring[j], up[j], s0, apd[j], a.max_aps);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        if (!on[j]) continue;
+        if (!(y[j][0] == y[j][0])) atomicOr(a.status, kStatusNaN);
+#pragma unroll
+        for (int k = 0; k < S; ++k) ys[(size_t)k * a.n_cells + cell[j]] = y[j][k];
+        a.trk[(size_t)prec * a.n_cells + cell[j]] = trk[j];
+    }
 }
 
-// blocks [0, blocks_per_precision) integrate in FP64, the rest in FP32; each
-// block walks 32*blockDim/32 cells at a time over the population (persistent).
-template <class M>
+// blocks [0, blocks_per_precision) integrate in FP64, the rest in FP32; thread t of
+// a precision handles cells t, t + T, ..., t + (K-1) T (T = blocks_per_precision *
+// blockDim), then the next K*T cells (persistent over the population).
+template <class M, int K>
 __global__ void batch_kernel(BatchArgs a) {
     const bool fp64 = blockIdx.x < (unsigned)a.blocks_per_precision;
     const int b = fp64 ? blockIdx.x : blockIdx.x - a.blocks_per_precision;
-    for (int cell = b * blockDim.x + threadIdx.x; cell < a.n_cells; cell += a.blocks_per_precision * blockDim.x) {
-        if (fp64) batch_cell<M, double>(a, cell, 0, a.y64);
-        else batch_cell<M, float>(a, cell, 1, a.y32);
+    const int T_threads = a.blocks_per_precision * blockDim.x;
+    for (int c = b * blockDim.x + threadIdx.x; c < a.n_cells; c += K * T_threads) {
+        if (fp64) batch_cells<M, double, K>(a, c, T_threads, 0, a.y64);
+        else batch_cells<M, float, K>(a, c, T_threads, 1, a.y32);
     }
 }
 

@@ -83,6 +83,7 @@ __device__ __forceinline__ void ode_half_step(const OdeArgs<T>& a, double t0, do
             const double sv = stimulus_value(st, ts.time);
             const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
             if (METHOD == 1) rl_step<M, T>(y, s, cm, p, (T)a.dt_ode);
+            else if (METHOD == 2) be_step<M, T>(y, s, cm, p, (T)a.dt_ode, true);
             else fe_step<M, T>(y, s, cm, p, (T)(ts.next - ts.time));
             ts.advance();
         }
@@ -140,18 +141,30 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
         DevStimulus st{0, 0, 0, 0, 0, 0};
         if (sid != 0xFF) st = a.stims[sid];
         const T cm = (T)a.cm;
-        DevTimeStepper ts(t0, t1, a.dt_ode);
-        while (!ts.at_end()) {
-            // cell stimulus in uA/cm^2 = tissue stimulus / Am (GetIntracellularAreaStimulus);
-            // most nodes have none, and 0 / Am = +0 needs no division
-            const double sv = stimulus_value(st, ts.time);
-            const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
-            if (METHOD == 1) {
-                rl_step_except_voltage<M, T>(y, s, cm, p, (T)a.dt_ode);
-            } else {
-                fe_step_except_voltage<M, T>(y, s, cm, p, (T)(ts.next - ts.time));
+        if (METHOD == 2) {
+            // AbstractBackwardEulerCardiacCell::ComputeExceptVoltage: (t1 - t0)/dt + 0.5
+            // steps at t0 + i dt, V fixed
+            const unsigned n_sub = (unsigned)((t1 - t0) / a.dt_ode + 0.5);
+            for (unsigned k = 0; k < n_sub; ++k) {
+                const double sv = stimulus_value(st, t0 + k * a.dt_ode);
+                const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
+                be_step<M, T>(y, s, cm, p, (T)a.dt_ode, false);
+                y[0] = (T)v;
             }
-            ts.advance();
+        } else {
+            DevTimeStepper ts(t0, t1, a.dt_ode);
+            while (!ts.at_end()) {
+                // cell stimulus in uA/cm^2 = tissue stimulus / Am (GetIntracellularAreaStimulus);
+                // most nodes have none, and 0 / Am = +0 needs no division
+                const double sv = stimulus_value(st, ts.time);
+                const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
+                if (METHOD == 1) {
+                    rl_step_except_voltage<M, T>(y, s, cm, p, (T)a.dt_ode);
+                } else {
+                    fe_step_except_voltage<M, T>(y, s, cm, p, (T)(ts.next - ts.time));
+                }
+                ts.advance();
+            }
         }
 #pragma unroll
         for (int k = 1; k < S; ++k) a.states[(size_t)(k - 1) * a.n + i] = y[k];

@@ -157,6 +157,74 @@ CHB_UNROLL
 
 // VerifyStateVariables analogue: true when every gate is in [0,1] and every
 // concentration is positive (and nothing is NaN).
+// Backward-Euler step (AbstractBackwardEulerCardiacCell, heart/src/odes/
+// AbstractBackwardEulerCardiacCell.hpp: ComputeOneStepExceptVoltage, and
+// SolveAndUpdateState with V first by UpdateTransmembranePotential).  With
+// with_voltage, V takes an explicit Euler step first; then every state whose ODE is
+// linear in itself, f = a + b y (the Rush-Larsen states: b = rate, a = -rate * inf),
+// takes the exact implicit step y' = (y + dt a) / (1 - dt b) at the (new) V; then the
+// remaining states solve the implicit residual R(y') = y' - y - dt f(V, gates', y')
+// by Newton's method (CardiacNewtonSolver, heart/src/odes/CardiacNewtonSolver.hpp:
+// Gaussian elimination without pivoting), here with a finite-difference Jacobian and
+// iterated until the update is below 1e-13 (double) / 1e-6 (float) relative, at most
+// 20 times.  Chaste's generated cells (chaste_codegen's backward-Euler option) take
+// the same steps with an analytic Jacobian and stop at an update of 1e-6.
+template <class Model, typename T>
+CHB_HD void be_step(T* y, T stim, T cm, const T* p, T dt, bool with_voltage) {
+    constexpr int S = Model::kNumStates;
+    T dy[S], rate[S], inf[S], old[S];
+    if (with_voltage) {
+        Model::template rhs<T>(y, stim, cm, p, dy);
+        y[0] += dt * dy[0];
+    }
+    Model::template rl_terms<T>(y, stim, cm, p, rate, inf);
+CHB_UNROLL
+    for (int k = 0; k < S; ++k) old[k] = y[k];
+CHB_UNROLL
+    for (int k = 1; k < S; ++k)
+        if (Model::rush_larsen(k)) y[k] = (old[k] - dt * rate[k] * inf[k]) / (T(1) - dt * rate[k]);
+    int nl[S];
+    int m = 0;
+    for (int k = 1; k < S; ++k)
+        if (!Model::rush_larsen(k)) nl[m++] = k;
+    if (m == 0) return;
+    const T tol = sizeof(T) == 8 ? T(1e-13) : T(1e-6);
+    const T fd = sizeof(T) == 8 ? T(1e-7) : T(3e-3);
+    T r[S], r2[S], J[S][S], upd[S], yy[S];
+    for (int it = 0; it < 20; ++it) {
+        Model::template rhs<T>(y, stim, cm, p, dy);
+        for (int q = 0; q < m; ++q) r[q] = y[nl[q]] - old[nl[q]] - dt * dy[nl[q]];
+        for (int c = 0; c < m; ++c) {
+            for (int k = 0; k < S; ++k) yy[k] = y[k];
+            const T base = y[nl[c]] < T(0) ? -y[nl[c]] : y[nl[c]];
+            const T hh = fd * (base > T(1e-8) ? base : T(1e-8));
+            yy[nl[c]] += hh;
+            Model::template rhs<T>(yy, stim, cm, p, dy);
+            for (int q = 0; q < m; ++q) r2[q] = yy[nl[q]] - old[nl[q]] - dt * dy[nl[q]];
+            for (int q = 0; q < m; ++q) J[q][c] = (r2[q] - r[q]) / hh;
+        }
+        for (int i = 0; i < m; ++i)
+            for (int ii = i + 1; ii < m; ++ii) {
+                const T fact = J[ii][i] / J[i][i];
+                for (int j = i; j < m; ++j) J[ii][j] -= fact * J[i][j];
+                r[ii] -= fact * r[i];
+            }
+        bool done = true;
+        for (int i = m; i-- > 0;) {
+            upd[i] = r[i];
+            for (int j = i + 1; j < m; ++j) upd[i] -= J[i][j] * upd[j];
+            upd[i] /= J[i][i];
+        }
+        for (int q = 0; q < m; ++q) {
+            y[nl[q]] -= upd[q];
+            const T a = upd[q] < T(0) ? -upd[q] : upd[q];
+            const T b = y[nl[q]] < T(0) ? -y[nl[q]] : y[nl[q]];
+            if (a > tol * (b > T(1) ? b : T(1))) done = false;
+        }
+        if (done) break;
+    }
+}
+
 template <class Model, typename T>
 CHB_HD bool states_in_range(const T* y) {
     bool ok = true;

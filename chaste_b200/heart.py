@@ -211,6 +211,15 @@ def CellTenTusscher2006EpiFromCellML(stimulus=None, solver="RushLarsen"):
     return CellSpec(N.MODEL_TT06, stimulus or ZeroStimulus(), solver)
 
 
+def CellLuoRudy1991FromCellMLBackwardEuler(stimulus=None):
+    """The backward-Euler variant chaste_codegen generates (CellLuoRudy1991FromCellMLBackwardEuler)."""
+    return CellLuoRudy1991FromCellML(stimulus, "BackwardEuler")
+
+
+def CellTenTusscher2006EpiFromCellMLBackwardEuler(stimulus=None):
+    return CellTenTusscher2006EpiFromCellML(stimulus, "BackwardEuler")
+
+
 class AbstractCardiacCellFactory:
     """Per-node cell creation (AbstractCardiacCellFactory.cpp:42-67)."""
 
@@ -358,7 +367,8 @@ class MonodomainProblem:
         if len(models) != 1 or len(solvers) != 1:
             raise ValueError("a GPU tissue runs one cell model with one ODE solver")
         cfg.model = models.pop()
-        cfg.ode_method = N.ODE_RUSH_LARSEN if solvers.pop() == "RushLarsen" else N.ODE_FORWARD_EULER
+        cfg.ode_method = {"RushLarsen": N.ODE_RUSH_LARSEN,
+                          "BackwardEuler": N.ODE_BACKWARD_EULER}.get(solvers.pop(), N.ODE_FORWARD_EULER)
         native = N.Tissue(cfg)
         if self.mesh is None:
             native.set_slab_mesh(dim, hc.slab[3], hc.slab[0], hc.slab[1], hc.slab[2], hc.sigma)

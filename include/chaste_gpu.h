@@ -46,7 +46,10 @@ typedef enum {
 } cg_status;
 
 enum { CG_MODEL_LR91 = 0, CG_MODEL_TT06 = 1 };
-enum { CG_ODE_FORWARD_EULER = 0, CG_ODE_RUSH_LARSEN = 1 };
+/* Forward Euler (EulerIvpOdeSolver), Rush-Larsen (AbstractRushLarsenCardiacCell) or
+ * backward Euler (AbstractBackwardEulerCardiacCell: implicit steps for the states
+ * linear in themselves, Newton for the rest). */
+enum { CG_ODE_FORWARD_EULER = 0, CG_ODE_RUSH_LARSEN = 1, CG_ODE_BACKWARD_EULER = 2 };
 enum { CG_PC_NONE = 0, CG_PC_JACOBI = 1, CG_PC_BJACOBI = 2 };
 enum { CG_PRECISION_FP64 = 0, CG_PRECISION_MIXED = 1 };
 enum { CG_STIM_NONE = 0, CG_STIM_SIMPLE = 1, CG_STIM_REGULAR = 2 };
@@ -182,9 +185,15 @@ const char* cg_status_string(int status);
 typedef struct cg_batch cg_batch;
 int cg_batch_create(int model, int n_cells, const int* beats, const double* params, const cg_stimulus* stim,
                     double dt, double beat_length, int max_aps, int device, cg_batch** out);
-/* Times each candidate block size on `steps` steps and keeps the fastest;
- * the population is reset to its initial state afterwards. */
+/* Times each candidate launch shape -- threads per block (32, 64, 128, 256) x
+ * cells advanced together by each thread (1, 2) -- on `steps` steps and keeps the
+ * fastest; the population is reset to its initial state afterwards. */
 int cg_batch_autotune(cg_batch* b, int steps, int* threads_per_block);
+/* Set the launch shape (threads per block a multiple of 32 up to 1024, cells per
+ * thread 1 or 2) without timing; results do not depend on it. */
+int cg_batch_set_launch_shape(cg_batch* b, int threads_per_block, int cells_per_thread);
+/* The launch shape in use (after cg_batch_autotune, or the default 64 x 1). */
+int cg_batch_launch_shape(const cg_batch* b, int* threads_per_block, int* cells_per_thread);
 /* Runs every beat (one CUDA-graph replay per beat); ms = device time. */
 int cg_batch_run(cg_batch* b, double* ms);
 /* apd64/apd32: n_cells x max_aps (-1 where no AP), n_ap: APs completed per cell,

@@ -18,7 +18,7 @@ extern "C" {
 #endif
 
 enum { ORC_LR91 = 0, ORC_TT06 = 1 };
-enum { ORC_FE = 0, ORC_RL = 1 };
+enum { ORC_FE = 0, ORC_RL = 1, ORC_BE = 2 };   /* BE: operator-splitting tissues only */
 enum { ORC_PC_NONE = 0, ORC_PC_JACOBI = 1, ORC_PC_BJACOBI = 2 };
 enum { ORC_STIM_NONE = 0, ORC_STIM_SIMPLE = 1, ORC_STIM_REGULAR = 2 };
 /* MonodomainSolver (default) or OperatorSplittingMonodomainSolver */

@@ -78,10 +78,26 @@ static void rl_except_voltage(double* y, const double* p, const orc_stimulus* st
     }
 }
 
+// AbstractBackwardEulerCardiacCell::ComputeExceptVoltage (heart/src/odes/
+// AbstractBackwardEulerCardiacCell.hpp): n = (t1 - t0)/dt + 0.5 steps at times
+// t0 + i dt, each ComputeOneStepExceptVoltage with V fixed.
+template <class M>
+static void be_except_voltage(double* y, const double* p, const orc_stimulus* stim,
+                              double am_div, double cm, double t0, double t1, double dt) {
+    const unsigned n_steps = (unsigned)((t1 - t0) / dt + 0.5);
+    const double v = y[0];
+    for (unsigned i = 0; i < n_steps; ++i) {
+        const double s = stimulus_value(stim, t0 + i * dt) / am_div;
+        chb::be_step<M, double>(y, s, cm, p, dt, false);
+        y[0] = v;
+    }
+}
+
 template <class M>
 void except_voltage(int method, double* y, const double* p, const orc_stimulus* stim,
                     double am_div, double cm, double t0, double t1, double dt) {
     if (method == ORC_RL) rl_except_voltage<M>(y, p, stim, am_div, cm, t0, t1, dt);
+    else if (method == ORC_BE) be_except_voltage<M>(y, p, stim, am_div, cm, t0, t1, dt);
     else fe_except_voltage<M>(y, p, stim, am_div, cm, t0, t1, dt);
 }
 

@@ -399,8 +399,9 @@ static void solve_cells(Tissue& T, double t0, double t1) {
 // SolveCellSystems(..., updateVoltage = true) for the operator-splitting solver
 // (AbstractCardiacTissue.cpp:531-536): every cell's SolveAndUpdateState over
 // [t0, t1] including V -- forward Euler through AbstractOneStepIvpOdeSolver's
-// InternalSolve (ode/src/solver/AbstractOneStepIvpOdeSolver.cpp:115-153), or
-// Rush-Larsen (AbstractRushLarsenCardiacCell.cpp:130-147, V by Euler first) --
+// InternalSolve (ode/src/solver/AbstractOneStepIvpOdeSolver.cpp:115-153), Rush-Larsen
+// (AbstractRushLarsenCardiacCell.cpp:130-147, V by Euler first) or backward Euler
+// (AbstractBackwardEulerCardiacCell.hpp SolveAndUpdateState, chb::be_step) --
 // then V from the cell and UpdateCaches at t1.
 template <class Mdl>
 static void solve_cells_with_voltage(Tissue& T, double t0, double t1) {
@@ -423,6 +424,8 @@ static void solve_cells_with_voltage(Tissue& T, double t0, double t1) {
                 const double sv = stimulus_value(st, ts.Time()) / T.cfg.am;   // GetIntracellularAreaStimulus
                 if (T.cfg.ode_method == ORC_RL) {
                     chb::rl_step<Mdl, double>(y, sv, T.cfg.cm, p, T.cfg.dt_ode);
+                } else if (T.cfg.ode_method == ORC_BE) {
+                    chb::be_step<Mdl, double>(y, sv, T.cfg.cm, p, T.cfg.dt_ode, true);
                 } else {
                     const double h = ts.NextStep();
                     Mdl::template rhs<double>(y, sv, T.cfg.cm, p, dy);

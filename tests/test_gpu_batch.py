@@ -51,3 +51,18 @@ def test_population_matches_oracle_cells(N, oracle):
         assert np.max(np.abs(r["apd64"][cell, :k] - r["apd32"][cell, :k])) <= 1.0
     dv = r["max_dv"][np.arange(n)[:, None], np.arange(b.max_beats)[None, :]]
     assert np.all(np.isfinite(dv))
+
+
+def test_cells_per_thread_do_not_change_results(N):
+    """Two cells per thread (interleaved in one step loop) give bitwise the results of
+    one cell per thread, for an odd population that leaves partial groups."""
+    params, beats = population(37, seed=7, max_beats=2)
+    out = []
+    for tpb, cpt in ((64, 1), (32, 2)):
+        b = N.CellBatch(N.MODEL_TT06, beats, params)
+        b.set_launch_shape(tpb, cpt)
+        assert b.launch_shape() == (tpb, cpt)
+        b.run()
+        out.append(b.results())
+    for key in ("apd64", "apd32", "states64", "states32", "max_dv", "n_ap64", "n_ap32"):
+        assert np.array_equal(out[0][key], out[1][key]), key

@@ -133,6 +133,46 @@ def test_operator_splitting_parity(N, oracle, case_name):
     assert float(np.max(np.abs(m.voltage() - g.voltage()))) <= 0.5
 
 
+def test_operator_splitting_backward_euler_known_answer_on_gpu(N):
+    """TestOperatorSplittingMonodomainSolver.hpp:102-146 through the GPU: 1D slab of
+    101 nodes, backward-Euler LR91 cells, ODE/PDE steps 0.005/0.01 ms, 4 ms,
+    -1e6 uA/cm^3 for 0.5 ms on x <= 0.02: V at node 30 is 5.0567 (+- 1e-3)."""
+    cfg = N.default_config()
+    cfg.model, cfg.ode_method = N.MODEL_LR91, N.ODE_BACKWARD_EULER
+    cfg.ode_time_step, cfg.pde_time_step = 0.005, 0.01
+    cfg.use_absolute_tolerance, cfg.ksp_tolerance = 1, 2e-4
+    cfg.ksp_preconditioner = N.PC_JACOBI
+    cfg.solver = N.SOLVER_OPERATOR_SPLITTING
+    t = N.Tissue(cfg)
+    t.set_slab_mesh(1, 0.01, 1.0, 0.0, 0.0, sigma=(1.75, 1.75, 1.75))
+    t.set_cells()
+    x = np.arange(t.n) * 0.01
+    t.set_stimulus(np.where(np.abs(x) < 0.02 + 1e-6, 0, -1).astype(np.int32),
+                   [N.stimulus(N.STIM_SIMPLE, -1e6, 0.5, 0.0)])
+    t.step(400)
+    assert abs(t.voltage()[30] - 5.0567) <= 1e-3
+
+
+@pytest.mark.parametrize("solver,case_name", [(0, "LR91_2D"), (1, "LR91_2D"), (0, "TT06_3D")])
+def test_backward_euler_cells_parity(N, oracle, solver, case_name):
+    """Backward-Euler cells on the GPU (FP64) against the oracle, with V clamped
+    (default solver) and with V (operator splitting)."""
+    case = dict(getattr(TC, case_name))
+    case.update(method=2, solver=solver)
+    g, _ = TC.make_gpu(N, **case)
+    o, _ = TC.make_oracle(oracle, **case)
+    worst = 0.0
+    for _ in range(5):
+        g.step(4)
+        o.step(4)
+        vo = o.voltage()
+        worst = max(worst, float(np.max(np.abs(g.voltage() - vo) / np.maximum(np.abs(vo), 1.0))))
+    assert worst <= FP64_RTOL, worst
+    m, _ = TC.make_gpu(N, precision=1, **case)
+    m.step(20)
+    assert float(np.max(np.abs(m.voltage() - g.voltage()))) <= 0.5
+
+
 def test_snapshot_restore_is_bitwise(N):
     case = dict(TC.LR91_2D)
     a, _ = TC.make_gpu(N, **case)

@@ -150,3 +150,21 @@ def test_operator_splitting_against_the_default_solver(oracle):
     away = normal > -80.0
     assert away.any() and np.all(normal[away] != split[away])
     assert normal.max() > 0.0
+
+
+def test_operator_splitting_with_backward_euler_cells_known_answer(oracle):
+    """TestOperatorSplittingMonodomainSolver.hpp:102-146: with CellLuoRudy1991FromCellML
+    BackwardEulerOpt cells, V at node 30 after 4 ms is 5.0567 (+- 1e-3)."""
+    import numpy as np
+
+    O = oracle
+    n, h = 101, 0.01
+    xyz = np.zeros((n, 3))
+    xyz[:, 0] = np.arange(n) * h
+    conn = np.stack([np.arange(n - 1), np.arange(1, n)], 1).astype(np.int32)
+    sig = np.full((n - 1, 1), 1.75)
+    sid = np.where(np.abs(xyz[:, 0]) < 0.02 + 1e-6, 0, -1).astype(np.int32)
+    cfg = O.Config(0, O.BE, 0.005, 0.01, 1400.0, 1.0, O.PC_JACOBI, 1, 2e-4, 0, 10000, 1)
+    t = O.Tissue(cfg, 1, xyz, conn, sig, sid, [O.simple(-1e6, 0.5)])
+    t.step(400)
+    assert abs(t.voltage()[30] - 5.0567) <= 1e-3
