@@ -48,7 +48,7 @@ class Config(C.Structure):
         ("use_absolute_tolerance", C.c_int), ("ksp_tolerance", C.c_double),
         ("use_mass_lumping", C.c_int), ("max_iterations", C.c_int), ("precision", C.c_int),
         ("device", C.c_int), ("check_state_ranges", C.c_int), ("activation_threshold", C.c_double),
-        ("solver", C.c_int),
+        ("solver", C.c_int), ("use_state_variable_interpolation", C.c_int),
     ]
 
 

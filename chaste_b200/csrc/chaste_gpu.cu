@@ -16,6 +16,7 @@
 #include "kernels/cg.cuh"
 #include "kernels/cg_mixed.cuh"
 #include "kernels/ode.cuh"
+#include "kernels/svi.cuh"
 
 using namespace chb;
 
@@ -52,6 +53,13 @@ struct cg_ctx {
     // device arrays
     double* d_V = nullptr;
     double* d_Vprev = nullptr;    // mixed precision: V of the previous step (extrapolated CG guess)
+    // state-variable interpolation: element nodes, weights, node -> elements, correction
+    int* d_econn = nullptr;
+    double* d_ewj = nullptr;
+    int* d_nptr = nullptr;
+    int* d_nel = nullptr;
+    double* d_corr = nullptr;
+    bool svi = false;
     void* d_states = nullptr;     // (S-1) x n of T
     void* d_iion = nullptr;
     void* d_z = nullptr;
@@ -254,6 +262,10 @@ int cg_create(const cg_config* cfg, cg_ctx** out) {
     if (cfg->ksp_preconditioner != CG_PC_NONE && cfg->ksp_preconditioner != CG_PC_JACOBI) return CG_ERR_ARG;
     if (cfg->precision != CG_PRECISION_FP64 && cfg->precision != CG_PRECISION_MIXED) return CG_ERR_ARG;
     if (cfg->solver != CG_SOLVER_MONODOMAIN && cfg->solver != CG_SOLVER_OPERATOR_SPLITTING) return CG_ERR_ARG;
+    if (cfg->use_state_variable_interpolation != 0 && cfg->use_state_variable_interpolation != 1) return CG_ERR_ARG;
+    // Chaste's operator-splitting solver has no correction-term assembler
+    if (cfg->use_state_variable_interpolation && cfg->solver == CG_SOLVER_OPERATOR_SPLITTING)
+        return CG_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -528,6 +540,49 @@ int upload_operator(cg_ctx* c) {
     return alloc_vectors(c);
 }
 
+// Element data for state-variable interpolation: node lists, |det J| times the
+// order-2 rule's reference weight, and each node's elements in ascending order.
+int setup_svi(cg_ctx* c, int dim, int n, const double* xyz, int n_elems, const int* conn) {
+    const int nb = dim + 1;
+    const double wref = dim == 1 ? 0.5 : (dim == 2 ? 1.0 / 6.0 : 1.0 / 24.0);
+    std::vector<double> wj(n_elems);
+    for (int e = 0; e < n_elems; ++e) {
+        const double* x0 = &xyz[(size_t)conn[e * nb] * 3];
+        double d[3][3] = {{0}};
+        for (int a = 1; a < nb; ++a)
+            for (int k = 0; k < 3; ++k) d[a - 1][k] = xyz[(size_t)conn[e * nb + a] * 3 + k] - x0[k];
+        double det;
+        if (dim == 1) det = d[0][0];
+        else if (dim == 2) det = d[0][0] * d[1][1] - d[0][1] * d[1][0];
+        else
+            det = d[0][0] * (d[1][1] * d[2][2] - d[1][2] * d[2][1]) - d[0][1] * (d[1][0] * d[2][2] - d[1][2] * d[2][0]) +
+                  d[0][2] * (d[1][0] * d[2][1] - d[1][1] * d[2][0]);
+        wj[e] = std::fabs(det) * wref;
+    }
+    std::vector<int> nptr(n + 1, 0), nel;
+    for (int e = 0; e < n_elems; ++e)
+        for (int a = 0; a < nb; ++a) nptr[conn[e * nb + a] + 1]++;
+    for (int i = 0; i < n; ++i) nptr[i + 1] += nptr[i];
+    nel.resize(nptr[n]);
+    std::vector<int> fill(nptr.begin(), nptr.end() - 1);
+    for (int e = 0; e < n_elems; ++e)
+        for (int a = 0; a < nb; ++a) nel[fill[conn[e * nb + a]]++] = e;
+    cudaStream_t s = c->stream;
+    CG_TRY(dalloc(c, &c->d_econn, (size_t)n_elems * nb * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_ewj, (size_t)n_elems * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_nptr, (size_t)(n + 1) * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_nel, (size_t)std::max<int>(1, (int)nel.size()) * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_corr, (size_t)n * sizeof(double)));
+    CG_CUDA(cudaMemcpyAsync(c->d_econn, conn, (size_t)n_elems * nb * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(c->d_ewj, wj.data(), wj.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(c->d_nptr, nptr.data(), nptr.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(c->d_nel, nel.data(), nel.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemsetAsync(c->d_corr, 0, (size_t)n * sizeof(double), s));
+    CG_CUDA(cudaStreamSynchronize(s));
+    c->svi = true;
+    return CG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -544,6 +599,7 @@ int cg_set_mesh(cg_ctx* c, int n_nodes, int dim, const double* xyz, int n_elems,
     if (!assemble(dim, n_nodes, xyz, n_elems, conn, sigma, mass_scale, c->cfg.use_mass_lumping != 0, c->csr))
         return CG_ERR_ARG;
     CG_TRY(upload_operator(c));
+    if (c->cfg.use_state_variable_interpolation) CG_TRY(setup_svi(c, dim, n_nodes, xyz, n_elems, conn));
     c->have_mesh = true;
     return CG_OK;
 }
@@ -576,6 +632,8 @@ int cg_set_slab_mesh(cg_ctx* c, int dim, double h, double width, double height, 
         std::swap(c->csr, empty);
     }
     CG_TRY(upload_operator(c));
+    if (c->cfg.use_state_variable_interpolation)
+        CG_TRY(setup_svi(c, dim, c->n, xyz.data(), n_elems, conn.data()));
     c->have_mesh = true;
     if (n_nodes_out) *n_nodes_out = c->n;
     return CG_OK;
@@ -668,7 +726,8 @@ void launch_ode(cg_ctx* c, int half = 0) {
     OdeArgs<T> a;
     a.n = c->n;
     a.V = c->d_V;
-    a.vprev = c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING ? nullptr : c->d_Vprev;
+    // the extrapolated guess replaces V^n in place, which splitting and SVI still need
+    a.vprev = (c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING || c->svi) ? nullptr : c->d_Vprev;
     a.half = half;
     a.states = (T*)c->d_states;
     a.iion = (T*)c->d_iion;
@@ -726,6 +785,7 @@ CgArgs make_cg_args(cg_ctx* c) {
     a.zrhs = c->mixed() ? nullptr : (const double*)c->d_z;
     a.zrhs32 = c->mixed() ? (const float*)c->d_z : nullptr;
     a.cls8 = c->d_cls8;
+    a.corr = c->svi ? c->d_corr : nullptr;
     a.r = c->d_r;
     a.zp = c->d_zp;
     a.p0 = c->d_p;
@@ -786,10 +846,59 @@ void launch_odes(cg_ctx* c, int half) {
 
 bool split(const cg_ctx* c) { return c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING; }
 
+template <class M, typename T>
+void launch_svi_t(cg_ctx* c) {
+    SviArgs<T> a;
+    a.n = c->n;
+    a.dim = c->dim;
+    a.V = c->d_V;
+    a.states = (const T*)c->d_states;
+    a.iion = (const T*)c->d_iion;
+    a.pset = c->d_pset;
+    a.params = (const T*)c->d_params;
+    a.econn = c->d_econn;
+    a.ewj = c->d_ewj;
+    a.nptr = c->d_nptr;
+    a.nel = c->d_nel;
+    a.corr = c->d_corr;
+    a.am = c->cfg.surface_area_to_volume_ratio;
+    a.cm = c->cfg.capacitance;
+    // order-2 Gaussian rules: quadrature point q has basis value qa at node big[q]
+    if (c->dim == 1) {
+        const double r = std::sqrt(1.0 / 3.0);
+        a.qa = (r + 1.0) / 2.0, a.qb = (-r + 1.0) / 2.0;
+        a.big[0] = 0, a.big[1] = 1, a.big[2] = a.big[3] = 0;
+    } else if (c->dim == 2) {
+        a.qa = 2.0 / 3.0, a.qb = 1.0 / 6.0;
+        a.big[0] = 1, a.big[1] = 0, a.big[2] = 2, a.big[3] = 0;
+    } else {
+        const double sf = 1.0 / std::sqrt(5.0);
+        a.qa = (1.0 + 3.0 * sf) / 4.0, a.qb = (1.0 - sf) / 4.0;
+        a.big[0] = 1, a.big[1] = 2, a.big[2] = 3, a.big[3] = 0;
+    }
+    svi_kernel<M, T><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+}
+
+void launch_svi(cg_ctx* c) {
+    const bool tt = c->cfg.model == CG_MODEL_TT06;
+    if (c->mixed()) {
+        if (tt) launch_svi_t<TenTusscher2006Epi, float>(c);
+        else launch_svi_t<LuoRudy1991, float>(c);
+    } else {
+        if (tt) launch_svi_t<TenTusscher2006Epi, double>(c);
+        else launch_svi_t<LuoRudy1991, double>(c);
+    }
+}
+
 cudaError_t launch_step(cg_ctx* c) {
     launch_odes(c, split(c) ? 1 : 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (c->svi) {
+        launch_svi(c);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     e = launch_cg(c);
     if (e != cudaSuccess || !split(c)) return e;
     launch_odes(c, 2);
@@ -1140,6 +1249,7 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
         cudaEventRecord(e[0], c->stream);
         launch_odes(c, split(c) ? 1 : 0);
         cudaEventRecord(e[1], c->stream);
+        if (c->svi) launch_svi(c);   // part of assembling the RHS (ASSEMBLE_RHS)
         if (cudaGetLastError() != cudaSuccess || launch_cg(c) != cudaSuccess) rc = CG_ERR_CUDA;
         cudaEventRecord(e[2], c->stream);
         if (split(c)) launch_odes(c, 2);

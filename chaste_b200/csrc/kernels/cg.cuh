@@ -44,6 +44,7 @@ struct CgArgs {
     const double* zrhs;         // per-node RHS term z (FP64 path, haloed)
     const float* zrhs32;        // z (mixed path, haloed)
     const uint8_t* cls8;        // slab class per node
+    const double* corr;         // state-variable interpolation correction added to b = M z (or null)
     double* r;
     double* zp;                 // preconditioned residual B r (haloed)
     double* p0;                 // search direction
@@ -130,7 +131,7 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
         double v[4] = {0, 0, 0, 0};
         for (int i = t0; i < n; i += stride) {
             const int c = class_of<SLAB>(a, i);
-            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs);
+            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs) + (a.corr ? a.corr[i] : 0.0);
             const double av = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, x);
             const double rr = b - av;
             const double d = dinv_of<SLAB>(a, sh, c, i);
@@ -152,7 +153,7 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
         double v[2] = {0, 0};
         for (int i = t0; i < n; i += stride) {
             const int c = class_of<SLAB>(a, i);
-            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs);
+            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs) + (a.corr ? a.corr[i] : 0.0);
             const double zz = dinv_of<SLAB>(a, sh, c, i) * b;
             x[i] = 0.0;
             r[i] = b;

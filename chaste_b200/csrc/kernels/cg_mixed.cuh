@@ -84,7 +84,7 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
         double v[4] = {0, 0, 0, 0};
         for (int i = t0; i < n; i += stride) {
             const int c = class_of<SLAB>(a, i);
-            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs32);
+            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs32) + (a.corr ? a.corr[i] : 0.0);
             const double av = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, x);
             const double rr = b - av;
             const double d = dinv_of<SLAB>(a, sh, c, i);
@@ -375,7 +375,7 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
             r[k] = u[k] = 0.0f;
             if (!on[k]) continue;
             const int i = node[k], c = cls[k];
-            const double b = apply_row<true, NOFF, true>(a, sh, nullptr, c, i, a.zrhs32);
+            const double b = apply_row<true, NOFF, true>(a, sh, nullptr, c, i, a.zrhs32) + (a.corr ? a.corr[i] : 0.0);
             const double av = apply_row<true, NOFF, false>(a, sh, nullptr, c, i, x);
             const double rr = b - av;
             const double d = dinv_of<true>(a, sh, c, i);

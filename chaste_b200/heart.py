@@ -64,6 +64,7 @@ class HeartConfig:
         self.check_state_ranges = False
         self.device = 0
         self.operator_splitting = False
+        self.state_variable_interpolation = False
 
     # HeartConfig.cpp:1581-1587, 2337
     def SetOdeTimeStep(self, dt):
@@ -135,6 +136,14 @@ class HeartConfig:
 
     def GetUseReactionDiffusionOperatorSplitting(self):
         return self.operator_splitting
+
+    # HeartConfig::SetUseStateVariableInterpolation (MonodomainSolver.cpp:200-209 then
+    # adds MonodomainCorrectionTermAssembler's vector to the RHS at :122-126)
+    def SetUseStateVariableInterpolation(self, flag=True):
+        self.state_variable_interpolation = bool(flag)
+
+    def GetUseStateVariableInterpolation(self):
+        return self.state_variable_interpolation
 
     def SetFibreLength(self, length, h):
         self.space_dimension, self.slab = 1, (length, 0.0, 0.0, h)
@@ -341,6 +350,7 @@ class MonodomainProblem:
         cfg.check_state_ranges = 1 if hc.check_state_ranges else 0
         cfg.device = hc.device
         cfg.solver = N.SOLVER_OPERATOR_SPLITTING if hc.operator_splitting else N.SOLVER_MONODOMAIN
+        cfg.use_state_variable_interpolation = int(hc.state_variable_interpolation)
         return cfg
 
     def Initialise(self):

@@ -78,6 +78,9 @@ typedef struct {
     int check_state_ranges;    /* 1: device-side VerifyStateVariables analogue */
     double activation_threshold; /* mV; activation time = first step with V above it */
     int solver;                /* CG_SOLVER_* (default CG_SOLVER_MONODOMAIN) */
+    int use_state_variable_interpolation; /* 1: SVI correction of the RHS
+                                  (HeartConfig::SetUseStateVariableInterpolation,
+                                  MonodomainCorrectionTermAssembler); default solver only */
 } cg_config;
 
 /* SimpleStimulus (heart/src/stimulus/SimpleStimulus.cpp:44-76) / RegularStimulus

@@ -83,6 +83,7 @@ typedef struct {
     int mass_lumping;
     int max_iterations;   /* PETSc default 10000 */
     int solver;           /* ORC_SOLVER_* */
+    int svi;              /* 1: state-variable interpolation (HeartConfig::SetUseStateVariableInterpolation) */
 } orc_config;
 
 typedef struct orc_tissue orc_tissue;

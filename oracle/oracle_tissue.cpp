@@ -235,6 +235,8 @@ struct Tissue {
     std::vector<double> ilu;                  // ILU(0) factors in A's pattern
     std::vector<int> ilu_diag;
     std::vector<double> b, z, r, p, w, x;
+    std::vector<int> conn;                    // kept for state-variable interpolation
+    std::vector<double> detj;                 // |det J| per element
     double t = 0.0;
     long long steps = 0;
 };
@@ -468,6 +470,62 @@ static int step_split(Tissue& T, int* iters) {
     return 0;
 }
 
+// State-variable interpolation: MonodomainCorrectionTermAssembler::ComputeVectorTerm
+// (heart/src/solver/electrics/monodomain/MonodomainCorrectionTermAssembler.cpp:47-66)
+// on the elements AbstractCorrectionTermAssembler::ElementAssemblyCriterion selects
+// (heart/src/solver/electrics/AbstractCorrectionTermAssembler.cpp:109-146: largest
+// |Iion_a - Iion_b| over the element's nodes above 1), with the order-2 Gaussian rule
+// (pde/src/solver/GaussianQuadratureRule.cpp) -- at quadrature point q one node has
+// basis value A and the others B -- accumulated element by element onto b.
+template <class Mdl>
+static void svi_correction(Tissue& T, double* b) {
+    constexpr int S = Mdl::kNumStates;
+    const int nb = T.dim + 1;
+    const int ne = (int)T.detj.size();
+    double A, B, wref;
+    int big[4];
+    if (T.dim == 1) {
+        const double r = std::sqrt(1.0 / 3.0);
+        A = (r + 1.0) / 2.0;       // basis 1 - xi at xi = (1 - r)/2
+        B = (-r + 1.0) / 2.0;
+        wref = 0.5;
+        big[0] = 0, big[1] = 1;
+    } else if (T.dim == 2) {
+        A = 2.0 / 3.0, B = 1.0 / 6.0, wref = 1.0 / 6.0;
+        big[0] = 1, big[1] = 0, big[2] = 2;
+    } else {
+        const double sf = 1.0 / std::sqrt(5.0);
+        A = (1.0 + 3.0 * sf) / 4.0, B = (1.0 - sf) / 4.0, wref = 1.0 / 24.0;
+        big[0] = 1, big[1] = 2, big[2] = 3, big[3] = 0;
+    }
+    double pdef[16];
+    for (int k = 0; k < T.np; ++k) pdef[k] = 1.0;
+    for (int e = 0; e < ne; ++e) {
+        const int* nd = &T.conn[(size_t)e * nb];
+        double di = 0.0;
+        for (int x = 0; x < nb; ++x)
+            for (int y = x + 1; y < nb; ++y) di = std::max(di, std::fabs(T.iion[nd[x]] - T.iion[nd[y]]));
+        if (!(di > 1.0)) continue;
+        const double wj = T.detj[e] * wref;
+        const double* p = pdef;
+        if (!T.param_id.empty() && T.param_id[nd[0]] >= 0) p = &T.param_table[(size_t)T.param_id[nd[0]] * T.np];
+        double be[4] = {0, 0, 0, 0};
+        for (int q = 0; q < nb; ++q) {
+            double phi[4], y[S], iint = 0.0;
+            for (int j = 0; j < nb; ++j) phi[j] = j == big[q] ? A : B;
+            for (int k = 0; k < S; ++k) y[k] = 0.0;
+            for (int j = 0; j < nb; ++j) {
+                iint += phi[j] * T.iion[nd[j]];
+                const double* sj = &T.states[(size_t)nd[j] * T.ns];
+                for (int k = 0; k < S; ++k) y[k] += phi[j] * sj[k];
+            }
+            const double isv = Mdl::template iionic<double>(y, T.cfg.cm, p);
+            for (int i = 0; i < nb; ++i) be[i] += phi[i] * (-T.cfg.am) * (isv - iint) * wj;
+        }
+        for (int i = 0; i < nb; ++i) b[nd[i]] += be[i];
+    }
+}
+
 static int step_once(Tissue& T, int* iters) {
     if (T.cfg.solver == ORC_SOLVER_OPERATOR_SPLITTING) return step_split(T, iters);
     const double t0 = T.t;
@@ -485,6 +543,10 @@ static int step_once(Tissue& T, int* iters) {
         }
     });
     T.M.matvec(zz, T.b.data());
+    if (T.cfg.svi) {
+        if (T.cfg.model == ORC_TT06) svi_correction<chb::TenTusscher2006Epi>(T, T.b.data());
+        else svi_correction<chb::LuoRudy1991>(T, T.b.data());
+    }
     T.x = T.V;
     const int rc = cg_solve(T, T.x.data(), T.b.data(), iters);
     if (rc != 0) return rc;
@@ -626,6 +688,23 @@ orc_tissue* orc_tissue_create(const orc_config* cfg, int dim, int n_nodes, const
     T.M.rp = T.A.rp;
     T.M.ci = T.A.ci;
     T.M.v.assign(T.A.ci.size(), 0.0);
+    if (cfg->svi) {
+        T.conn.assign(conn, conn + (size_t)n_elems * nb);
+        T.detj.resize(n_elems);
+        for (int e = 0; e < n_elems; ++e) {
+            const double* x0 = &xyz[(size_t)conn[e * nb] * 3];
+            double d[3][3] = {{0}};
+            for (int a = 1; a < nb; ++a)
+                for (int s2 = 0; s2 < 3; ++s2) d[a - 1][s2] = xyz[(size_t)conn[e * nb + a] * 3 + s2] - x0[s2];
+            double det;
+            if (dim == 1) det = d[0][0];
+            else if (dim == 2) det = d[0][0] * d[1][1] - d[0][1] * d[1][0];
+            else
+                det = d[0][0] * (d[1][1] * d[2][2] - d[1][2] * d[2][1]) - d[0][1] * (d[1][0] * d[2][2] - d[1][2] * d[2][0]) +
+                      d[0][2] * (d[1][0] * d[2][1] - d[1][1] * d[2][0]);
+            T.detj[e] = std::fabs(det);
+        }
+    }
     // assemble (AbstractFeVolumeIntegralAssembler::DoAssemble, element loop)
     const double mass_scale = cfg->am * cfg->cm / cfg->dt_pde;
     for (int e = 0; e < n_elems; ++e) {

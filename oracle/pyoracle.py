@@ -57,7 +57,8 @@ class Config(C.Structure):
     _fields_ = [("model", C.c_int), ("ode_method", C.c_int), ("dt_ode", C.c_double),
                 ("dt_pde", C.c_double), ("am", C.c_double), ("cm", C.c_double),
                 ("pc", C.c_int), ("use_abs_tol", C.c_int), ("tol", C.c_double),
-                ("mass_lumping", C.c_int), ("max_iterations", C.c_int), ("solver", C.c_int)]
+                ("mass_lumping", C.c_int), ("max_iterations", C.c_int), ("solver", C.c_int),
+                ("svi", C.c_int)]
 
 
 class CableConfig(C.Structure):

@@ -22,6 +22,13 @@ def kats():
 
 
 @pytest.fixture(scope="session")
+def golden_dir():
+    import pathlib
+
+    return pathlib.Path(ROOT) / "tests" / "golden"
+
+
+@pytest.fixture(scope="session")
 def oracle():
     from oracle import pyoracle
 

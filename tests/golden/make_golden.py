@@ -8,6 +8,11 @@ Sources:
   heart/test/data/ionicmodels/TenTusscherValidData.dat       (TestIonicModels.hpp:793-835)
   hard-coded values of heart/test/monodomain/TestMonodomainProblem.hpp
   (:166-218, :226-297, :303-340, :784-974) and TestIonicModels.hpp GetIIonic checks.
+It also copies the Niederer et al. 2011 benchmark activation map Chaste checks in
+heart/test/monodomain/TestNiederer2011BenchmarkSimulation.hpp:278-290
+(heart/test/data/benchmark_data_orig/activation_time_h0.05_dt0.01.dat, one
+activation time in ms per node of the h = 0.05 slab) into
+niederer_activation_h0.05_dt0.01.txt.
 """
 import json
 import os
@@ -87,3 +92,9 @@ here = os.path.dirname(os.path.abspath(__file__))
 with open(os.path.join(here, "chaste_kats.json"), "w") as f:
     json.dump(out, f, indent=1)
 print("wrote chaste_kats.json")
+
+with open(os.path.join(REF, "heart/test/data/benchmark_data_orig/activation_time_h0.05_dt0.01.dat")) as f:
+    act = [float(x) for x in f.read().split()]
+with open(os.path.join(here, "niederer_activation_h0.05_dt0.01.txt"), "w") as f:
+    f.write("".join(f"{a!r}\n" for a in act))
+print(f"wrote niederer_activation_h0.05_dt0.01.txt ({len(act)} nodes)")

@@ -173,6 +173,53 @@ def test_backward_euler_cells_parity(N, oracle, solver, case_name):
     assert float(np.max(np.abs(m.voltage() - g.voltage()))) <= 0.5
 
 
+@pytest.mark.parametrize("method,case_name,use_csr", [(1, "TT06_3D", False), (2, "TT06_3D", True),
+                                                     (0, "LR91_2D", False)])
+def test_state_variable_interpolation_parity(N, oracle, method, case_name, use_csr):
+    """SVI correction on the GPU (FP64, stencil and CSR operators) against the oracle,
+    and a check that it changes the solution (elements on the wavefront qualify)."""
+    case = dict(getattr(TC, case_name))
+    case.update(method=method, svi=1)
+    g, _ = TC.make_gpu(N, use_csr=use_csr, **case)
+    o, _ = TC.make_oracle(oracle, **case)
+    plain, _ = TC.make_gpu(N, **dict(case, svi=0))
+    worst, moved = 0.0, 0.0
+    for _ in range(5):
+        g.step(4)
+        o.step(4)
+        plain.step(4)
+        vg, vo = g.voltage(), o.voltage()
+        worst = max(worst, _cmp(vg, vo))
+        moved = max(moved, float(np.abs(vg - plain.voltage()).max()))
+    assert worst <= FP64_RTOL, worst
+    assert moved > 1e-3, moved
+    m, _ = TC.make_gpu(N, precision=1, **case)
+    m.step(20)
+    assert float(np.max(np.abs(m.voltage() - g.voltage()))) <= 0.5
+
+
+def test_state_variable_interpolation_rejects_operator_splitting(N):
+    cfg = N.default_config()
+    cfg.use_state_variable_interpolation, cfg.solver = 1, N.SOLVER_OPERATOR_SPLITTING
+    with pytest.raises(N.ChasteGpuError) as e:
+        N.Tissue(cfg)
+    assert e.value.status == 10  # CG_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_niederer_benchmark_activation_map(N, golden_dir, precision):
+    """TestNiederer2011BenchmarkSimulation::TestRunOnCoarsestMesh on the GPU: TT06
+    backward-Euler cells with SVI on the h = 0.05 slab for 40 ms; Chaste's activation
+    map within its 1.5e-3 ms (FP64), within 0.05 ms in mixed precision."""
+    gold = np.loadtxt(golden_dir / "niederer_activation_h0.05_dt0.01.txt")
+    t, xyz = TC.make_gpu(N, precision=precision, **TC.NIEDERER)
+    assert t.n == gold.size == xyz.shape[0]
+    act = TC.niederer_activation(t, t.n)
+    assert (act > 0).all()
+    err = float(np.abs(act - gold).max())
+    assert err <= (1.5e-3 if precision == 0 else 0.05), err
+
+
 def test_snapshot_restore_is_bitwise(N):
     case = dict(TC.LR91_2D)
     a, _ = TC.make_gpu(N, **case)

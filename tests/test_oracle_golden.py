@@ -3,6 +3,8 @@ and hard-coded values), extracted into tests/golden/chaste_kats.json."""
 import numpy as np
 import pytest
 
+from tests import tissue_cases as TC
+
 
 def _stim(O, d):
     if d["kind"] == "simple":
@@ -168,3 +170,18 @@ def test_operator_splitting_with_backward_euler_cells_known_answer(oracle):
     t = O.Tissue(cfg, 1, xyz, conn, sig, sid, [O.simple(-1e6, 0.5)])
     t.step(400)
     assert abs(t.voltage()[30] - 5.0567) <= 1e-3
+
+
+def test_oracle_svi_only_corrects_elements_with_current_jumps(oracle):
+    """AbstractCorrectionTermAssembler::ElementAssemblyCriterion: with every node in the
+    same state no element qualifies, so the first step is bitwise the plain one; once a
+    wavefront exists the correction changes the solution."""
+    case = dict(TC.LR91_2D, size=(0.1, 0.1, 0.0))
+    a, _ = TC.make_oracle(oracle, **dict(case, svi=1))
+    b, _ = TC.make_oracle(oracle, **case)
+    a.step(1)
+    b.step(1)
+    assert np.array_equal(a.voltage(), b.voltage())
+    a.step(15)
+    b.step(15)
+    assert float(np.abs(a.voltage() - b.voltage()).max()) > 1e-3

@@ -17,7 +17,7 @@ def slab_stim_ids(xyz, box_hi):
 
 def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
              abs_tol=None, rel_tol=1e-8, precision=0, use_csr=False, param_set=None, param_table=None,
-             init_states=None, max_iterations=10000, solver=0):
+             init_states=None, max_iterations=10000, solver=0, svi=0):
     """A GPU tissue on a regular slab (stencil operator, or CSR through cg_set_mesh when use_csr)."""
     from oracle import pyoracle as O  # mesh generator only: the same node/element order as the library
 
@@ -33,6 +33,7 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
     cfg.precision = precision
     cfg.max_iterations = max_iterations
     cfg.solver = solver
+    cfg.use_state_variable_interpolation = svi
     t = N.Tissue(cfg)
     xyz, conn, _ = O.slab_mesh(dim, h, *size)
     if use_csr:
@@ -46,11 +47,11 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
 
 
 def make_oracle(O, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
-                abs_tol=None, rel_tol=1e-8, param_set=None, param_table=None, init_states=None, solver=0, **_):
+                abs_tol=None, rel_tol=1e-8, param_set=None, param_table=None, init_states=None, solver=0, svi=0, **_):
     xyz, conn, _ = O.slab_mesh(dim, h, *size)
     use_abs = abs_tol is not None
     cfg = O.Config(model, method, dt_ode, dt_pde, am, cm, O.PC_JACOBI, 1 if use_abs else 0,
-                   abs_tol if use_abs else rel_tol, 0, 10000, solver)
+                   abs_tol if use_abs else rel_tol, 0, 10000, solver, svi)
     sig = np.tile(np.asarray(sigma[:dim], float), (conn.shape[0], 1))
     sid = slab_stim_ids(xyz, box_hi)
     return O.Tissue(cfg, dim, xyz, conn, sig, sid, [O.simple(*stim)], param_id=param_set,
@@ -62,3 +63,23 @@ LR91_2D = dict(model=LR91, method=FE, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, si
                sigma=(1.75, 1.75, 1.75), stim=(-5e5, 0.5, 0.0), box_hi=(0.0199, 1e9))
 TT06_3D = dict(model=TT06, method=RL, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01, size=(0.2, 0.07, 0.03),
                sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0), box_hi=(0.03, 0.03, 0.03))
+
+# TestNiederer2011BenchmarkSimulation.hpp:82-157 at h = 0.05, dt = 0.01 (TestRunOnCoarsestMesh)
+NIEDERER = dict(model=TT06, method=2, dt_ode=0.005, dt_pde=0.01, dim=3, h=0.05, size=(2.0, 0.7, 0.3),
+                sigma=(0.17 * 0.62 / (0.17 + 0.62) * 10, 0.019 * 0.24 / (0.019 + 0.24) * 10,
+                       0.019 * 0.24 / (0.019 + 0.24) * 10),
+                stim=(-50000.0, 2.0, 0.0), box_hi=(0.15 + 1e-6,) * 3, am=1400.0, cm=1.0, abs_tol=2e-4, svi=1)
+
+
+def niederer_activation(t, n, printing_steps=10, n_prints=400, printing_dt=0.1):
+    """Activation times as TestNiederer2011BenchmarkSimulation.hpp:161-203 computes
+    them from the printed voltages: linear interpolation to the first V > 0."""
+    act = -np.ones(n)
+    last = np.ones(n)
+    for k in range(1, n_prints + 1):
+        t.step(printing_steps)
+        v = t.voltage()
+        new = (v > 0) & (act < 0)
+        act[new] = (k - v[new] / (v[new] - last[new])) * printing_dt
+        last = np.where(v <= 0, v, last)
+    return act
