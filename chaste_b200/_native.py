@@ -21,7 +21,7 @@ STATUS_NAMES = {
     9: "CG_ERR_NOMEM", 10: "CG_ERR_UNSUPPORTED",
 }
 MODEL_LR91, MODEL_TT06 = 0, 1
-ODE_FORWARD_EULER, ODE_RUSH_LARSEN, ODE_BACKWARD_EULER = 0, 1, 2
+ODE_FORWARD_EULER, ODE_RUSH_LARSEN, ODE_BACKWARD_EULER, ODE_GRL1, ODE_GRL2 = 0, 1, 2, 3, 4
 PC_NONE, PC_JACOBI, PC_BJACOBI = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 STIM_NONE, STIM_SIMPLE, STIM_REGULAR = 0, 1, 2

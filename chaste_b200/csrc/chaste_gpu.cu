@@ -56,9 +56,11 @@ struct cg_ctx {
     // state-variable interpolation: element nodes, weights, node -> elements, correction
     int* d_econn = nullptr;
     double* d_ewj = nullptr;
-    int* d_nptr = nullptr;
-    int* d_nel = nullptr;
+    uint8_t* d_eflag = nullptr;
+    double* d_ebuf = nullptr;
+    int* d_ell = nullptr;
     double* d_corr = nullptr;
+    int n_elems = 0, ell_width = 0;
     bool svi = false;
     void* d_states = nullptr;     // (S-1) x n of T
     void* d_iion = nullptr;
@@ -252,8 +254,7 @@ int cg_create(const cg_config* cfg, cg_ctx** out) {
     if (!cfg || !out) return CG_ERR_ARG;
     *out = nullptr;
     if (cfg->model != CG_MODEL_LR91 && cfg->model != CG_MODEL_TT06) return CG_ERR_ARG;
-    if (cfg->ode_method != CG_ODE_FORWARD_EULER && cfg->ode_method != CG_ODE_RUSH_LARSEN &&
-        cfg->ode_method != CG_ODE_BACKWARD_EULER)
+    if (cfg->ode_method < CG_ODE_FORWARD_EULER || cfg->ode_method > CG_ODE_GRL2)
         return CG_ERR_ARG;
     if (!(cfg->ode_time_step > 0) || !(cfg->pde_time_step > 0)) return CG_ERR_ARG;
     if (!(cfg->surface_area_to_volume_ratio > 0) || !(cfg->capacitance > 0)) return CG_ERR_ARG;
@@ -541,7 +542,8 @@ int upload_operator(cg_ctx* c) {
 }
 
 // Element data for state-variable interpolation: node lists, |det J| times the
-// order-2 rule's reference weight, and each node's elements in ascending order.
+// order-2 rule's reference weight, and each node's (element, local node) entries in
+// ascending element order, stored column-major and padded with -1 (ELL).
 int setup_svi(cg_ctx* c, int dim, int n, const double* xyz, int n_elems, const int* conn) {
     const int nb = dim + 1;
     const double wref = dim == 1 ? 0.5 : (dim == 2 ? 1.0 / 6.0 : 1.0 / 24.0);
@@ -559,26 +561,33 @@ int setup_svi(cg_ctx* c, int dim, int n, const double* xyz, int n_elems, const i
                   d[0][2] * (d[1][0] * d[2][1] - d[1][1] * d[2][0]);
         wj[e] = std::fabs(det) * wref;
     }
-    std::vector<int> nptr(n + 1, 0), nel;
+    if (n_elems > (1 << 28)) return CG_ERR_UNSUPPORTED;   // entries 4e + j stay in int
+    std::vector<int> deg(n, 0);
     for (int e = 0; e < n_elems; ++e)
-        for (int a = 0; a < nb; ++a) nptr[conn[e * nb + a] + 1]++;
-    for (int i = 0; i < n; ++i) nptr[i + 1] += nptr[i];
-    nel.resize(nptr[n]);
-    std::vector<int> fill(nptr.begin(), nptr.end() - 1);
+        for (int a = 0; a < nb; ++a) deg[conn[e * nb + a]]++;
+    int width = 0;
+    for (int i = 0; i < n; ++i) width = std::max(width, deg[i]);
+    std::vector<int> ell((size_t)width * n, -1);
+    std::fill(deg.begin(), deg.end(), 0);
     for (int e = 0; e < n_elems; ++e)
-        for (int a = 0; a < nb; ++a) nel[fill[conn[e * nb + a]]++] = e;
+        for (int a = 0; a < nb; ++a) {
+            const int i = conn[e * nb + a];
+            ell[(size_t)deg[i]++ * n + i] = 4 * e + a;
+        }
     cudaStream_t s = c->stream;
     CG_TRY(dalloc(c, &c->d_econn, (size_t)n_elems * nb * sizeof(int)));
     CG_TRY(dalloc(c, &c->d_ewj, (size_t)n_elems * sizeof(double)));
-    CG_TRY(dalloc(c, &c->d_nptr, (size_t)(n + 1) * sizeof(int)));
-    CG_TRY(dalloc(c, &c->d_nel, (size_t)std::max<int>(1, (int)nel.size()) * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_eflag, (size_t)n_elems));
+    CG_TRY(dalloc(c, &c->d_ebuf, (size_t)n_elems * 4 * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_ell, std::max<size_t>(1, ell.size()) * sizeof(int)));
     CG_TRY(dalloc(c, &c->d_corr, (size_t)n * sizeof(double)));
     CG_CUDA(cudaMemcpyAsync(c->d_econn, conn, (size_t)n_elems * nb * sizeof(int), cudaMemcpyHostToDevice, s));
     CG_CUDA(cudaMemcpyAsync(c->d_ewj, wj.data(), wj.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    CG_CUDA(cudaMemcpyAsync(c->d_nptr, nptr.data(), nptr.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-    CG_CUDA(cudaMemcpyAsync(c->d_nel, nel.data(), nel.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(c->d_ell, ell.data(), ell.size() * sizeof(int), cudaMemcpyHostToDevice, s));
     CG_CUDA(cudaMemsetAsync(c->d_corr, 0, (size_t)n * sizeof(double), s));
     CG_CUDA(cudaStreamSynchronize(s));
+    c->n_elems = n_elems;
+    c->ell_width = width;
     c->svi = true;
     return CG_OK;
 }
@@ -749,6 +758,10 @@ void launch_ode(cg_ctx* c, int half = 0) {
         ode_kernel<M, T, 1><<<c->ode_blocks, 256, 0, c->stream>>>(a);
     else if (c->cfg.ode_method == CG_ODE_BACKWARD_EULER)
         ode_kernel<M, T, 2><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+    else if (c->cfg.ode_method == CG_ODE_GRL1)
+        ode_kernel<M, T, 3><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+    else if (c->cfg.ode_method == CG_ODE_GRL2)
+        ode_kernel<M, T, 4><<<c->ode_blocks, 256, 0, c->stream>>>(a);
     else
         ode_kernel<M, T, 0><<<c->ode_blocks, 256, 0, c->stream>>>(a);
 }
@@ -856,10 +869,13 @@ void launch_svi_t(cg_ctx* c) {
     a.iion = (const T*)c->d_iion;
     a.pset = c->d_pset;
     a.params = (const T*)c->d_params;
+    a.n_elems = c->n_elems;
     a.econn = c->d_econn;
     a.ewj = c->d_ewj;
-    a.nptr = c->d_nptr;
-    a.nel = c->d_nel;
+    a.flag = c->d_eflag;
+    a.ebuf = c->d_ebuf;
+    a.ell = c->d_ell;
+    a.ell_width = c->ell_width;
     a.corr = c->d_corr;
     a.am = c->cfg.surface_area_to_volume_ratio;
     a.cm = c->cfg.capacitance;
@@ -876,7 +892,9 @@ void launch_svi_t(cg_ctx* c) {
         a.qa = (1.0 + 3.0 * sf) / 4.0, a.qb = (1.0 - sf) / 4.0;
         a.big[0] = 1, a.big[1] = 2, a.big[2] = 3, a.big[3] = 0;
     }
-    svi_kernel<M, T><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+    const int eb = (int)std::max(1LL, std::min(((long long)a.n_elems + 255) / 256, (long long)c->ode_blocks * 8));
+    svi_element_kernel<M, T><<<eb, 256, 0, c->stream>>>(a);
+    svi_gather_kernel<<<c->ode_blocks, 256, 0, c->stream>>>(a.n, a.ell_width, a.ell, a.flag, a.ebuf, a.corr);
 }
 
 void launch_svi(cg_ctx* c) {

@@ -46,8 +46,8 @@ __global__ void activation_kernel(int n, const double* __restrict__ V, double* _
 
 // Half a PDE step of every cell including V, for the operator-splitting solver:
 // SolveCellSystems(..., updateVoltage = true) (AbstractCardiacTissue.cpp:531-536) --
-// SolveAndUpdateState over [t0, t0 + dt/2] or [t0 + dt/2, t1] by forward Euler
-// (AbstractOneStepIvpOdeSolver::InternalSolve) or Rush-Larsen
+// SolveAndUpdateState over [t0, t0 + dt/2] or [t0 + dt/2, t1] by forward Euler, GRL1
+// or GRL2 (AbstractOneStepIvpOdeSolver::InternalSolve), backward Euler or Rush-Larsen
 // (AbstractRushLarsenCardiacCell.cpp:130-147), V written back, then UpdateCaches at
 // the end of the half; after the first half z = Am*Cm*V/dt, the diffusion-only
 // right-hand side term (OperatorSplittingMonodomainSolver.cpp:86-89).
@@ -84,6 +84,8 @@ __device__ __forceinline__ void ode_half_step(const OdeArgs<T>& a, double t0, do
             const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
             if (METHOD == 1) rl_step<M, T>(y, s, cm, p, (T)a.dt_ode);
             else if (METHOD == 2) be_step<M, T>(y, s, cm, p, (T)a.dt_ode, true);
+            else if (METHOD == 3) grl1_step<M, T, true>(y, s, cm, p, (T)(ts.next - ts.time));
+            else if (METHOD == 4) grl2_step<M, T, true>(y, s, cm, p, (T)(ts.next - ts.time));
             else fe_step<M, T>(y, s, cm, p, (T)(ts.next - ts.time));
             ts.advance();
         }
@@ -160,6 +162,10 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
                 const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
                 if (METHOD == 1) {
                     rl_step_except_voltage<M, T>(y, s, cm, p, (T)a.dt_ode);
+                } else if (METHOD == 3) {
+                    grl1_step<M, T, false>(y, s, cm, p, (T)(ts.next - ts.time));
+                } else if (METHOD == 4) {
+                    grl2_step<M, T, false>(y, s, cm, p, (T)(ts.next - ts.time));
                 } else {
                     fe_step_except_voltage<M, T>(y, s, cm, p, (T)(ts.next - ts.time));
                 }

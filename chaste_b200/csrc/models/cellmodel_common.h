@@ -10,13 +10,16 @@
 #pragma once
 
 #include <cmath>
+#include <type_traits>
 
 #if defined(__CUDACC__)
 #define CHB_HD __host__ __device__ __forceinline__
 #define CHB_UNROLL _Pragma("unroll")
+#define CHB_NOUNROLL _Pragma("unroll 1")
 #else
 #define CHB_HD inline
 #define CHB_UNROLL
+#define CHB_NOUNROLL
 #endif
 
 #ifndef NAN
@@ -223,6 +226,108 @@ CHB_UNROLL
         }
         if (done) break;
     }
+}
+
+// Generalised Rush-Larsen steps (GRL1IvpOdeSolver::CalculateNextYValue,
+// ode/src/solver/GRL1IvpOdeSolver.cpp:47-93; GRL2IvpOdeSolver::CalculateNextYValue,
+// ode/src/solver/GRL2IvpOdeSolver.cpp:47-119) of a cell whose ODE solver is GRL1 or
+// GRL2: every state is advanced by the exponential step linearised in itself,
+//     y_i' = y_i + f_i / a_i (exp(a_i dt) - 1),  a_i = (f_i(y + delta e_i) - f_i(y)) / delta,
+// or by forward Euler where |a_i| < delta, with delta = 1e-8.  GRL2 takes a half step
+// to the midpoint first, then re-linearises each state at the midpoint with its own
+// component held at the start value.  With VOLT false the voltage derivative is zero
+// (ComputeExceptVoltage's SetVoltageDerivativeToZero), so V and its partial are skipped.
+// In single precision a perturbation of 1e-8 is below the resolution of most states,
+// so the float step perturbs by 2^-10 max(|y_i|, 1e-6) and divides by the perturbation.
+template <typename T>
+CHB_HD T grl_perturbation(T y) {
+    if (sizeof(T) == 8) return T(1.0e-8);
+    const T a = y < T(0) ? -y : y;
+    return T(0.0009765625) * (a > T(1e-6) ? a : T(1e-6));
+}
+
+template <typename T>
+CHB_HD T grl_update(T y, T f, T a, T dt) {
+    const T aa = a < T(0) ? -a : a;
+    return aa < T(1.0e-8) ? y + f * dt : y + (f / a) * (m_exp(a * dt) - T(1));
+}
+
+// Calls f(std::integral_constant<int, i>) for a runtime i in [I, N): a loop over the
+// states that dispatches to straight-line code per state keeps each state's
+// perturbed evaluation (pruned by the compiler to what its own derivative needs)
+// in a block of its own, so that nothing stays live from one state to the next.
+template <int I, int N, class F>
+CHB_HD void dispatch_state(int i, F& f) {
+    if constexpr (I < N) {
+        if (i == I) f(std::integral_constant<int, I>{});
+        else dispatch_state<I + 1, N>(i, f);
+    }
+}
+
+// a_i = (f_i(y + d e_i) - f_i(y)) / d for every integrated state, unrolled: the
+// compiler shares what the perturbed evaluations have in common with f(y).
+template <class Model, typename T, bool VOLT>
+CHB_HD void grl_partials(const T* y, const T* f, T stim, T cm, const T* p, T* a) {
+    constexpr int S = Model::kNumStates;
+CHB_UNROLL
+    for (int i = VOLT ? 0 : 1; i < S; ++i) {
+        T yy[S], g[S];
+CHB_UNROLL
+        for (int k = 0; k < S; ++k) yy[k] = y[k];
+        const T d = grl_perturbation<T>(y[i]);
+        yy[i] = y[i] + d;
+        Model::template rhs<T>(yy, stim, cm, p, g);
+        a[i] = (g[i] - f[i]) / d;
+    }
+}
+
+template <class Model, typename T, bool VOLT>
+CHB_HD void grl1_step(T* y, T stim, T cm, const T* p, T dt) {
+    constexpr int S = Model::kNumStates;
+    T f[S], a[S];
+    Model::template rhs<T>(y, stim, cm, p, f);
+    grl_partials<Model, T, VOLT>(y, f, stim, cm, p, a);
+CHB_UNROLL
+    for (int i = VOLT ? 0 : 1; i < S; ++i) y[i] = grl_update<T>(y[i], f[i], a[i], dt);
+}
+
+template <class Model, typename T, bool VOLT>
+CHB_HD void grl2_step(T* y, T stim, T cm, const T* p, T dt) {
+    constexpr int S = Model::kNumStates;
+    T y0[S], f[S], a[S];
+CHB_UNROLL
+    for (int k = 0; k < S; ++k) y0[k] = y[k];
+    Model::template rhs<T>(y0, stim, cm, p, f);
+    grl_partials<Model, T, VOLT>(y0, f, stim, cm, p, a);
+    T ym[S];
+    ym[0] = y0[0];
+CHB_UNROLL
+    for (int i = VOLT ? 0 : 1; i < S; ++i) ym[i] = grl_update<T>(y0[i], f[i], a[i], T(0.5) * dt);
+    // each state re-linearised at the midpoint with its own component at the start value
+    auto second = [&](auto ic) {
+        constexpr int I = decltype(ic)::value;
+        T yy[S], g[S], h[S];
+CHB_UNROLL
+        for (int k = 0; k < S; ++k) yy[k] = ym[k];
+        yy[I] = y0[I];
+        Model::template rhs<T>(yy, stim, cm, p, g);
+        const T d = grl_perturbation<T>(y0[I]);
+        yy[I] = y0[I] + d;
+        Model::template rhs<T>(yy, stim, cm, p, h);
+        f[I] = g[I];
+        a[I] = (h[I] - g[I]) / d;
+    };
+    // in double precision one block per state (unrolled, the midpoint evaluations of
+    // all states stay live together and spill); in single precision unrolled
+    if (sizeof(T) == 8) {
+CHB_NOUNROLL
+        for (int i = VOLT ? 0 : 1; i < S; ++i) dispatch_state<0, S>(i, second);
+    } else {
+CHB_UNROLL
+        for (int i = VOLT ? 0 : 1; i < S; ++i) dispatch_state<0, S>(i, second);
+    }
+CHB_UNROLL
+    for (int i = VOLT ? 0 : 1; i < S; ++i) y[i] = grl_update<T>(y0[i], f[i], a[i], dt);
 }
 
 template <class Model, typename T>

@@ -46,10 +46,12 @@ typedef enum {
 } cg_status;
 
 enum { CG_MODEL_LR91 = 0, CG_MODEL_TT06 = 1 };
-/* Forward Euler (EulerIvpOdeSolver), Rush-Larsen (AbstractRushLarsenCardiacCell) or
+/* Forward Euler (EulerIvpOdeSolver), Rush-Larsen (AbstractRushLarsenCardiacCell),
  * backward Euler (AbstractBackwardEulerCardiacCell: implicit steps for the states
- * linear in themselves, Newton for the rest). */
-enum { CG_ODE_FORWARD_EULER = 0, CG_ODE_RUSH_LARSEN = 1, CG_ODE_BACKWARD_EULER = 2 };
+ * linear in themselves, Newton for the rest), or the generalised Rush-Larsen
+ * solvers GRL1IvpOdeSolver / GRL2IvpOdeSolver (ode/src/solver/GRL{1,2}IvpOdeSolver.cpp). */
+enum { CG_ODE_FORWARD_EULER = 0, CG_ODE_RUSH_LARSEN = 1, CG_ODE_BACKWARD_EULER = 2,
+       CG_ODE_GRL1 = 3, CG_ODE_GRL2 = 4 };
 enum { CG_PC_NONE = 0, CG_PC_JACOBI = 1, CG_PC_BJACOBI = 2 };
 enum { CG_PRECISION_FP64 = 0, CG_PRECISION_MIXED = 1 };
 enum { CG_STIM_NONE = 0, CG_STIM_SIMPLE = 1, CG_STIM_REGULAR = 2 };

@@ -18,7 +18,9 @@ extern "C" {
 #endif
 
 enum { ORC_LR91 = 0, ORC_TT06 = 1 };
-enum { ORC_FE = 0, ORC_RL = 1, ORC_BE = 2 };   /* BE: operator-splitting tissues only */
+/* cell ODE methods: forward Euler, Rush-Larsen, backward Euler, and the cell's ODE
+ * solver set to GRL1IvpOdeSolver / GRL2IvpOdeSolver */
+enum { ORC_FE = 0, ORC_RL = 1, ORC_BE = 2, ORC_GRL1 = 3, ORC_GRL2 = 4 };
 enum { ORC_PC_NONE = 0, ORC_PC_JACOBI = 1, ORC_PC_BJACOBI = 2 };
 enum { ORC_STIM_NONE = 0, ORC_STIM_SIMPLE = 1, ORC_STIM_REGULAR = 2 };
 /* MonodomainSolver (default) or OperatorSplittingMonodomainSolver */

@@ -49,6 +49,82 @@ double stimulus_value(const orc_stimulus* s, double t) {
     }
 }
 
+// EvaluateYDerivatives of a cell whose voltage derivative may be forced to zero
+// (AbstractCardiacCell::SetVoltageDerivativeToZero).
+template <class M>
+static void derivs(const std::vector<double>& y, double stim, double cm, const double* p, bool zero_dv,
+                   std::vector<double>& dy) {
+    M::template rhs<double>(y.data(), stim, cm, p, dy.data());
+    if (zero_dv) dy[0] = 0.0;
+}
+
+// GRL1IvpOdeSolver::CalculateNextYValue (ode/src/solver/GRL1IvpOdeSolver.cpp:47-93)
+// and GRL2IvpOdeSolver::CalculateNextYValue (ode/src/solver/GRL2IvpOdeSolver.cpp:47-119),
+// in the order those functions evaluate and perturb the state vector.
+template <class M>
+void grl_next(int method, double* yio, double stim, double cm, const double* p, double h, bool zero_dv) {
+    const double delta = 1.0e-8;
+    const int n = M::kNumStates;
+    std::vector<double> cur(yio, yio + n), next(n), evalf(n), partial(n), temp(n);
+    if (method == ORC_GRL1) {
+        derivs<M>(cur, stim, cm, p, zero_dv, evalf);
+        for (int i = 0; i < n; ++i) {
+            const double t = cur[i];
+            cur[i] = t + delta;
+            derivs<M>(cur, stim, cm, p, zero_dv, temp);
+            partial[i] = (temp[i] - evalf[i]) / delta;
+            cur[i] = t;
+        }
+        for (int i = 0; i < n; ++i)
+            next[i] = std::fabs(partial[i]) < delta ? cur[i] + evalf[i] * h
+                                                    : cur[i] + (evalf[i] / partial[i]) * (std::exp(partial[i] * h) - 1);
+    } else {
+        next = cur;
+        const std::vector<double> yinit = next;
+        derivs<M>(next, stim, cm, p, zero_dv, evalf);
+        for (int i = 0; i < n; ++i) {
+            next[i] = next[i] + delta;
+            derivs<M>(next, stim, cm, p, zero_dv, temp);
+            partial[i] = (temp[i] - evalf[i]) / delta;
+            next[i] = next[i] - delta;
+        }
+        for (int i = 0; i < n; ++i)   // midpoint
+            next[i] = std::fabs(partial[i]) < delta ? next[i] + 0.5 * evalf[i] * h
+                                                    : next[i] + (evalf[i] / partial[i]) * (std::exp(partial[i] * 0.5 * h) - 1);
+        for (int i = 0; i < n; ++i) {
+            const double ysave = next[i];
+            next[i] = yinit[i];
+            derivs<M>(next, stim, cm, p, zero_dv, temp);
+            evalf[i] = temp[i];
+            next[i] = next[i] + delta;
+            derivs<M>(next, stim, cm, p, zero_dv, temp);
+            partial[i] = (temp[i] - evalf[i]) / delta;
+            next[i] = ysave;
+        }
+        for (int i = 0; i < n; ++i)
+            next[i] = std::fabs(partial[i]) < delta ? yinit[i] + evalf[i] * h
+                                                    : yinit[i] + (evalf[i] / partial[i]) * (std::exp(partial[i] * h) - 1);
+    }
+    for (int i = 0; i < n; ++i) yio[i] = next[i];
+}
+
+template void grl_next<chb::LuoRudy1991>(int, double*, double, double, const double*, double, bool);
+template void grl_next<chb::TenTusscher2006Epi>(int, double*, double, double, const double*, double, bool);
+
+// AbstractCardiacCell::ComputeExceptVoltage (heart/src/odes/AbstractCardiacCell.cpp:90-105)
+// with a GRL1/GRL2 ODE solver: AbstractOneStepIvpOdeSolver::InternalSolve over
+// TimeStepper steps, dV/dt forced to 0.
+template <class M>
+static void grl_except_voltage(int method, double* y, const double* p, const orc_stimulus* stim,
+                               double am_div, double cm, double t0, double t1, double dt) {
+    TimeStepper st(t0, t1, dt);
+    while (!st.AtEnd()) {
+        const double s = stimulus_value(stim, st.Time()) / am_div;
+        grl_next<M>(method, y, s, cm, p, st.NextStep(), true);
+        st.Advance();
+    }
+}
+
 template <class M>
 static void fe_except_voltage(double* y, const double* p, const orc_stimulus* stim,
                               double am_div, double cm, double t0, double t1, double dt) {
@@ -98,6 +174,7 @@ void except_voltage(int method, double* y, const double* p, const orc_stimulus* 
                     double am_div, double cm, double t0, double t1, double dt) {
     if (method == ORC_RL) rl_except_voltage<M>(y, p, stim, am_div, cm, t0, t1, dt);
     else if (method == ORC_BE) be_except_voltage<M>(y, p, stim, am_div, cm, t0, t1, dt);
+    else if (method == ORC_GRL1 || method == ORC_GRL2) grl_except_voltage<M>(method, y, p, stim, am_div, cm, t0, t1, dt);
     else fe_except_voltage<M>(y, p, stim, am_div, cm, t0, t1, dt);
 }
 
@@ -120,7 +197,7 @@ static int compute(int method, double* y, const double* p, const orc_stimulus* s
     };
     record();
     double dy[M::kNumStates];
-    if (method == ORC_FE) {
+    if (method == ORC_FE || method == ORC_GRL1 || method == ORC_GRL2) {
         // AbstractOneStepIvpOdeSolver::Solve with sampling (.cpp:41-91)
         TimeStepper outer(t0, t1, tsamp);
         while (!outer.AtEnd()) {
@@ -128,8 +205,12 @@ static int compute(int method, double* y, const double* p, const orc_stimulus* s
             while (!inner.AtEnd()) {
                 const double h = inner.NextStep();
                 const double s = stimulus_value(stim, inner.Time());
-                M::template rhs<double>(y, s, cm, p, dy);
-                for (int i = 0; i < n; ++i) y[i] += h * dy[i];
+                if (method == ORC_FE) {
+                    M::template rhs<double>(y, s, cm, p, dy);
+                    for (int i = 0; i < n; ++i) y[i] += h * dy[i];
+                } else {
+                    grl_next<M>(method, y, s, cm, p, h, false);
+                }
                 inner.Advance();
             }
             outer.Advance();

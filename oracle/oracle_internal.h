@@ -27,6 +27,9 @@ class TimeStepper {
 double stimulus_value(const orc_stimulus* s, double t);
 
 template <class M>
+void grl_next(int method, double* y, double stim, double cm, const double* p, double h, bool zero_dv);
+
+template <class M>
 void except_voltage(int method, double* y, const double* p, const orc_stimulus* stim,
                     double am_div, double cm, double t0, double t1, double dt);
 

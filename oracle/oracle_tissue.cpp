@@ -428,6 +428,8 @@ static void solve_cells_with_voltage(Tissue& T, double t0, double t1) {
                     chb::rl_step<Mdl, double>(y, sv, T.cfg.cm, p, T.cfg.dt_ode);
                 } else if (T.cfg.ode_method == ORC_BE) {
                     chb::be_step<Mdl, double>(y, sv, T.cfg.cm, p, T.cfg.dt_ode, true);
+                } else if (T.cfg.ode_method == ORC_GRL1 || T.cfg.ode_method == ORC_GRL2) {
+                    grl_next<Mdl>(T.cfg.ode_method, y, sv, T.cfg.cm, p, ts.NextStep(), false);
                 } else {
                     const double h = ts.NextStep();
                     Mdl::template rhs<double>(y, sv, T.cfg.cm, p, dy);

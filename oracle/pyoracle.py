@@ -35,7 +35,7 @@ def _host_tag():
 LIB_PATH = os.path.join(HERE, "build", f"liboracle-{_host_tag()}.so")
 
 LR91, TT06 = 0, 1
-FE, RL, BE = 0, 1, 2
+FE, RL, BE, GRL1, GRL2 = 0, 1, 2, 3, 4
 PC_NONE, PC_JACOBI, PC_BJACOBI = 0, 1, 2
 STIM_NONE, STIM_SIMPLE, STIM_REGULAR = 0, 1, 2
 

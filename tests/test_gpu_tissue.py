@@ -173,6 +173,27 @@ def test_backward_euler_cells_parity(N, oracle, solver, case_name):
     assert float(np.max(np.abs(m.voltage() - g.voltage()))) <= 0.5
 
 
+@pytest.mark.parametrize("method,solver,case_name", [(3, 0, "LR91_2D"), (4, 0, "LR91_2D"), (3, 1, "LR91_2D"),
+                                                     (4, 1, "LR91_2D"), (3, 0, "TT06_3D"), (4, 0, "TT06_3D")])
+def test_generalised_rush_larsen_cells_parity(N, oracle, method, solver, case_name):
+    """Cells whose ODE solver is GRL1 (method 3) or GRL2 (method 4), on the GPU in FP64
+    against the oracle, with V clamped (default solver) and with V (operator
+    splitting); mixed precision within 0.5 mV of FP64."""
+    case = dict(getattr(TC, case_name))
+    case.update(method=method, solver=solver)
+    g, _ = TC.make_gpu(N, **case)
+    o, _ = TC.make_oracle(oracle, **case)
+    worst = 0.0
+    for _ in range(5):
+        g.step(4)
+        o.step(4)
+        worst = max(worst, _cmp(g.voltage(), o.voltage()))
+    assert worst <= FP64_RTOL, worst
+    m, _ = TC.make_gpu(N, precision=1, **case)
+    m.step(20)
+    assert float(np.max(np.abs(m.voltage() - g.voltage()))) <= 0.5
+
+
 @pytest.mark.parametrize("method,case_name,use_csr", [(1, "TT06_3D", False), (2, "TT06_3D", True),
                                                      (0, "LR91_2D", False)])
 def test_state_variable_interpolation_parity(N, oracle, method, case_name, use_csr):
