@@ -120,6 +120,11 @@ SIGNATURES = {
     "cg_cable_backward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
     "cg_cable_destroy": (C.c_int, [_vp]),
     "cg_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_double, _ip, _dp]),
+    "cg_output_configure": (C.c_int, [_vp, C.c_int, C.c_int, _ip, C.c_int]),
+    "cg_output_frames": (C.c_int, [_vp, _ip, _dp]),
+    "cg_output_fetch": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
+    "cg_output_cell_properties": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _dp, _ip, _dp, _dp, _ip]),
+    "cg_output_conduction_velocity": (C.c_int, [_vp, C.c_int, _dp, C.c_double, C.c_int, _dp, _ip]),
     "cg_slab_solve_noalloc": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, _dp, _vp, _vp, _vp, _ip]),
 }
@@ -270,6 +275,52 @@ class Tissue:
         it = np.zeros(n, dtype=np.int32)
         check(lib().cg_get_iteration_history(self.h, n, iptr(it)), "cg_get_iteration_history")
         return it
+
+    # -- printing-step output on the device
+    def configure_output(self, printing_steps, max_frames, state_vars=()):
+        sv = np.ascontiguousarray(state_vars, dtype=np.int32)
+        check(lib().cg_output_configure(self.h, int(printing_steps), int(max_frames),
+                                        iptr(sv) if sv.size else None, int(sv.size)), "cg_output_configure")
+        self._out_nv = 1 + int(sv.size)
+
+    def output_times(self):
+        nf = C.c_int()
+        check(lib().cg_output_frames(self.h, C.byref(nf), None), "cg_output_frames")
+        t = np.zeros(nf.value)
+        check(lib().cg_output_frames(self.h, C.byref(nf), dptr(t)), "cg_output_frames")
+        return t
+
+    def output_frames(self, first=0, count=None):
+        """Frames as Hdf5DataWriter's Data dataset: (frames, nodes, variables), V first."""
+        nf = C.c_int()
+        check(lib().cg_output_frames(self.h, C.byref(nf), None), "cg_output_frames")
+        count = nf.value - first if count is None else count
+        out = np.zeros((count, self.n, getattr(self, "_out_nv", 1)))
+        check(lib().cg_output_fetch(self.h, int(first), int(count), dptr(out)), "cg_output_fetch")
+        return out
+
+    @staticmethod
+    def _rows(arr, counts):
+        return [list(arr[i, :min(int(c), arr.shape[1])]) for i, c in enumerate(counts)]
+
+    def cell_property_maps(self, percentage=90.0, threshold=-30.0, max_aps=16):
+        """(APD map, upstroke-time map, max-upstroke-velocity map) as per-node lists, and
+        the raw padded arrays with the list lengths."""
+        n = self.n
+        apd, ut, uv = (np.zeros((n, max_aps)) for _ in range(3))
+        na, nu = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        check(lib().cg_output_cell_properties(self.h, float(percentage), float(threshold), int(max_aps), dptr(apd),
+                                              iptr(na), dptr(ut), dptr(uv), iptr(nu)), "cg_output_cell_properties")
+        return dict(apd=self._rows(apd, na), upstroke_time=self._rows(ut, nu), max_upstroke_velocity=self._rows(uv, nu),
+                    apd_array=apd, upstroke_time_array=ut, max_upstroke_velocity_array=uv, n_apd=na, n_upstroke=nu)
+
+    def conduction_velocity_map(self, origin, distances, threshold=-30.0, max_aps=16):
+        d = np.ascontiguousarray(distances, dtype=np.float64)
+        cv = np.zeros((self.n, max_aps))
+        nc = np.zeros(self.n, np.int32)
+        check(lib().cg_output_conduction_velocity(self.h, int(origin), dptr(d), float(threshold), int(max_aps),
+                                                  dptr(cv), iptr(nc)), "cg_output_conduction_velocity")
+        return self._rows(cv, nc)
 
     def snapshot(self) -> bytes:
         sz = C.c_size_t()

@@ -17,6 +17,7 @@
 #include "kernels/cg_mixed.cuh"
 #include "kernels/ode.cuh"
 #include "kernels/svi.cuh"
+#include "kernels/output.cuh"
 
 using namespace chb;
 
@@ -62,6 +63,12 @@ struct cg_ctx {
     double* d_corr = nullptr;
     int n_elems = 0, ell_width = 0;
     bool svi = false;
+    // printing-step output: frames of V and chosen state variables (cg_output_*)
+    int out_every = 0, out_max = 0, out_count = 0, out_nv = 0;
+    long long out_origin = 0;
+    double* d_frames = nullptr;      // out_max x out_nv x n
+    int* d_out_vars = nullptr;       // out_nv (entry 0 = V)
+    std::vector<double> out_times;
     void* d_states = nullptr;     // (S-1) x n of T
     void* d_iion = nullptr;
     void* d_z = nullptr;
@@ -296,6 +303,8 @@ int cg_destroy(cg_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->d_frames) cudaFree(c->d_frames);
+    if (c->d_out_vars) cudaFree(c->d_out_vars);
     c->mem.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -908,6 +917,29 @@ void launch_svi(cg_ctx* c) {
     }
 }
 
+// Frames the next n_steps PDE steps add, and the frame written after step s.
+long long out_frames_added(const cg_ctx* c, long long n_steps) {
+    if (!c->out_every) return 0;
+    const long long a = c->steps - c->out_origin, b = a + n_steps;
+    return b / c->out_every - a / c->out_every;
+}
+
+void launch_frame(cg_ctx* c, double t) {
+    double* out = c->d_frames + (size_t)c->out_count * c->out_nv * c->n;
+    if (c->mixed())
+        frame_kernel<float><<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, (const float*)c->d_states,
+                                                                   c->d_out_vars, c->out_nv, out);
+    else
+        frame_kernel<double><<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, (const double*)c->d_states,
+                                                                    c->d_out_vars, c->out_nv, out);
+    c->out_times.push_back(t);
+    c->out_count++;
+}
+
+void out_after_step(cg_ctx* c, long long s) {
+    if (c->out_every && (s - c->out_origin) % c->out_every == 0) launch_frame(c, (double)s * c->cfg.pde_time_step);
+}
+
 cudaError_t launch_step(cg_ctx* c) {
     launch_odes(c, split(c) ? 1 : 0);
     cudaError_t e = cudaGetLastError();
@@ -1007,6 +1039,7 @@ int cg_step(cg_ctx* c, int n_steps) {
         if (build_graph(c) != CG_OK) c->graph = nullptr;   // plain launches instead
         c->graph_dirty = false;
     }
+    if (c->out_count + out_frames_added(c, n_steps) > c->out_max && c->out_every) return CG_ERR_NOMEM;
     CG_CUDA(cudaEventRecord(c->ev0, c->stream));
     for (int k = 0; k < n_steps; ++k) {
         const cudaError_t e = c->graph ? cudaGraphLaunch(c->graph, c->stream) : launch_step(c);
@@ -1014,6 +1047,7 @@ int cg_step(cg_ctx* c, int n_steps) {
             cudaGetLastError();
             return CG_ERR_CUDA;
         }
+        out_after_step(c, c->steps + k + 1);
     }
     CG_CUDA(cudaEventRecord(c->ev1, c->stream));
     CG_CUDA(cudaStreamSynchronize(c->stream));
@@ -1263,6 +1297,7 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
         }
     double t_ode = 0.0, t_cg = 0.0;
     int rc = CG_OK;
+    if (c->out_count + out_frames_added(c, n_steps) > c->out_max && c->out_every) rc = CG_ERR_NOMEM;
     for (int k = 0; k < n_steps && rc == CG_OK; ++k) {
         cudaEventRecord(e[0], c->stream);
         launch_odes(c, split(c) ? 1 : 0);
@@ -1279,6 +1314,7 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
         cudaEventElapsedTime(&d, e[2], e[3]);
         t_ode += a + d;
         t_cg += b;
+        out_after_step(c, c->steps + k + 1);
     }
     for (auto& x : e) cudaEventDestroy(x);
     cudaGetLastError();
@@ -1299,3 +1335,176 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
     c->ms_last = t_ode + t_cg;
     return status_from_bits(bits);
 }
+
+// -------------------------------------------------------------- output --
+extern "C" {
+
+int cg_output_configure(cg_ctx* c, int printing_steps, int max_frames, const int* state_vars, int n_state_vars) {
+    if (!c || printing_steps < 0 || n_state_vars < 0 || (n_state_vars > 0 && !state_vars)) return CG_ERR_ARG;
+    if (!c->have_mesh || !c->have_cells) return CG_ERR_ORDER;
+    for (int k = 0; k < n_state_vars; ++k)
+        if (state_vars[k] < 1 || state_vars[k] >= c->n_states) return CG_ERR_ARG;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->d_frames) cudaFree(c->d_frames);
+    if (c->d_out_vars) cudaFree(c->d_out_vars);
+    c->d_frames = nullptr;
+    c->d_out_vars = nullptr;
+    c->out_every = c->out_max = c->out_count = c->out_nv = 0;
+    c->out_times.clear();
+    if (printing_steps == 0) return CG_OK;
+    if (max_frames < 1) return CG_ERR_ARG;
+    const int nv = 1 + n_state_vars;
+    const size_t bytes = (size_t)max_frames * nv * c->n * sizeof(double);
+    if (cudaMalloc(&c->d_frames, bytes) != cudaSuccess || cudaMalloc(&c->d_out_vars, nv * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->d_frames) cudaFree(c->d_frames);
+        c->d_frames = nullptr;
+        return CG_ERR_NOMEM;
+    }
+    std::vector<int> vars(nv, 0);
+    for (int k = 0; k < n_state_vars; ++k) vars[k + 1] = state_vars[k];
+    CG_CUDA(cudaMemcpyAsync(c->d_out_vars, vars.data(), nv * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    c->out_every = printing_steps;
+    c->out_max = max_frames;
+    c->out_nv = nv;
+    c->out_origin = c->steps;
+    launch_frame(c, (double)c->steps * c->cfg.pde_time_step);   // the initial condition
+    CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    return CG_OK;
+}
+
+int cg_output_frames(const cg_ctx* c, int* n_frames, double* times) {
+    if (!c || !n_frames) return CG_ERR_ARG;
+    *n_frames = c->out_count;
+    if (times) std::copy(c->out_times.begin(), c->out_times.end(), times);
+    return CG_OK;
+}
+
+int cg_output_fetch(cg_ctx* c, int first, int count, double* data) {
+    if (!c || !data || first < 0 || count < 0 || first + count > c->out_count) return CG_ERR_ARG;
+    if (count == 0) return CG_OK;
+    CG_CUDA(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->n, nv = (size_t)c->out_nv, fb = nv * n;
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    if (nv == 1) {
+        CG_CUDA(cudaMemcpy(data, c->d_frames + (size_t)first * fb, (size_t)count * fb * sizeof(double),
+                           cudaMemcpyDeviceToHost));
+        return CG_OK;
+    }
+    // device frames are variable-major; Hdf5DataWriter's Data dataset is [time][node][variable]
+    std::vector<double> buf(fb);
+    for (int f = 0; f < count; ++f) {
+        CG_CUDA(cudaMemcpy(buf.data(), c->d_frames + (size_t)(first + f) * fb, fb * sizeof(double),
+                           cudaMemcpyDeviceToHost));
+        double* out = data + (size_t)f * fb;
+        for (size_t v = 0; v < nv; ++v)
+            for (size_t i = 0; i < n; ++i) out[i * nv + v] = buf[v * n + i];
+    }
+    return CG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct DevBuf {
+    std::vector<void*> p;
+    template <typename P>
+    int get(P** q, size_t count) {
+        void* x = nullptr;
+        if (cudaMalloc(&x, std::max<size_t>(count, 1) * sizeof(P)) != cudaSuccess) {
+            cudaGetLastError();
+            return CG_ERR_NOMEM;
+        }
+        p.push_back(x);
+        *q = (P*)x;
+        return CG_OK;
+    }
+    ~DevBuf() {
+        for (void* x : p) cudaFree(x);
+    }
+};
+
+// CellProperties over every node's stored voltage frames; device results in a.
+int run_cellprops(cg_ctx* c, DevBuf& db, CellPropsArgs& a, double percentage, double threshold, int cap) {
+    if (c->out_count < 1) return CG_ERR_ORDER;
+    const size_t n = (size_t)c->n;
+    a.n = c->n;
+    a.n_frames = c->out_count;
+    a.nv = c->out_nv;
+    a.cap = cap;
+    a.frames = c->d_frames;
+    a.threshold = threshold;
+    a.percentage = percentage;
+    double* times = nullptr;
+    CG_TRY(db.get(&times, c->out_times.size()));
+    CG_CUDA(cudaMemcpyAsync(times, c->out_times.data(), c->out_times.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, c->stream));
+    a.times = times;
+    CG_TRY(db.get(&a.onset, (size_t)cap * n));
+    CG_TRY(db.get(&a.rest, (size_t)cap * n));
+    CG_TRY(db.get(&a.peak, (size_t)cap * n));
+    CG_TRY(db.get(&a.apd, (size_t)cap * n));
+    CG_TRY(db.get(&a.up_time, (size_t)cap * n));
+    CG_TRY(db.get(&a.up_vel, (size_t)cap * n));
+    CG_TRY(db.get(&a.n_apd, n));
+    CG_TRY(db.get(&a.n_up, n));
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((n + 127) / 128, (size_t)c->ode_blocks * 2));
+    cellprops_kernel<<<blocks, 128, 0, c->stream>>>(a);
+    CG_CUDA(cudaGetLastError());
+    return CG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cg_output_cell_properties(cg_ctx* c, double percentage, double threshold, int max_aps, double* apd, int* n_apd,
+                              double* upstroke_time, double* max_upstroke_velocity, int* n_upstroke) {
+    if (!c || max_aps < 1 || !(percentage > 0.0 && percentage < 100.0)) return CG_ERR_ARG;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    DevBuf db;
+    CellPropsArgs a;
+    CG_TRY(run_cellprops(c, db, a, percentage, threshold, max_aps));
+    const size_t n = (size_t)c->n, cells = n * max_aps;
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    if (apd) CG_CUDA(cudaMemcpy(apd, a.apd, cells * sizeof(double), cudaMemcpyDeviceToHost));
+    if (n_apd) CG_CUDA(cudaMemcpy(n_apd, a.n_apd, n * sizeof(int), cudaMemcpyDeviceToHost));
+    if (upstroke_time) CG_CUDA(cudaMemcpy(upstroke_time, a.up_time, cells * sizeof(double), cudaMemcpyDeviceToHost));
+    if (max_upstroke_velocity)
+        CG_CUDA(cudaMemcpy(max_upstroke_velocity, a.up_vel, cells * sizeof(double), cudaMemcpyDeviceToHost));
+    if (n_upstroke) {
+        CG_CUDA(cudaMemcpy(n_upstroke, a.n_up, n * sizeof(int), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) n_upstroke[i] = std::max(1, n_upstroke[i]);   // [0] when none
+    }
+    return CG_OK;
+}
+
+int cg_output_conduction_velocity(cg_ctx* c, int origin, const double* distances, double threshold, int max_aps,
+                                  double* cv, int* n_cv) {
+    if (!c || !distances || !cv || max_aps < 1 || origin < 0 || origin >= c->n) return CG_ERR_ARG;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    DevBuf db;
+    CellPropsArgs a;
+    CG_TRY(run_cellprops(c, db, a, 90.0, threshold, max_aps));
+    const size_t n = (size_t)c->n;
+    double *d_dist = nullptr, *d_cv = nullptr;
+    int* d_ncv = nullptr;
+    CG_TRY(db.get(&d_dist, n));
+    CG_TRY(db.get(&d_cv, n * max_aps));
+    CG_TRY(db.get(&d_ncv, n));
+    CG_CUDA(cudaMemcpyAsync(d_dist, distances, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)c->ode_blocks));
+    cv_kernel<<<blocks, 256, 0, c->stream>>>(c->n, max_aps, origin, d_dist, a.up_time, a.n_up, d_cv, d_ncv);
+    CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    CG_CUDA(cudaMemcpy(cv, d_cv, n * max_aps * sizeof(double), cudaMemcpyDeviceToHost));
+    if (n_cv) CG_CUDA(cudaMemcpy(n_cv, d_ncv, n * sizeof(int), cudaMemcpyDeviceToHost));
+    return CG_OK;
+}
+
+}  // extern "C"

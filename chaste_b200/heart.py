@@ -25,7 +25,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
-from .codegen import PARAM_NAMES
+from .codegen import PARAM_NAMES, STATE_NAMES
 
 DBL_MAX = 1.7976931348623157e308
 
@@ -65,6 +65,12 @@ class HeartConfig:
         self.device = 0
         self.operator_splitting = False
         self.state_variable_interpolation = False
+        self.output_variables = []
+        self.apd_maps = []
+        self.upstroke_time_maps = []
+        self.max_upstroke_velocity_maps = []
+        self.conduction_velocity_maps = []
+        self.keep_output = True
 
     # HeartConfig.cpp:1581-1587, 2337
     def SetOdeTimeStep(self, dt):
@@ -144,6 +150,32 @@ class HeartConfig:
 
     def GetUseStateVariableInterpolation(self):
         return self.state_variable_interpolation
+
+    # Output at printing steps (HeartConfig::SetOutputVariables) and the post-processing
+    # maps PostProcessingWriter writes (HeartConfig::SetApdMaps, SetUpstrokeTimeMaps,
+    # SetMaxUpstrokeVelocityMaps, SetConductionVelocityMaps), computed on the device
+    def SetOutputVariables(self, names):
+        self.output_variables = list(names)
+
+    def SetApdMaps(self, maps):
+        self.apd_maps = [(float(p), float(t)) for p, t in maps]
+
+    def SetUpstrokeTimeMaps(self, thresholds):
+        self.upstroke_time_maps = [float(t) for t in thresholds]
+
+    def SetMaxUpstrokeVelocityMaps(self, thresholds):
+        self.max_upstroke_velocity_maps = [float(t) for t in thresholds]
+
+    def SetConductionVelocityMaps(self, origin_nodes):
+        self.conduction_velocity_maps = [int(o) for o in origin_nodes]
+
+    def IsPostProcessingRequested(self):
+        return bool(self.apd_maps or self.upstroke_time_maps or self.max_upstroke_velocity_maps
+                    or self.conduction_velocity_maps)
+
+    # extension of this library: keep the printing-step frames on the device (default on)
+    def SetKeepOutputOnDevice(self, flag=True):
+        self.keep_output = bool(flag)
 
     def SetFibreLength(self, length, h):
         self.space_dimension, self.slab = 1, (length, 0.0, 0.0, h)
@@ -227,6 +259,22 @@ def CellLuoRudy1991FromCellMLBackwardEuler(stimulus=None):
 
 def CellTenTusscher2006EpiFromCellMLBackwardEuler(stimulus=None):
     return CellTenTusscher2006EpiFromCellML(stimulus, "BackwardEuler")
+
+
+def CellLuoRudy1991FromCellMLGRL1(stimulus=None):
+    return CellSpec(N.MODEL_LR91, stimulus or ZeroStimulus(), "GRL1")
+
+
+def CellLuoRudy1991FromCellMLGRL2(stimulus=None):
+    return CellSpec(N.MODEL_LR91, stimulus or ZeroStimulus(), "GRL2")
+
+
+def CellTenTusscher2006EpiFromCellMLGRL1(stimulus=None):
+    return CellSpec(N.MODEL_TT06, stimulus or ZeroStimulus(), "GRL1")
+
+
+def CellTenTusscher2006EpiFromCellMLGRL2(stimulus=None):
+    return CellSpec(N.MODEL_TT06, stimulus or ZeroStimulus(), "GRL2")
 
 
 class AbstractCardiacCellFactory:
@@ -325,6 +373,9 @@ class MonodomainProblem:
         self.native = None
         self.output_modifiers = []
         self._initialised = False
+        self._output_on = False
+        self.post_processing = {}
+        self.max_paces = 32        # columns kept per node in the post-processing maps
 
     def SetMesh(self, xyz, conn):
         self.mesh = (np.asarray(xyz, float), np.asarray(conn, np.int32))
@@ -377,8 +428,8 @@ class MonodomainProblem:
         if len(models) != 1 or len(solvers) != 1:
             raise ValueError("a GPU tissue runs one cell model with one ODE solver")
         cfg.model = models.pop()
-        cfg.ode_method = {"RushLarsen": N.ODE_RUSH_LARSEN,
-                          "BackwardEuler": N.ODE_BACKWARD_EULER}.get(solvers.pop(), N.ODE_FORWARD_EULER)
+        cfg.ode_method = {"RushLarsen": N.ODE_RUSH_LARSEN, "BackwardEuler": N.ODE_BACKWARD_EULER,
+                          "GRL1": N.ODE_GRL1, "GRL2": N.ODE_GRL2}.get(solvers.pop(), N.ODE_FORWARD_EULER)
         native = N.Tissue(cfg)
         if self.mesh is None:
             native.set_slab_mesh(dim, hc.slab[3], hc.slab[0], hc.slab[1], hc.slab[2], hc.sigma)
@@ -420,12 +471,77 @@ class MonodomainProblem:
         n_total = int(round(hc.simulation_duration / hc.pde_dt))
         per_print = max(1, int(round(hc.printing_dt / hc.pde_dt)))
         done = self.native.stats().steps
+        if (hc.keep_output or hc.IsPostProcessingRequested()) and not self._output_on:
+            names = STATE_NAMES[self.native.cfg.model]
+            idx = [names.index(v) for v in hc.output_variables]
+            self.native.configure_output(per_print, (n_total - done) // per_print + 1, idx)
+            self._output_on = True
         while done < n_total:
             k = min(per_print, n_total - done)
             self.native.step(k)
             done += k
             for m in self.output_modifiers:
                 m(done * hc.pde_dt, self.native)
+        if hc.IsPostProcessingRequested():
+            self._post_process(hc)
+
+    @staticmethod
+    def _hdf5_friendly(threshold):
+        """PostProcessingWriter::ConvertToHdf5FriendlyString (PostProcessingWriter.cpp:394-416)."""
+        extra = "_"
+        if threshold < 0.0:
+            extra += "minus_"
+            threshold = -threshold
+        if threshold - np.floor(threshold) > 1e-8:
+            return f"{extra}{int(np.floor(threshold))}pt{int(np.floor(threshold * 100) - np.floor(threshold) * 100)}"
+        return f"{extra}{threshold:g}"
+
+    def _post_process(self, hc):
+        """PostProcessingWriter::WritePostProcessingFiles (PostProcessingWriter.cpp:73-125),
+        each map as per-node lists under its dataset name."""
+        out = {}
+        for pct, thr in hc.apd_maps:
+            m = self.native.cell_property_maps(pct, thr, max_aps=self.max_paces)
+            out[f"Apd_{pct:g}{self._hdf5_friendly(thr)}_Map"] = m["apd"]
+        for thr in hc.upstroke_time_maps:
+            out[f"UpstrokeTimeMap{self._hdf5_friendly(thr)}"] = self.native.cell_property_maps(
+                90.0, thr, max_aps=self.max_paces)["upstroke_time"]
+        for thr in hc.max_upstroke_velocity_maps:
+            out[f"MaxUpstrokeVelocityMap{self._hdf5_friendly(thr)}"] = self.native.cell_property_maps(
+                90.0, thr, max_aps=self.max_paces)["max_upstroke_velocity"]
+        xyz = self.tissue.xyz
+        for origin in hc.conduction_velocity_maps:
+            dist = np.linalg.norm(xyz - xyz[origin], axis=1)
+            out[f"ConductionVelocityFromNode{origin}"] = self.native.conduction_velocity_map(
+                origin, dist, max_aps=self.max_paces)
+        self.post_processing = out
+
+    def GetOutput(self):
+        """The printing-step output as Hdf5DataWriter writes it: Time, Data (time x node x
+        variable) and the variable names, V first."""
+        hc = HeartConfig.Instance()
+        return dict(Time=self.native.output_times(), Data=self.native.output_frames(),
+                    variables=["V"] + list(hc.output_variables))
+
+    def GetPostProcessingMaps(self):
+        return dict(self.post_processing)
+
+    def WriteOutput(self, directory):
+        """Time.npy and Data.npy (the HDF5 file's two datasets), and one .npy per
+        post-processing map padded with -999 as PostProcessingWriter pads them (no HDF5
+        library is linked, so the container is NumPy's)."""
+        import os
+
+        os.makedirs(directory, exist_ok=True)
+        o = self.GetOutput()
+        np.save(os.path.join(directory, "Time.npy"), o["Time"])
+        np.save(os.path.join(directory, "Data.npy"), o["Data"])
+        for name, rows in self.post_processing.items():
+            width = max(len(r) for r in rows)
+            arr = np.full((width, len(rows)), -999.0)   # pace x node, as the HDF5 map datasets
+            for i, r in enumerate(rows):
+                arr[:len(r), i] = r
+            np.save(os.path.join(directory, name + ".npy"), arr)
 
     def GetSolution(self):
         return self.native.voltage()

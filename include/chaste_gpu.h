@@ -271,6 +271,41 @@ int cg_cable_destroy(cg_cable* c);
  * fault, trap or hang is involved, and the device stays usable afterwards. */
 int cg_selftest_barrier_timeout(int device, double limit_ms, int* status_bits, double* waited_ms);
 
+/* ---------------------------------------------------------------- output --
+ * Printing-step output kept on the device.  Replaces what
+ * AbstractCardiacProblem::Solve writes through Hdf5DataWriter at t = 0 and every
+ * printing time step (heart/src/problem/AbstractCardiacProblem.cpp:552-565; extra
+ * state variables as HeartConfig::SetOutputVariables adds them), and the maps
+ * PostProcessingWriter then derives from that file
+ * (heart/src/postprocessing/PostProcessingWriter.cpp:226-345).
+ *
+ * cg_output_configure: a frame of V (and the listed state variables, indices
+ * 1..S-1 as in cg_get_cell_state) is stored on the device now and after every
+ * printing_steps PDE steps of cg_step / cg_step_profiled, up to max_frames
+ * frames; a cg_step call that would need more returns CG_ERR_NOMEM without
+ * stepping.  printing_steps = 0 turns the output off and frees the frames.
+ * cg_output_frames: frames so far and their times (ms).
+ * cg_output_fetch: frames [first, first + count) in Hdf5DataWriter's Data
+ * layout, count x n_nodes x (1 + n_state_vars) doubles, V first.
+ * cg_output_cell_properties: CellProperties (heart/src/postprocessing/
+ * CellProperties.cpp:55-330) of every node's stored voltage frames with the
+ * given threshold: the APD map of WriteApdMapFile(percentage, threshold), the
+ * upstroke-time map of WriteUpstrokeTimeMap and the maximum-upstroke-velocity
+ * map of WriteMaxUpstrokeVelocityMap, each n_nodes x max_aps (row i: node i's
+ * list, -999 after it; [0] where CellProperties raises) with the list lengths
+ * in n_apd / n_upstroke (which may exceed max_aps; lists are then truncated).
+ * Any output pointer may be NULL.
+ * cg_output_conduction_velocity: WriteConductionVelocityMap(origin, distances)
+ * (PropagationPropertiesCalculator::CalculateAllConductionVelocities), same
+ * layout, distances[i] from the origin node to node i. */
+int cg_output_configure(cg_ctx* ctx, int printing_steps, int max_frames, const int* state_vars, int n_state_vars);
+int cg_output_frames(const cg_ctx* ctx, int* n_frames, double* times);
+int cg_output_fetch(cg_ctx* ctx, int first, int count, double* data);
+int cg_output_cell_properties(cg_ctx* ctx, double percentage, double threshold, int max_aps, double* apd,
+                              int* n_apd, double* upstroke_time, double* max_upstroke_velocity, int* n_upstroke);
+int cg_output_conduction_velocity(cg_ctx* ctx, int origin, const double* distances, double threshold, int max_aps,
+                                  double* cv, int* n_cv);
+
 /* Allocation-free diffusion solve of one PDE step on a regular slab.
  *
  * No counterpart in the reference: Chaste always owns its PETSc vectors.  This
