@@ -123,6 +123,8 @@ SIGNATURES = {
     "cg_output_configure": (C.c_int, [_vp, C.c_int, C.c_int, _ip, C.c_int]),
     "cg_output_frames": (C.c_int, [_vp, _ip, _dp]),
     "cg_output_fetch": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
+    "cg_output_activation": (C.c_int, [_vp, C.c_double]),
+    "cg_output_get_activation": (C.c_int, [_vp, _dp]),
     "cg_output_cell_properties": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _dp, _ip, _dp, _dp, _ip]),
     "cg_output_conduction_velocity": (C.c_int, [_vp, C.c_int, _dp, C.c_double, C.c_int, _dp, _ip]),
     "cg_slab_solve_noalloc": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double,
@@ -282,6 +284,15 @@ class Tissue:
         check(lib().cg_output_configure(self.h, int(printing_steps), int(max_frames),
                                         iptr(sv) if sv.size else None, int(sv.size)), "cg_output_configure")
         self._out_nv = 1 + int(sv.size)
+
+    def enable_activation_modifier(self, threshold):
+        check(lib().cg_output_activation(self.h, float(threshold)), "cg_output_activation")
+
+    def activation_modifier_times(self):
+        """(n, 4): first activation, first recovery, second activation, second recovery."""
+        t = np.zeros((self.n, 4))
+        check(lib().cg_output_get_activation(self.h, dptr(t)), "cg_output_get_activation")
+        return t
 
     def output_times(self):
         nf = C.c_int()

@@ -69,6 +69,8 @@ struct cg_ctx {
     double* d_frames = nullptr;      // out_max x out_nv x n
     int* d_out_vars = nullptr;       // out_nv (entry 0 = V)
     std::vector<double> out_times;
+    double* d_act4 = nullptr;        // ActivationOutputModifier times, 4 x n
+    double act4_threshold = 0.0;
     void* d_states = nullptr;     // (S-1) x n of T
     void* d_iion = nullptr;
     void* d_z = nullptr;
@@ -305,6 +307,7 @@ int cg_destroy(cg_ctx* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->d_frames) cudaFree(c->d_frames);
     if (c->d_out_vars) cudaFree(c->d_out_vars);
+    if (c->d_act4) cudaFree(c->d_act4);
     c->mem.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -925,6 +928,11 @@ long long out_frames_added(const cg_ctx* c, long long n_steps) {
 }
 
 void launch_frame(cg_ctx* c, double t) {
+    if (c->d_act4)
+        activation_modifier_kernel<<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, c->act4_threshold, t,
+                                                                          c->d_act4);
+    c->out_times.push_back(t);
+    if (c->out_max == 0) return;   // modifiers only
     double* out = c->d_frames + (size_t)c->out_count * c->out_nv * c->n;
     if (c->mixed())
         frame_kernel<float><<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, (const float*)c->d_states,
@@ -932,7 +940,6 @@ void launch_frame(cg_ctx* c, double t) {
     else
         frame_kernel<double><<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, (const double*)c->d_states,
                                                                     c->d_out_vars, c->out_nv, out);
-    c->out_times.push_back(t);
     c->out_count++;
 }
 
@@ -1039,7 +1046,7 @@ int cg_step(cg_ctx* c, int n_steps) {
         if (build_graph(c) != CG_OK) c->graph = nullptr;   // plain launches instead
         c->graph_dirty = false;
     }
-    if (c->out_count + out_frames_added(c, n_steps) > c->out_max && c->out_every) return CG_ERR_NOMEM;
+    if (c->out_max && c->out_count + out_frames_added(c, n_steps) > c->out_max) return CG_ERR_NOMEM;
     CG_CUDA(cudaEventRecord(c->ev0, c->stream));
     for (int k = 0; k < n_steps; ++k) {
         const cudaError_t e = c->graph ? cudaGraphLaunch(c->graph, c->stream) : launch_step(c);
@@ -1297,7 +1304,7 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
         }
     double t_ode = 0.0, t_cg = 0.0;
     int rc = CG_OK;
-    if (c->out_count + out_frames_added(c, n_steps) > c->out_max && c->out_every) rc = CG_ERR_NOMEM;
+    if (c->out_max && c->out_count + out_frames_added(c, n_steps) > c->out_max) rc = CG_ERR_NOMEM;
     for (int k = 0; k < n_steps && rc == CG_OK; ++k) {
         cudaEventRecord(e[0], c->stream);
         launch_odes(c, split(c) ? 1 : 0);
@@ -1348,14 +1355,16 @@ int cg_output_configure(cg_ctx* c, int printing_steps, int max_frames, const int
     CG_CUDA(cudaStreamSynchronize(c->stream));
     if (c->d_frames) cudaFree(c->d_frames);
     if (c->d_out_vars) cudaFree(c->d_out_vars);
+    if (c->d_act4) cudaFree(c->d_act4);
     c->d_frames = nullptr;
     c->d_out_vars = nullptr;
+    c->d_act4 = nullptr;
     c->out_every = c->out_max = c->out_count = c->out_nv = 0;
     c->out_times.clear();
     if (printing_steps == 0) return CG_OK;
-    if (max_frames < 1) return CG_ERR_ARG;
+    if (max_frames < 0) return CG_ERR_ARG;
     const int nv = 1 + n_state_vars;
-    const size_t bytes = (size_t)max_frames * nv * c->n * sizeof(double);
+    const size_t bytes = (size_t)std::max(max_frames, 1) * nv * c->n * sizeof(double);
     if (cudaMalloc(&c->d_frames, bytes) != cudaSuccess || cudaMalloc(&c->d_out_vars, nv * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         if (c->d_frames) cudaFree(c->d_frames);
@@ -1378,7 +1387,42 @@ int cg_output_configure(cg_ctx* c, int printing_steps, int max_frames, const int
 int cg_output_frames(const cg_ctx* c, int* n_frames, double* times) {
     if (!c || !n_frames) return CG_ERR_ARG;
     *n_frames = c->out_count;
-    if (times) std::copy(c->out_times.begin(), c->out_times.end(), times);
+    if (times) std::copy(c->out_times.begin(), c->out_times.begin() + c->out_count, times);
+    return CG_OK;
+}
+
+int cg_output_activation(cg_ctx* c, double threshold) {
+    if (!c) return CG_ERR_ARG;
+    if (!c->out_every) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    if (!c->d_act4) {
+        if (cudaMalloc(&c->d_act4, 4 * (size_t)c->n * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            c->d_act4 = nullptr;
+            return CG_ERR_NOMEM;
+        }
+    }
+    std::vector<double> init(4 * (size_t)c->n, -1.0);
+    CG_CUDA(cudaMemcpyAsync(c->d_act4, init.data(), init.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    c->act4_threshold = threshold;
+    // InitialiseAtStart then the initial condition (AbstractCardiacProblem.cpp:460-464)
+    activation_modifier_kernel<<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, threshold,
+                                                                      (double)c->steps * c->cfg.pde_time_step, c->d_act4);
+    CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    return CG_OK;
+}
+
+int cg_output_get_activation(cg_ctx* c, double* times) {
+    if (!c || !times) return CG_ERR_ARG;
+    if (!c->d_act4) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)c->n;
+    std::vector<double> buf(4 * n);
+    CG_CUDA(cudaMemcpy(buf.data(), c->d_act4, buf.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < 4; ++k) times[i * 4 + k] = buf[k * n + i];
     return CG_OK;
 }
 

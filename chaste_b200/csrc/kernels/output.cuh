@@ -33,6 +33,24 @@ __global__ void __launch_bounds__(256) frame_kernel(int n, const double* __restr
     }
 }
 
+// ActivationOutputModifier::ProcessSolutionAtTimeStep (heart/src/problem/
+// ActivationOutputModifier.cpp:91-119) at a printing time: first activation, first
+// recovery, second activation and second recovery per node (4 x n, -1 until seen).
+__global__ void __launch_bounds__(256) activation_modifier_kernel(int n, const double* __restrict__ V, double thr,
+                                                                  double t, double* __restrict__ a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = V[i];
+        double* fa = a + i;
+        double* fr = a + (size_t)n + i;
+        double* sa = a + 2 * (size_t)n + i;
+        double* sr = a + 3 * (size_t)n + i;
+        if (v > thr && *fa < 0.0) *fa = t;
+        else if (*fa >= 0.0 && *fr < 0.0 && v < thr) *fr = t;
+        else if (*fr >= 0.0 && *sa < 0.0 && v > thr) *sa = t;
+        else if (*sa >= 0.0 && *sr < 0.0 && v < thr) *sr = t;
+    }
+}
+
 constexpr double kMapPad = -999.0;   // WriteOutputDataToHdf5 pads missing paces with -999
 
 struct CellPropsArgs {

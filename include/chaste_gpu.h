@@ -282,8 +282,14 @@ int cg_selftest_barrier_timeout(int device, double limit_ms, int* status_bits, d
  * cg_output_configure: a frame of V (and the listed state variables, indices
  * 1..S-1 as in cg_get_cell_state) is stored on the device now and after every
  * printing_steps PDE steps of cg_step / cg_step_profiled, up to max_frames
- * frames; a cg_step call that would need more returns CG_ERR_NOMEM without
- * stepping.  printing_steps = 0 turns the output off and frees the frames.
+ * frames (0: no frames, printing-step modifiers only); a cg_step call that would
+ * need more returns CG_ERR_NOMEM without stepping.  printing_steps = 0 turns the
+ * output off and frees the frames.
+ * cg_output_activation: ActivationOutputModifier (heart/src/problem/
+ * ActivationOutputModifier.cpp:91-119) on the device at the current time and every
+ * printing time from now on; cg_output_get_activation gives its four columns per
+ * node (first activation, first recovery, second activation, second recovery;
+ * -1 where not reached), n_nodes x 4.
  * cg_output_frames: frames so far and their times (ms).
  * cg_output_fetch: frames [first, first + count) in Hdf5DataWriter's Data
  * layout, count x n_nodes x (1 + n_state_vars) doubles, V first.
@@ -300,6 +306,8 @@ int cg_selftest_barrier_timeout(int device, double limit_ms, int* status_bits, d
  * layout, distances[i] from the origin node to node i. */
 int cg_output_configure(cg_ctx* ctx, int printing_steps, int max_frames, const int* state_vars, int n_state_vars);
 int cg_output_frames(const cg_ctx* ctx, int* n_frames, double* times);
+int cg_output_activation(cg_ctx* ctx, double threshold);
+int cg_output_get_activation(cg_ctx* ctx, double* times);
 int cg_output_fetch(cg_ctx* ctx, int first, int count, double* data);
 int cg_output_cell_properties(cg_ctx* ctx, double percentage, double threshold, int max_aps, double* apd,
                               int* n_apd, double* upstroke_time, double* max_upstroke_velocity, int* n_upstroke);

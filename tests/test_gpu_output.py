@@ -76,6 +76,7 @@ def paced_run(N, oracle):
     g, o, xyz = _paced(N, oracle)
     steps = int(round(T_END / PACED["dt_pde"]))
     g.configure_output(EVERY, steps // EVERY + 1)
+    g.enable_activation_modifier(-40.0)
     g.step(steps)
     frames = g.output_frames()[:, :, 0]
     times = g.output_times()
@@ -112,6 +113,37 @@ def test_cell_property_maps_against_the_oracle_frames(N, paced_run):
     assert worst_apd <= 1e-3
     assert all(np.array_equal(m["upstroke_time"][i], up_t_ref[i]) or
                np.abs(np.subtract(m["upstroke_time"][i], up_t_ref[i])).max() <= 0.21 for i in range(g.n))
+
+
+def test_activation_output_modifier(N, paced_run):
+    """ActivationOutputModifier's four columns at the printing times, against its
+    restatement on the same frames."""
+    g, frames, times, _, _ = paced_run
+    got = g.activation_modifier_times()
+    ref = -np.ones((g.n, 4))
+    for f, t in enumerate(times):
+        v = frames[f]
+        a = (v > -40.0) & (ref[:, 0] < 0)
+        b = ~a & (ref[:, 0] >= 0) & (ref[:, 1] < 0) & (v < -40.0)
+        c = ~a & ~b & (ref[:, 1] >= 0) & (ref[:, 2] < 0) & (v > -40.0)
+        d = ~a & ~b & ~c & (ref[:, 2] >= 0) & (ref[:, 3] < 0) & (v < -40.0)
+        ref[a, 0] = t
+        ref[b, 1] = t
+        ref[c, 2] = t
+        ref[d, 3] = t
+    assert np.array_equal(got, ref)
+    assert (got > 0).all()
+
+
+def test_modifiers_without_frames(N):
+    g, _ = TC.make_gpu(N, **PACED)
+    g.configure_output(5, 0)
+    g.enable_activation_modifier(-40.0)
+    g.step(200)
+    assert g.output_times().size == 0
+    act = g.activation_modifier_times()
+    assert (act[:, 0] >= 0).all() and (act[:, 1:] < 0).all()
+    assert np.all(np.round(act[:, 0] / 0.5, 9) % 1 == 0)   # printing times of 0.5 ms
 
 
 def test_conduction_velocity_map(N, paced_run):
