@@ -26,6 +26,7 @@ PC_NONE, PC_JACOBI, PC_BJACOBI = 0, 1, 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 STIM_NONE, STIM_SIMPLE, STIM_REGULAR = 0, 1, 2
 SOLVER_MONODOMAIN, SOLVER_OPERATOR_SPLITTING = 0, 1
+INNER_PC_LINE, INNER_PC_JACOBI = 0, 1
 
 
 class ChasteGpuError(RuntimeError):
@@ -49,6 +50,7 @@ class Config(C.Structure):
         ("use_mass_lumping", C.c_int), ("max_iterations", C.c_int), ("precision", C.c_int),
         ("device", C.c_int), ("check_state_ranges", C.c_int), ("activation_threshold", C.c_double),
         ("solver", C.c_int), ("use_state_variable_interpolation", C.c_int),
+        ("mixed_inner_preconditioner", C.c_int),
     ]
 
 

@@ -107,6 +107,8 @@ struct cg_ctx {
     StageArgs stage{};    // its shared-memory staging of the operator input
     size_t pipe_smem = 0; // dynamic shared memory of that launch
     int diag_slot = 0;
+    int xm_slot = -1, xp_slot = -1;   // stencil slots of offsets -1 and +1
+    bool line_pc = false;             // the pipelined mixed solve uses the x-line inner preconditioner
     // stats
     long long steps = 0;
     long long total_iters = 0;
@@ -228,6 +230,7 @@ void cg_default_config(cg_config* c) {
     c->device = 0;
     c->check_state_ranges = 0;
     c->activation_threshold = -40.0;
+    c->mixed_inner_preconditioner = CG_INNER_PC_LINE;
 }
 
 const char* cg_status_string(int s) {
@@ -273,6 +276,8 @@ int cg_create(const cg_config* cfg, cg_ctx** out) {
     if (cfg->precision != CG_PRECISION_FP64 && cfg->precision != CG_PRECISION_MIXED) return CG_ERR_ARG;
     if (cfg->solver != CG_SOLVER_MONODOMAIN && cfg->solver != CG_SOLVER_OPERATOR_SPLITTING) return CG_ERR_ARG;
     if (cfg->use_state_variable_interpolation != 0 && cfg->use_state_variable_interpolation != 1) return CG_ERR_ARG;
+    if (cfg->mixed_inner_preconditioner != CG_INNER_PC_LINE && cfg->mixed_inner_preconditioner != CG_INNER_PC_JACOBI)
+        return CG_ERR_ARG;
     // Chaste's operator-splitting solver has no correction-term assembler
     if (cfg->use_state_variable_interpolation && cfg->solver == CG_SOLVER_OPERATOR_SPLITTING)
         return CG_ERR_UNSUPPORTED;
@@ -367,6 +372,17 @@ CgKernel pick_cg_kernel(const cg_ctx* c) {
 // Bands of the slab offsets for the pipelined solve's window copies: offsets
 // closer than 1024 share a band (3D: one band per z plane).  False when the
 // offsets need more than kMaxBands bands.
+int allow_max_dynamic_smem(CgKernel k, int device) {
+    int optin = 0;
+    CG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa;
+    CG_CUDA(cudaFuncGetAttributes(&fa, k));
+    const int dyn = optin - (int)fa.sharedSizeBytes;
+    if (dyn > fa.maxDynamicSharedSizeBytes)
+        CG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    return CG_OK;
+}
+
 bool plan_stage(cg_ctx* c, int threads) {
     StageArgs& g = c->stage;
     g = StageArgs{};
@@ -456,10 +472,27 @@ int alloc_vectors(cg_ctx* c) {
         const long long k0 = ((long long)n + sms * per_sm_guess * pt - 1) / (sms * per_sm_guess * pt);
         if (k0 <= 4 && plan_stage(c, pt)) {
             CgKernel kern0 = pick_pipe(c, (int)k0);
-            const size_t smem0 = (size_t)k0 * c->stage.cap * sizeof(float);
-            CG_CUDA(cudaFuncSetAttribute(kern0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
+            // the x-line factors live after the staged windows; without room for both
+            // the inner solve keeps Jacobi
+            c->line_pc = c->cfg.mixed_inner_preconditioner == CG_INNER_PC_LINE && c->xm_slot >= 0 && c->xp_slot >= 0;
+            auto smem_of = [&](long long k) {
+                return (size_t)k * ((size_t)c->stage.cap + (c->line_pc ? (size_t)kLineCoef * pt : 0)) * sizeof(float);
+            };
+            // the dynamic shared-memory limit is a property of the kernel for the whole
+            // process, so it is raised once to the device's maximum (contexts with other
+            // slab sizes launch the same kernels) and each launch passes its own size
+            CG_TRY(allow_max_dynamic_smem(kern0, c->device));
             int per_sm_pipe = 0;
-            CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, kern0, pt, smem0));
+            for (int attempt = 0; attempt < 2; ++attempt) {
+                const size_t smem0 = smem_of(k0);
+                per_sm_pipe = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_pipe, kern0, pt, smem0) != cudaSuccess) {
+                    cudaGetLastError();
+                    per_sm_pipe = 0;
+                }
+                if (per_sm_pipe >= 1 || !c->line_pc) break;
+                c->line_pc = false;
+            }
             if (per_sm_pipe >= 1) {
                 const long long blocks = std::max(1LL, std::min({((long long)n + pt - 1) / pt,
                                                                   (long long)per_sm_pipe * sms,
@@ -467,9 +500,8 @@ int alloc_vectors(cg_ctx* c) {
                 const long long k = ((long long)n + blocks * pt - 1) / (blocks * pt);
                 if (k <= k0) {
                     c->pipe_nodes = (int)k;
-                    c->pipe_smem = (size_t)k * c->stage.cap * sizeof(float);
-                    CG_CUDA(cudaFuncSetAttribute(pick_pipe(c, (int)k), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)c->pipe_smem));
+                    c->pipe_smem = smem_of(k);
+                    CG_TRY(allow_max_dynamic_smem(pick_pipe(c, (int)k), c->device));
                     c->cg_blocks = (int)blocks;
                     c->cg_threads = pt;
                 }
@@ -515,9 +547,12 @@ int upload_operator(cg_ctx* c) {
         c->halo = (far + 8 + 3) / 4 * 4;
         CG_TRY(dalloc(c, &c->d_cls8, cls.size()));
         CG_CUDA(cudaMemcpyAsync(c->d_cls8, cls.data(), cls.size(), cudaMemcpyHostToDevice, s));
-        c->diag_slot = -1;
-        for (int o = 0; o < st.n_offsets; ++o)
+        c->diag_slot = c->xm_slot = c->xp_slot = -1;
+        for (int o = 0; o < st.n_offsets; ++o) {
             if (st.offsets[o] == 0) c->diag_slot = o;
+            if (st.offsets[o] == -1) c->xm_slot = o;
+            if (st.offsets[o] == 1) c->xp_slot = o;
+        }
         if (c->diag_slot < 0) return CG_ERR_ARG;
         CG_CUDA(cudaStreamSynchronize(s));
     } else {
@@ -837,6 +872,9 @@ CgArgs make_cg_args(cg_ctx* c) {
     a.maxit = c->cfg.max_iterations;
     a.pc = c->cfg.ksp_preconditioner == CG_PC_JACOBI ? 1 : 0;
     a.diag_slot = c->diag_slot;
+    a.xm_slot = c->xm_slot;
+    a.xp_slot = c->xp_slot;
+    a.line_pc = c->pipe_nodes > 0 && c->line_pc ? 1 : 0;
     a.max_refine = 20;
     return a;
 }

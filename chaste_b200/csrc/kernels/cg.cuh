@@ -67,6 +67,8 @@ struct CgArgs {
     int maxit;
     int pc;                     // 0 none, 1 jacobi
     int diag_slot;
+    int xm_slot, xp_slot;       // stencil slots of the x-neighbours (offsets -1, +1)
+    int line_pc;                // pipelined mixed solve: inner preconditioner on x-line segments
     int max_refine;
 };
 

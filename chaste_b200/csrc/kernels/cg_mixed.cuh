@@ -10,6 +10,8 @@
 // as the FP64 kernel (one operator application per iteration).
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "cg.cuh"
 
 namespace chb {
@@ -333,6 +335,78 @@ __device__ __forceinline__ float apply_a32_staged(const CgArgs& a, const SlabSha
     return acc;
 }
 
+// Inner preconditioner of the pipelined solve on the slab stencil: T^-1 d, where T is
+// the tridiagonal part of A along x (the direction of the largest conductivity)
+// restricted to the 32 consecutive nodes a warp holds in one register slot (rows cut
+// at the warp's ends and, through the stencil, at the ends of each x-line).  T is a
+// principal block-diagonal part of the SPD matrix A, so it is SPD and fixed, as CG
+// needs.  Solved by parallel cyclic reduction over 5 levels of warp shuffles.  The
+// elimination factors depend on T only, so they are computed once per solve
+// (warp_line_setup) into kLineCoef words of shared memory per slot and thread (the
+// factors in half precision: they only shape the preconditioner, which stays a fixed
+// operator); each application (warp_line_apply) is then 10 shuffles and 10 FMAs.
+// Every lane of the warp takes part; the rows of nodes past n are the identity.
+constexpr int kLineCoef = 6;   // per level the two factors as one half2 word, then 1 / the reduced diagonal
+
+__device__ __forceinline__ void warp_line_setup(float lo, float di, float up, float* cf, int ld) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) lo = 0.0f;
+    if (lane == 31) up = 0.0f;
+    int j = 0;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1, ++j) {
+        const float am = __shfl_up_sync(full, lo, s), bm = __shfl_up_sync(full, di, s);
+        const float cm = __shfl_up_sync(full, up, s);
+        const float ap = __shfl_down_sync(full, lo, s), bp = __shfl_down_sync(full, di, s);
+        const float cp = __shfl_down_sync(full, up, s);
+        const float k1 = lane >= s ? lo / bm : 0.0f;
+        const float k2 = lane + s < 32 ? up / bp : 0.0f;
+        di = di - k1 * cm - k2 * ap;
+        lo = -k1 * am;
+        up = -k2 * cp;
+        reinterpret_cast<__half2*>(cf)[j * ld] = __floats2half2_rn(k1, k2);
+    }
+    cf[5 * ld] = 1.0f / di;
+}
+
+__device__ __forceinline__ float warp_line_apply(const float* cf, int ld, float d) {
+    const unsigned full = 0xffffffffu;
+    int j = 0;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1, ++j) {
+        const float dm = __shfl_up_sync(full, d, s);
+        const float dp = __shfl_down_sync(full, d, s);
+        const float2 k = __half22float2(reinterpret_cast<const __half2*>(cf)[j * ld]);
+        d = d - k.x * dm - k.y * dp;
+    }
+    return d * cf[5 * ld];
+}
+
+// T's three coefficients for a node of stencil class c (identity for nodes past n).
+template <int NOFF>
+__device__ __forceinline__ void line_row(const CgArgs& a, const SlabShared<float>& s32, bool on, int c, float& lo,
+                                         float& di, float& up) {
+    lo = 0.0f, di = 1.0f, up = 0.0f;
+    if (!on) return;
+    if (c == a.slab.interior) {
+        lo = a.slab.ia32[a.xm_slot];
+        di = a.slab.ia32[a.diag_slot];
+        up = a.slab.ia32[a.xp_slot];
+    } else {
+        lo = s32.a[c * NOFF + a.xm_slot];
+        di = s32.a[c * NOFF + a.diag_slot];
+        up = s32.a[c * NOFF + a.xp_slot];
+    }
+}
+
+// B d for register slot k: the x-line solve (a.line_pc) or Jacobi.
+__device__ __forceinline__ float apply_inner_pc(const CgArgs& a, const float* cf, int ld, bool on, float dinv,
+                                                float d) {
+    if (!a.line_pc) return dinv * d;
+    return warp_line_apply(cf, ld, on ? d : 0.0f);
+}
+
 template <int NOFF, int KMAX>
 __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsigned& round) {
     __shared__ SlabShared<double> sh;
@@ -340,6 +414,10 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
     __shared__ double red[32 * 4];
     extern __shared__ float4 stage4[];
     float* stage = reinterpret_cast<float*>(stage4);
+    // x-line factors after the staged windows: slot k, word j of thread t at
+    // line_cf[(k * kLineCoef + j) * blockDim.x + t]
+    float* line_cf = stage + KMAX * a.stage.cap;
+    const int ld = blockDim.x;
     __shared__ __align__(8) unsigned long long stage_bar;
     unsigned stage_parity = 0;
     if (threadIdx.x == 0) mbar_init(&stage_bar);
@@ -364,6 +442,14 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
         cls[k] = on[k] ? (int)a.cls8[node[k]] : 0;
         dinv[k] = on[k] ? (a.pc ? s32.dinv[cls[k]] : 1.0f) : 0.0f;
     }
+    if (a.line_pc) {
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            float lo, di, up;
+            line_row<NOFF>(a, s32, on[k], cls[k], lo, di, up);
+            warp_line_setup(lo, di, up, line_cf + k * kLineCoef * ld + threadIdx.x, ld);
+        }
+    }
     float r[KMAX], u[KMAX], w[KMAX], m[KMAX], zq[KMAX], q[KMAX], sv[KMAX], p[KMAX], e[KMAX];
     double res[4];
 
@@ -372,21 +458,23 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
         double v[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int k = 0; k < KMAX; ++k) {
-            r[k] = u[k] = 0.0f;
-            if (!on[k]) continue;
-            const int i = node[k], c = cls[k];
-            const double b = apply_row<true, NOFF, true>(a, sh, nullptr, c, i, a.zrhs32) + (a.corr ? a.corr[i] : 0.0);
-            const double av = apply_row<true, NOFF, false>(a, sh, nullptr, c, i, x);
-            const double rr = b - av;
-            const double d = dinv_of<true>(a, sh, c, i);
-            const double wb = d * b, zz = d * rr;
-            v[0] += fabs(b);
-            v[1] += wb * wb;
-            v[2] += zz * zz;
-            r64[i] = rr;
-            r[k] = (float)rr;
-            u[k] = dinv[k] * r[k];
-            z32[i] = u[k];
+            r[k] = 0.0f;
+            if (on[k]) {
+                const int i = node[k], c = cls[k];
+                const double b =
+                    apply_row<true, NOFF, true>(a, sh, nullptr, c, i, a.zrhs32) + (a.corr ? a.corr[i] : 0.0);
+                const double av = apply_row<true, NOFF, false>(a, sh, nullptr, c, i, x);
+                const double rr = b - av;
+                const double d = dinv_of<true>(a, sh, c, i);
+                const double wb = d * b, zz = d * rr;
+                v[0] += fabs(b);
+                v[1] += wb * wb;
+                v[2] += zz * zz;
+                r64[i] = rr;
+                r[k] = (float)rr;
+            }
+            u[k] = apply_inner_pc(a, line_cf + k * kLineCoef * ld + threadIdx.x, ld, on[k], dinv[k], r[k]);
+            if (on[k]) z32[node[k]] = u[k];
         }
         if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
     }
@@ -423,7 +511,7 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
             for (int k = 0; k < KMAX; ++k) {
                 v[0] += (double)r[k] * (double)u[k];
                 v[1] += (double)w[k] * (double)u[k];
-                m[k] = dinv[k] * w[k];
+                m[k] = apply_inner_pc(a, line_cf + k * kLineCoef * ld + threadIdx.x, ld, on[k], dinv[k], w[k]);
                 if (on[k]) mb[node[k]] = m[k];
             }
             if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
@@ -477,18 +565,19 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
             double v[1] = {0};
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) {
-                r[k] = u[k] = 0.0f;
-                if (!on[k]) continue;
-                const int i = node[k], c = cls[k];
-                const double ae = apply_a64_l2<NOFF>(a, sh, c, i, e32);
-                x[i] += (double)e[k];
-                const double rr = r64[i] - ae;
-                r64[i] = rr;
-                const double zz = dinv_of<true>(a, sh, c, i) * rr;
-                v[0] += zz * zz;
-                r[k] = (float)rr;
-                u[k] = dinv[k] * r[k];
-                z32[i] = u[k];
+                r[k] = 0.0f;
+                if (on[k]) {
+                    const int i = node[k], c = cls[k];
+                    const double ae = apply_a64_l2<NOFF>(a, sh, c, i, e32);
+                    x[i] += (double)e[k];
+                    const double rr = r64[i] - ae;
+                    r64[i] = rr;
+                    const double zz = dinv_of<true>(a, sh, c, i) * rr;
+                    v[0] += zz * zz;
+                    r[k] = (float)rr;
+                }
+                u[k] = apply_inner_pc(a, line_cf + k * kLineCoef * ld + threadIdx.x, ld, on[k], dinv[k], r[k]);
+                if (on[k]) z32[node[k]] = u[k];
             }
             if (!grid_reduce<1>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }

@@ -53,6 +53,10 @@ enum { CG_MODEL_LR91 = 0, CG_MODEL_TT06 = 1 };
 enum { CG_ODE_FORWARD_EULER = 0, CG_ODE_RUSH_LARSEN = 1, CG_ODE_BACKWARD_EULER = 2,
        CG_ODE_GRL1 = 3, CG_ODE_GRL2 = 4 };
 enum { CG_PC_NONE = 0, CG_PC_JACOBI = 1, CG_PC_BJACOBI = 2 };
+/* Inner preconditioner of the mixed-precision solve on the slab stencil: the
+ * tridiagonal x-line part of A over each warp's 32 consecutive nodes, or Jacobi.
+ * No Chaste counterpart (Chaste has no mixed-precision solve). */
+enum { CG_INNER_PC_LINE = 0, CG_INNER_PC_JACOBI = 1 };
 enum { CG_PRECISION_FP64 = 0, CG_PRECISION_MIXED = 1 };
 enum { CG_STIM_NONE = 0, CG_STIM_SIMPLE = 1, CG_STIM_REGULAR = 2 };
 /* MonodomainSolver (heart/src/solver/electrics/monodomain/MonodomainSolver.cpp) or
@@ -83,6 +87,9 @@ typedef struct {
     int use_state_variable_interpolation; /* 1: SVI correction of the RHS
                                   (HeartConfig::SetUseStateVariableInterpolation,
                                   MonodomainCorrectionTermAssembler); default solver only */
+    int mixed_inner_preconditioner; /* CG_INNER_PC_*: the FP32 inner solve of the mixed
+                                  mode on a slab (default CG_INNER_PC_LINE); the FP64 outer
+                                  residual and its stopping test keep ksp_preconditioner */
 } cg_config;
 
 /* SimpleStimulus (heart/src/stimulus/SimpleStimulus.cpp:44-76) / RegularStimulus

@@ -83,7 +83,7 @@ def test_tt06_3d_rush_larsen_parity(N, oracle):
     assert np.abs(its_g - its_o).max() <= 1
 
 
-@pytest.mark.parametrize("variant", ["slab", "csr", "slab_two_nodes_per_thread"])
+@pytest.mark.parametrize("variant", ["slab", "csr", "slab_two_nodes_per_thread", "slab_jacobi_inner"])
 def test_mixed_precision_against_fp64(N, variant):
     """Mixed mode (FP32 states, FP32 inner CG, FP64 refinement) within 0.5 mV of FP64 and activation within 1 ms.
 
@@ -96,6 +96,8 @@ def test_mixed_precision_against_fp64(N, variant):
         case["use_csr"] = True
     elif variant == "slab_two_nodes_per_thread":
         case.update(size=(1.0, 0.5, 0.3), box_hi=(0.1, 0.1, 0.1))
+    elif variant == "slab_jacobi_inner":
+        case["inner_pc"] = 1
     a, _ = TC.make_gpu(N, precision=0, **case)
     b, _ = TC.make_gpu(N, precision=1, **case)
     worst = 0.0
@@ -109,6 +111,23 @@ def test_mixed_precision_against_fp64(N, variant):
     act = ta >= 0
     assert act.sum() > 0
     assert np.abs(ta[act] - tb[act]).max() <= 1.0
+
+
+def test_line_preconditioned_inner_solve_takes_fewer_iterations(N):
+    """The mixed solve's x-line inner preconditioner against its Jacobi inner solve on
+    an anisotropic slab (sigma_x / sigma_y = 9): same FP64 stopping test, same answer
+    within the tolerance, fewer inner iterations.  The two contexts also share the
+    pipelined kernel with different shared-memory sizes."""
+    case = dict(TC.TT06_3D, size=(1.0, 0.5, 0.3), box_hi=(0.1, 0.1, 0.1))
+    line, _ = TC.make_gpu(N, precision=1, **case)
+    jac, _ = TC.make_gpu(N, precision=1, inner_pc=1, **case)
+    ref, _ = TC.make_gpu(N, precision=0, **case)
+    for t in (line, jac, ref):
+        t.step(40)
+    il, ij = line.stats().total_cg_iterations, jac.stats().total_cg_iterations
+    assert il <= 0.75 * ij, (il, ij)
+    assert np.abs(line.voltage() - ref.voltage()).max() <= 0.5
+    assert np.abs(line.voltage() - jac.voltage()).max() <= 0.5
 
 
 @pytest.mark.parametrize("case_name", ["LR91_2D", "TT06_3D"])

@@ -17,7 +17,7 @@ def slab_stim_ids(xyz, box_hi):
 
 def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
              abs_tol=None, rel_tol=1e-8, precision=0, use_csr=False, param_set=None, param_table=None,
-             init_states=None, max_iterations=10000, solver=0, svi=0):
+             init_states=None, max_iterations=10000, solver=0, svi=0, inner_pc=0):
     """A GPU tissue on a regular slab (stencil operator, or CSR through cg_set_mesh when use_csr)."""
     from oracle import pyoracle as O  # mesh generator only: the same node/element order as the library
 
@@ -34,6 +34,7 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
     cfg.max_iterations = max_iterations
     cfg.solver = solver
     cfg.use_state_variable_interpolation = svi
+    cfg.mixed_inner_preconditioner = inner_pc
     t = N.Tissue(cfg)
     xyz, conn, _ = O.slab_mesh(dim, h, *size)
     if use_csr:
