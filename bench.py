@@ -226,7 +226,7 @@ def run_ours(args, rank, world, device):
 # 442,401-node slab (profiles/cg_kernels_tt06_slab_3d.md, profiles/ode_kernel_tt06_slab_3d.md;
 # `bench.py --profile <precision> --steps 30`, 26th launch)
 NCU_TRAFFIC = {
-    ("tt06_slab_3d", "mixed", "cg_kernel"): 7.70e6,
+    ("tt06_slab_3d", "mixed", "cg_kernel"): 7.65e6,
     ("tt06_slab_3d", "mixed", "ode_kernel"): 39.7e6,
     ("tt06_slab_3d", "fp64", "cg_kernel"): 8.70e6,
     ("tt06_slab_3d", "fp64", "ode_kernel"): 127.2e6,
