@@ -1,10 +1,14 @@
 """Benchmark of the monodomain operator-split step on B200.
 
 Workload (default): the 3D ten Tusscher 2006 epicardial slab, 2 x 0.7 x 0.3 cm
-at h = 0.01 cm (201 x 71 x 31 = 442,371 nodes, 2.52M tetrahedra), Rush-Larsen
-dt_ode = 0.02 ms, PDE dt = 0.1 ms, sigma = (1.75, 0.19, 0.19) mS/cm, corner
-stimulus -5e5 uA/cm^3 for 1 ms in a 0.1 cm cube, CG + Jacobi at rtol 1e-8.
-A step is one PDE step of every node (ODE -> RHS -> CG).  Metric: node-steps/s.
+at h = 0.01 cm (ConstructRegularSlabMesh gives 201 x 71 x 31 = 442,401 nodes,
+2.52M tetrahedra), Rush-Larsen dt_ode = 0.02 ms, PDE dt = 0.1 ms,
+sigma = (1.75, 0.19, 0.19) mS/cm, corner stimulus -5e5 uA/cm^3 for 1 ms in a
+0.1 cm cube, CG + Jacobi at rtol 1e-8.  A step is one PDE step of every node
+(ODE -> RHS -> CG).  Metric: node-steps/s.  Every arm first advances the
+simulation, untimed, to --t-start-ms (default 10 ms: the wavefront is inside the
+slab), so the timed steps are the same window of the run for the GPU paths, the
+CPU baseline and the reference arm.
 
 The mixed-precision path (FP32 states, FP32 inner CG, FP64 residual
 refinement) is the headline when its Vm stays within 0.5 mV of the FP64 path
@@ -34,11 +38,12 @@ WORKLOADS = {
                          size=(2.0, 0.7, 0.3), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
                          box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8,
                          name="3D TT06-epi Rush-Larsen slab 2x0.7x0.3 cm h=0.01 (201x71x31 = 442,401 nodes)"),
-    # BASELINE config 5 (2.1M nodes), used for profiling at a size beyond L2
+    # BASELINE config 5 (2.1M nodes): endo / mid / epi layers by thirds of z
     "tt06_slab_3d_large": dict(model=1, method=1, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.0125,
                                size=(2.0, 2.0, 1.0), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
-                               box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8,
-                               name="3D TT06-epi Rush-Larsen slab 2x2x1 cm h=0.0125 (2,099,601 nodes)"),
+                               box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8, transmural=True,
+                               name="3D TT06 Rush-Larsen slab 2x2x1 cm h=0.0125 (2,099,601 nodes), "
+                                    "endo/mid/epi layers by z-thirds"),
     # BASELINE config 1 (2D LR91 forward Euler)
     "lr91_sheet_2d": dict(model=0, method=0, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, size=(1.0, 1.0, 0.0),
                           sigma=(1.75, 1.75, 1.75), stim=(-5e5, 0.5, 0.0), box_hi=(0.0199, 1e9),
@@ -59,6 +64,20 @@ def ode_bytes_per_node(model, w):
     s = 19 if model == 1 else 8
     # read+write S-1 states, read V (8) and the stimulus id (1), write Iion and z
     return 2 * (s - 1) * w + 8 + 1 + 2 * w
+
+
+def csr_equivalent_bytes(model, mixed, its, sweeps, r=15):
+    """The survey's algorithmic bytes per node-step of an assembled-CSR implementation
+    (int32 columns, r entries per row): B_ode + B_rhs + k B_cg, with w = 8 (FP64) or 4
+    (mixed inner iterations) and r*12 + 4 + 5*8 per FP64 refinement sweep.  The slab
+    stencil moves far less (no matrix bytes); this is the figure to compare with a CSR
+    solver's traffic, not this library's."""
+    s = 19 if model == 1 else 8
+    w = 4 if mixed else 8
+    b_ode = (2 * (s - 1) + 2) * w
+    b_rhs = r * (8 + 4) + 4 + 3 * 8
+    b_cg = r * (w + 4) + 4 + 9 * w
+    return b_ode + b_rhs + its * b_cg + (sweeps * (r * 12 + 4 + 5 * 8) if mixed else 0)
 
 
 def cg_bytes(mixed, its, sweeps, pipelined=False):
@@ -124,7 +143,26 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def transmural_cells(wl, xyz):
+    """(param_set, param_table) of the workload's cells: the TT06 endo / mid / epi layers
+    by thirds of z when the workload has them, else (None, None)."""
+    if not wl.get("transmural"):
+        return None, None
+    from chaste_b200.heart import transmural_layers, transmural_param_table
+
+    return transmural_layers(xyz[:, 2], wl["size"][2]), transmural_param_table()
+
+
+def stimulated(wl, xyz):
+    inside = np.ones(xyz.shape[0], bool)
+    for d, hi in enumerate(wl["box_hi"][: wl["dim"]]):
+        inside &= xyz[:, d] <= hi + 1e-12
+    return np.where(inside, 0, -1).astype(np.int32)
+
+
 def build_tissue(N, wl, precision, device):
+    from chaste_b200.heart import slab_coordinates
+
     cfg = N.default_config()
     cfg.model, cfg.ode_method = wl["model"], wl["method"]
     cfg.ode_time_step, cfg.pde_time_step = wl["dt_ode"], wl["dt_pde"]
@@ -134,15 +172,15 @@ def build_tissue(N, wl, precision, device):
     cfg.device = device
     t = N.Tissue(cfg)
     t.set_slab_mesh(wl["dim"], wl["h"], *wl["size"], sigma=wl["sigma"])
-    t.set_cells()
-    from chaste_b200.heart import slab_coordinates
-
     xyz = slab_coordinates(wl["dim"], wl["h"], *wl["size"])
-    inside = np.ones(t.n, bool)
-    for d, hi in enumerate(wl["box_hi"][: wl["dim"]]):
-        inside &= xyz[:, d] <= hi + 1e-12
-    t.set_stimulus(np.where(inside, 0, -1).astype(np.int32), [N.stimulus(N.STIM_SIMPLE, *wl["stim"])])
+    pset, ptab = transmural_cells(wl, xyz)
+    t.set_cells(param_set=pset, param_table=ptab)
+    t.set_stimulus(stimulated(wl, xyz), [N.stimulus(N.STIM_SIMPLE, *wl["stim"])])
     return t
+
+
+def start_steps(args, wl):
+    return int(round(args.t_start_ms / wl["dt_pde"]))
 
 
 def flush_l2(buf):
@@ -162,6 +200,7 @@ def run_ours(args, rank, world, device):
     results = {}
     tissues = {label: build_tissue(N, wl, prec, device) for prec, label in ((0, "fp64"), (1, "mixed"))}
     for t in tissues.values():
+        t.step(start_steps(args, wl))   # untimed: to the start of the timed window
         t.step(args.warmup)
     clk = ClockSampler(device)
     with clk:
@@ -222,15 +261,11 @@ def run_ours(args, rank, world, device):
     return dict(n=n, out=out, vm_err=vm_err, head=head, e2e_s=e2e_s, wl=wl)
 
 
-# DRAM bytes (read + write) per launch from one ncu capture of each kernel on the
-# 442,401-node slab (profiles/cg_kernels_tt06_slab_3d.md, profiles/ode_kernel_tt06_slab_3d.md;
-# `bench.py --profile <precision> --steps 30`, 26th launch)
-NCU_TRAFFIC = {
-    ("tt06_slab_3d", "mixed", "cg_kernel"): 7.65e6,
-    ("tt06_slab_3d", "mixed", "ode_kernel"): 39.7e6,
-    ("tt06_slab_3d", "fp64", "cg_kernel"): 8.70e6,
-    ("tt06_slab_3d", "fp64", "ode_kernel"): 127.2e6,
-}
+# DRAM bytes (read + write) per launch of the dominant kernels from one ncu capture of
+# the timed region's conditions (L2 flushed before the step, the window starting at
+# --t-start-ms), `bench.py --profile <precision> --steps 5`, summarised in
+# profiles/cg_kernels_tt06_slab_3d.md.  None where no such capture exists.
+NCU_TRAFFIC = {}
 
 
 def roofline(res, args):
@@ -248,16 +283,25 @@ def roofline(res, args):
     ach = ach_ode if dom == "ode" else ach_cg
     kern = "ode_kernel" if dom == "ode" else "cg_kernel"
     traffic = NCU_TRAFFIC.get((args.workload, head, kern))
+    csr = csr_equivalent_bytes(res["wl"]["model"], mixed, o["mean_cg_iterations"], o["sweeps"] if mixed else 0,
+                               r=15 if res["wl"]["dim"] == 3 else 7)
     return {"bound": "hbm", "kernel": kern, "achieved": round(ach, 1),
             "peak": peak, "peak_kind": kind, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": traffic,
+            "bytes_model": "matrix-free slab stencil: the bytes this kernel must move (states, vectors, "
+                           "1-byte class per node; no matrix)",
+            "csr_equivalent": {"bytes_per_node_step": csr,
+                               "node_steps_per_s_at_peak": round(peak * 1e9 / csr, 1),
+                               "note": "the survey's assembled-CSR byte model; a CSR solver at the HBM peak "
+                                       "reaches this rate"},
             "per_kernel": {"ode_kernel": {"ms": round(o["ms_ode"], 4), "algorithmic_bytes": b_ode,
                                           "achieved_gbs": round(ach_ode, 1)},
                            "cg_kernel": {"ms": round(o["ms_cg"], 4), "algorithmic_bytes": int(b_cg),
                                          "achieved_gbs": round(ach_cg, 1)}}}
 
 
-def cpu_baseline(wl, seconds=15.0, threads=None):
-    """The CPU oracle (a C++ restatement of Chaste's step) on the host cores, bounded sample."""
+def cpu_baseline(wl, start_steps, seconds=15.0, threads=None):
+    """The CPU oracle (a C++ restatement of Chaste's step) on the host cores: advanced
+    untimed to the start of the timed window, then a bounded sample of steps."""
     from oracle import pyoracle as O
 
     threads = threads or os.cpu_count() or 1
@@ -266,20 +310,21 @@ def cpu_baseline(wl, seconds=15.0, threads=None):
     cfg = O.Config(wl["model"], wl["method"], wl["dt_ode"], wl["dt_pde"], 1400.0, 1.0, O.PC_JACOBI, 0,
                    wl["rel_tol"], 0, 10000)
     sig = np.tile(np.asarray(wl["sigma"][: wl["dim"]]), (conn.shape[0], 1))
-    inside = np.ones(xyz.shape[0], bool)
-    for d, hi in enumerate(wl["box_hi"][: wl["dim"]]):
-        inside &= xyz[:, d] <= hi + 1e-12
-    t = O.Tissue(cfg, wl["dim"], xyz, conn, sig, np.where(inside, 0, -1).astype(np.int32),
-                 [O.simple(*wl["stim"])])
-    t.step(1)
+    pset, ptab = transmural_cells(wl, xyz)
+    t = O.Tissue(cfg, wl["dim"], xyz, conn, sig, stimulated(wl, xyz), [O.simple(*wl["stim"])],
+                 param_id=pset, param_table=ptab)
+    ta = time.perf_counter()
+    t.step(max(1, start_steps))
+    t_adv = time.perf_counter() - ta
     k, t0 = 0, time.perf_counter()
     while time.perf_counter() - t0 < seconds and k < 200:
         t.step(1)
         k += 1
     dt = time.perf_counter() - t0
+    t_ms = max(1, start_steps) * wl["dt_pde"]
     return {"value": xyz.shape[0] * k / dt, "unit": "node-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{k} PDE steps of the full {xyz.shape[0]}-node workload after 1 warm-up step, "
-                      f"{dt:.1f} s, FP64, {threads} threads"}
+            "sample": f"{k} PDE steps of the full {xyz.shape[0]}-node workload from t = {t_ms:g} ms "
+                      f"(reached untimed in {t_adv:.1f} s), {dt:.1f} s, FP64, {threads} threads"}
 
 
 def run_population(args):
@@ -430,9 +475,12 @@ def main():
                     choices=sorted(WORKLOADS) + ["tt06_population", "lr91_cable_adjoint"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--t-start-ms", type=float, default=10.0,
+                    help="simulated time reached, untimed, before the warm-up and timed steps")
     ap.add_argument("--profile", choices=["fp64", "mixed"],
-                    help="only build the workload's tissue in this precision and take --steps steps "
-                         "(the program the ncu captures in profiles/ run)")
+                    help="only build the workload's tissue in this precision, advance it to --t-start-ms and "
+                         "take --steps steps with an L2 flush before each (the program the ncu captures in "
+                         "profiles/ run)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.profile:
@@ -442,8 +490,14 @@ def main():
         from chaste_b200.build import build_native
 
         build_native()
-        t = build_tissue(N, WORKLOADS[args.workload], 0 if args.profile == "fp64" else 1, 0)
-        t.step(args.steps)
+        wl = WORKLOADS[args.workload]
+        t = build_tissue(N, wl, 0 if args.profile == "fp64" else 1, 0)
+        t.step(start_steps(args, wl))
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda:0")
+        for _ in range(args.steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            t.step(1)
         torch.cuda.synchronize()
         st = t.stats()
         print(json.dumps({"profile": args.profile, "workload": args.workload, "steps": int(st.steps),
@@ -463,12 +517,14 @@ def main():
         # Chaste's own CPU path (PETSc/MPI) cannot be built here; its restatement
         # (the oracle port) is timed on every host core, rank 0 only.
         if rank == 0:
-            cb = cpu_baseline(wl, seconds=max(5.0, args.cpu_seconds))
+            cb = cpu_baseline(wl, start_steps(args, wl), seconds=max(5.0, args.cpu_seconds))
             v = cb["value"]
             line = {"impl": "reference", "metric": metric, "value": v, "unit": "node-steps/s",
                     "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                     "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-                    "config": {"workload": wl["name"]}, "cpu_baseline": cb,
+                    "config": {"workload": wl["name"], "t_start_ms": args.t_start_ms,
+                               "window": "oracle port advanced untimed to t_start_ms, then timed"},
+                    "cpu_baseline": cb,
                     "e2e": {"value": v, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(line), flush=True)
         if dist:
@@ -496,6 +552,9 @@ def main():
                        "solver": "CG+Jacobi rtol 1e-8 (PETSc convergence test)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "flushed (256 MB write) before every timed step",
+                       "t_start_ms": args.t_start_ms,
+                       "window": f"timed steps start at t = {args.t_start_ms + args.warmup * wl['dt_pde']:g} ms "
+                                 f"(after {args.t_start_ms:g} ms untimed and {args.warmup} warm-up steps)",
                        "headline_precision": head},
             "fp64": res["out"]["fp64"], "mixed": res["out"]["mixed"],
             "mixed_vs_fp64": {"max_abs_vm_mv": res["vm_err"],
@@ -507,7 +566,7 @@ def main():
             "clocks": o["clocks"],
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(wl, seconds=args.cpu_seconds)
+            line["cpu_baseline"] = cpu_baseline(wl, start_steps(args, wl), seconds=args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -65,6 +65,7 @@ class Stats(C.Structure):
         ("max_cg_iterations", C.c_int), ("total_cg_iterations", C.c_longlong),
         ("refinement_sweeps", C.c_int), ("operator_kind", C.c_int), ("status_bits", C.c_int),
         ("ms_last_call", C.c_double), ("pipelined_nodes_per_thread", C.c_int), ("cg_blocks", C.c_int),
+        ("inner_preconditioner", C.c_int),
     ]
 
 
@@ -100,6 +101,7 @@ SIGNATURES = {
     "cg_get_activation_times": (C.c_int, [_vp, _dp]),
     "cg_get_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
     "cg_get_iteration_history": (C.c_int, [_vp, C.c_int, _ip]),
+    "cg_apply_inner_preconditioner": (C.c_int, [_vp, _dp, _dp]),
     "cg_num_nodes": (C.c_int, [_vp, _ip]),
     "cg_num_states": (C.c_int, [C.c_int, _ip]),
     "cg_num_params": (C.c_int, [C.c_int, _ip]),
@@ -279,6 +281,13 @@ class Tissue:
         it = np.zeros(n, dtype=np.int32)
         check(lib().cg_get_iteration_history(self.h, n, iptr(it)), "cg_get_iteration_history")
         return it
+
+    def apply_inner_preconditioner(self, x):
+        """B x for the mixed solve's x-line inner preconditioner (a diagnostic)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n)
+        check(lib().cg_apply_inner_preconditioner(self.h, dptr(x), dptr(y)), "cg_apply_inner_preconditioner")
+        return y
 
     # -- printing-step output on the device
     def configure_output(self, printing_steps, max_frames, state_vars=()):

@@ -15,7 +15,8 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"
 SOURCES = ["chaste_gpu.cu", "noalloc.cu", "batch.cu", "cable.cu", "selftest.cu", "host/assemble.cpp"]
 DEPS = SOURCES + [
     "kernels/common.cuh", "kernels/ops.cuh", "kernels/cg.cuh", "kernels/cg_mixed.cuh",
-    "kernels/ode.cuh", "kernels/batch.cuh", "kernels/cable.cuh", "kernels/svi.cuh", "models/cellmodel_common.h", "models/lr91.h", "models/tt06.h",
+    "kernels/ode.cuh", "kernels/batch.cuh", "kernels/cable.cuh", "kernels/svi.cuh", "kernels/output.cuh",
+    "models/cellmodel_common.h", "models/lr91.h", "models/tt06.h",
     "host/assemble.h", "../../include/chaste_gpu.h",
 ]
 

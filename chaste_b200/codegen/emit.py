@@ -482,6 +482,22 @@ class ModelEmitter:
             inf = -g / h
             self.rl[s] = (inf, h)
 
+    def _state_deps(self, exprs):
+        """States the expressions depend on, through the live algebraic variables
+        (the stimulus and the capacitance count as a state: they change per substep)."""
+        seen, out = set(), set()
+        stack = [x for e in exprs for x in _free(e)]
+        while stack:
+            s_ = stack.pop()
+            if s_ in seen:
+                continue
+            seen.add(s_)
+            if s_ in self.states or s_ in (self.stim_arg, self.cm_arg, self.m.time):
+                out.add(s_)
+            elif s_ in self.live:
+                stack.extend(_free(self.live[s_]))
+        return out
+
     # ------------------------------------------------------------------ emit
     def cname(self, s):
         if s == self.stim_arg:
@@ -630,6 +646,53 @@ class ModelEmitter:
                 A(f"        rate[{i}] = {pr(self._fold_expr(self.odes[s]))};")
         A("    }")
         A("")
+        # ---- the same terms split by what they depend on (V clamped over a PDE step)
+        vonly = [s_ for s_ in self.states[1:] if s_ in self.rl and self._state_deps(self.rl[s_]) <= {V}]
+        vflags = ", ".join("true" if s_ in vonly else "false" for s_ in self.states)
+        vidx = " || ".join(f"i == {self.states.index(s_)}" for s_ in vonly) or "false"
+        A("    // Rush-Larsen states whose (inf, rate) depend on the voltage alone (and the")
+        A("    // parameters): with V clamped over a PDE step (ComputeExceptVoltage) their terms,")
+        A("    // and so exp(rate*dt), are the same in every substep.")
+        A(f"    static constexpr bool kRlVoltageOnly[{n}] = {{{vflags}}};")
+        A(f"    CHB_HD static constexpr bool rl_voltage_only(int i) {{ return {vidx}; }}")
+        A("    // rl_terms of the voltage-only Rush-Larsen states (reads y[0] and p only).")
+        A("    template <typename T>")
+        A("    CHB_HD static void rl_terms_voltage(const T* __restrict__ y, const T* __restrict__ p,")
+        A("                                       T* __restrict__ rate, T* __restrict__ inf) {")
+        A("        (void)p;")
+        v_exprs = []
+        for s_ in vonly:
+            v_exprs += list(self.rl[s_])
+        lines.extend(self._body(v_exprs, pr))
+        for s_ in vonly:
+            i = self.states.index(s_)
+            inf, h = self.rl[s_]
+            A(f"        inf[{i}] = {pr(self._fold_expr(inf))};")
+            A(f"        rate[{i}] = {pr(self._fold_expr(h))};")
+        A("    }")
+        A("    // rl_terms of every other non-voltage state (no dV/dt).")
+        A("    template <typename T>")
+        A("    CHB_HD static void rl_terms_states(const T* __restrict__ y, T stim, T cm,")
+        A("                                       const T* __restrict__ p, T* __restrict__ rate,")
+        A("                                       T* __restrict__ inf) {")
+        A("        (void)stim; (void)cm; (void)p; (void)inf;")
+        r_exprs = []
+        for s_ in self.states[1:]:
+            if s_ in vonly:
+                continue
+            r_exprs += list(self.rl[s_]) if s_ in self.rl else [self.odes[s_]]
+        lines.extend(self._body(r_exprs, pr))
+        for i, s_ in enumerate(self.states):
+            if i == 0 or s_ in vonly:
+                continue
+            if s_ in self.rl:
+                inf, h = self.rl[s_]
+                A(f"        inf[{i}] = {pr(self._fold_expr(inf))};")
+                A(f"        rate[{i}] = {pr(self._fold_expr(h))};")
+            else:
+                A(f"        rate[{i}] = {pr(self._fold_expr(self.odes[s_]))};")
+        A("    }")
+        A("")
         # ---- iionic
         conv = "cm" if self.current_per_cap else None
         tot = sp.Add(*self.currents, evaluate=False)
@@ -759,7 +822,10 @@ def main(argv=None):
     here = os.path.dirname(os.path.abspath(__file__))
     repo = os.path.dirname(os.path.dirname(here))
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--cellml-dir", default="/root/reference/heart/src/odes/cellml")
+    # the Chaste source tree: --cellml-dir, else $CHASTE_SOURCE_DIR/heart/src/odes/cellml
+    src = os.environ.get("CHASTE_SOURCE_DIR")
+    ap.add_argument("--cellml-dir", default=os.path.join(src, "heart", "src", "odes", "cellml") if src else None,
+                    required=src is None)
     ap.add_argument("--out", nargs="*", default=[os.path.join(repo, "chaste_b200", "csrc", "models")])
     a = ap.parse_args(argv)
     for p in generate(a.cellml_dir, a.out):

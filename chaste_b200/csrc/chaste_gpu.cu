@@ -108,7 +108,8 @@ struct cg_ctx {
     size_t pipe_smem = 0; // dynamic shared memory of that launch
     int diag_slot = 0;
     int xm_slot = -1, xp_slot = -1;   // stencil slots of offsets -1 and +1
-    bool line_pc = false;             // the pipelined mixed solve uses the x-line inner preconditioner
+    bool line_pc = false;             // the mixed slab solve uses the x-line inner preconditioner
+    float2* d_line_ad = nullptr;      // its factors (a_i, 1/d_i) per node
     // stats
     long long steps = 0;
     long long total_iters = 0;
@@ -463,6 +464,8 @@ int alloc_vectors(cg_ctx* c) {
     c->cg_threads = 512;
     const int blocks_512 = c->cg_blocks;
     c->pipe_nodes = 0;
+    const bool want_line = c->d_line_ad != nullptr;
+    c->line_pc = want_line;
     if (c->mixed() && c->slab && pick_pipe(c, 1)) {
         // one block of kPipeThreads per SM when the slab fills every SM with them (fewer
         // arrivals per grid reduction), else blocks of 512 so small slabs still spread
@@ -474,7 +477,6 @@ int alloc_vectors(cg_ctx* c) {
             CgKernel kern0 = pick_pipe(c, (int)k0);
             // the x-line factors live after the staged windows; without room for both
             // the inner solve keeps Jacobi
-            c->line_pc = c->cfg.mixed_inner_preconditioner == CG_INNER_PC_LINE && c->xm_slot >= 0 && c->xp_slot >= 0;
             auto smem_of = [&](long long k) {
                 return (size_t)k * ((size_t)c->stage.cap + (c->line_pc ? (size_t)kLineCoef * pt : 0)) * sizeof(float);
             };
@@ -508,10 +510,37 @@ int alloc_vectors(cg_ctx* c) {
             }
         }
     }
+    // the HBM-resident mixed solve takes the x-line preconditioner whenever it is asked for
+    if (c->pipe_nodes == 0) c->line_pc = want_line;
     CG_TRY(dalloc(c, &c->d_partials,
                   (size_t)2 * std::max(blocks_512, c->cg_blocks) * kPartialStride * sizeof(double)));
     c->ode_blocks = (int)std::max(1LL, std::min(((long long)n + 255) / 256, (long long)sms * 16));
     CG_CUDA(cudaStreamSynchronize(s));
+    return CG_OK;
+}
+
+// Factors of the mixed solve's x-line inner preconditioner (kernels/cg_mixed.cuh):
+// T = L D L^T on each segment of 32 nodes aligned on a multiple of 32, T the
+// tridiagonal x part of A (sub-diagonal = the coefficient of offset -1, cut at the
+// segment start), in FP64; stored per node as (a_i = -T_{i,i-1} / d_{i-1}, 1 / d_i).
+int build_line_factors(cg_ctx* c, const std::vector<uint8_t>& cls) {
+    const SlabStencil& st = c->stencil;
+    const int no = st.n_offsets;
+    std::vector<float2> ad((size_t)c->n);
+    double dprev = 1.0;
+    for (int i = 0; i < c->n; ++i) {
+        const double* row = &st.a[(size_t)cls[i] * no];
+        const double di = row[c->diag_slot];
+        const double lo = (i % 32 == 0) ? 0.0 : row[c->xm_slot];
+        const double l = lo / dprev;
+        const double d = di - l * lo;
+        if (!(d > 0.0)) return CG_ERR_ARG;   // A is SPD, so every pivot is positive
+        ad[i] = make_float2((float)(-l), (float)(1.0 / d));
+        dprev = d;
+    }
+    CG_TRY(dalloc(c, &c->d_line_ad, ad.size() * sizeof(float2)));
+    CG_CUDA(cudaMemcpyAsync(c->d_line_ad, ad.data(), ad.size() * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
     return CG_OK;
 }
 
@@ -554,6 +583,8 @@ int upload_operator(cg_ctx* c) {
             if (st.offsets[o] == 1) c->xp_slot = o;
         }
         if (c->diag_slot < 0) return CG_ERR_ARG;
+        if (c->mixed() && c->cfg.mixed_inner_preconditioner == CG_INNER_PC_LINE && c->xm_slot >= 0)
+            CG_TRY(build_line_factors(c, cls));
         CG_CUDA(cudaStreamSynchronize(s));
     } else {
         const HostCsr& m = c->csr;
@@ -874,7 +905,8 @@ CgArgs make_cg_args(cg_ctx* c) {
     a.diag_slot = c->diag_slot;
     a.xm_slot = c->xm_slot;
     a.xp_slot = c->xp_slot;
-    a.line_pc = c->pipe_nodes > 0 && c->line_pc ? 1 : 0;
+    a.line_pc = c->line_pc ? 1 : 0;
+    a.line_ad = c->d_line_ad;
     a.max_refine = 20;
     return a;
 }
@@ -1237,6 +1269,7 @@ int cg_get_stats(cg_ctx* c, cg_stats* s) {
     s->ms_last_call = c->ms_last;
     s->pipelined_nodes_per_thread = c->pipe_nodes;
     s->cg_blocks = c->cg_blocks;
+    s->inner_preconditioner = !c->mixed() ? -1 : (c->line_pc ? CG_INNER_PC_LINE : CG_INNER_PC_JACOBI);
     if (c->have_cells && c->steps > 0) {
         CG_CUDA(cudaSetDevice(c->device));
         CG_CUDA(cudaMemcpy(&s->last_cg_iterations, c->d_ring + ((c->steps - 1) % kRing), sizeof(int),
@@ -1245,6 +1278,37 @@ int cg_get_stats(cg_ctx* c, cg_stats* s) {
         CG_CUDA(cudaMemcpy(&s->status_bits, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     }
     return CG_OK;
+}
+
+int cg_apply_inner_preconditioner(cg_ctx* c, const double* x, double* y) {
+    if (!c || !x || !y) return CG_ERR_ARG;
+    if (!c->have_mesh) return CG_ERR_ORDER;
+    if (!c->line_pc || !c->d_line_ad) return CG_ERR_UNSUPPORTED;
+    CG_CUDA(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->n;
+    std::vector<float> h(n);
+    for (size_t i = 0; i < n; ++i) h[i] = (float)x[i];
+    float* d = nullptr;
+    if (cudaMalloc(&d, 2 * n * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return CG_ERR_NOMEM;
+    }
+    int rc = CG_OK;
+    if (cudaMemcpyAsync(d, h.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
+        rc = CG_ERR_CUDA;
+    } else {
+        const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)c->ode_blocks);
+        line_pc_apply_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->n, c->d_line_ad, d, d + n);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(h.data(), d + n, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess)
+            rc = CG_ERR_CUDA;
+    }
+    cudaFree(d);
+    cudaGetLastError();
+    if (rc == CG_OK)
+        for (size_t i = 0; i < n; ++i) y[i] = (double)h[i];
+    return rc;
 }
 
 int cg_get_iteration_history(cg_ctx* c, int n, int* it) {

@@ -68,7 +68,8 @@ struct CgArgs {
     int pc;                     // 0 none, 1 jacobi
     int diag_slot;
     int xm_slot, xp_slot;       // stencil slots of the x-neighbours (offsets -1, +1)
-    int line_pc;                // pipelined mixed solve: inner preconditioner on x-line segments
+    int line_pc;                // mixed slab solve: inner preconditioner on x-line segments
+    const float2* line_ad;      // its factors (a_i, 1/d_i) per node
     int max_refine;
 };
 

@@ -10,8 +10,6 @@
 // as the FP64 kernel (one operator application per iteration).
 #pragma once
 
-#include <cuda_fp16.h>
-
 #include "cg.cuh"
 
 namespace chb {
@@ -53,6 +51,113 @@ __device__ __forceinline__ float apply_row32(const CgArgs& a, const SlabShared<f
     }
 }
 
+// Inner preconditioner of the mixed solve on the slab stencil: T^-1 d, where T is the
+// tridiagonal part of A along x (the direction of the largest conductivity)
+// restricted to the 32 consecutive nodes a warp holds (rows cut at the warp's ends
+// and, through the stencil, at the ends of each x-line).  T is a principal
+// block-diagonal part of the SPD matrix A, so it is SPD.
+//
+// T = L D L^T with L unit lower bidiagonal (l_i = T_{i,i-1} / d_{i-1},
+// d_i = T_ii - l_i T_{i,i-1}), so T^-1 = F^T D^-1 F with F = L^-1.  F applies the
+// recurrence y_i = v_i + a_i y_{i-1} (a_i = -l_i, a_0 = 0) as a Hillis-Steele scan
+// over the warp: five levels s = 1, 2, 4, 8, 16 of y_i += A^(s)_i y_{i-s}, where
+// A^(s)_i is the product of the s coefficients a_{i-s+1..i} (zero for i < s, since
+// a_0 = 0).  The application is B d = F^T (D^-1 (F d)): the scan, a scaling, then the
+// transposed levels in reverse order (z_i += A^(s)_{i+s} z_{i+s}).  B is therefore
+// symmetric for the stored coefficients whatever their rounding, and positive
+// definite while every d_i > 0: a fixed SPD operator, as CG needs.  The pivots depend
+// on A only: the host computes (a_i, 1/d_i) per node once, in FP64 rounded to FP32
+// (CgArgs::line_ad, segments of 32 nodes aligned on multiples of 32, which are the
+// nodes one warp holds in one register slot or grid-stride step).  A solve forms the
+// five A^(s) from a_i by four shuffle levels (warp_line_levels); an application is
+// then 10 shuffles and 11 multiply-adds.  Every lane of the warp takes part; the rows
+// of nodes past n are the identity (a = 0, 1/d = 1).
+constexpr int kLineCoef = 6;   // A^(1), A^(2), A^(4), A^(8), A^(16), 1 / d
+
+__device__ __forceinline__ void warp_line_levels(float a, float (&A)[5]) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    A[0] = a;
+#pragma unroll
+    for (int j = 1; j < 5; ++j) {
+        const int s = 1 << (j - 1);
+        const float Am = __shfl_up_sync(full, A[j - 1], s);
+        A[j] = lane >= s ? A[j - 1] * Am : 0.0f;
+    }
+}
+
+__device__ __forceinline__ float warp_line_solve(const float (&A)[5], float dinv, float v) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    // y = F v
+#pragma unroll
+    for (int j = 0; j < 5; ++j) v += A[j] * __shfl_up_sync(full, v, 1 << j);
+    // z = F^T D^-1 y
+    float z = v * dinv;
+#pragma unroll
+    for (int j = 4; j >= 0; --j) {
+        const int s = 1 << j;
+        const float t = __shfl_down_sync(full, A[j] * z, s);
+        if (lane + s < 32) z += t;
+    }
+    return z;
+}
+
+// Per-slot factors kept in shared memory by the pipelined solve.
+__device__ __forceinline__ void warp_line_setup(float2 ad, float* cf, int ld) {
+    float A[5];
+    warp_line_levels(ad.x, A);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) cf[j * ld] = A[j];
+    cf[5 * ld] = ad.y;
+}
+
+__device__ __forceinline__ float warp_line_apply(const float* cf, int ld, float v) {
+    float A[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) A[j] = cf[j * ld];
+    return warp_line_solve(A, cf[5 * ld], v);
+}
+
+// (a_i, 1/d_i) of node i, identity for nodes past n.
+__device__ __forceinline__ float2 line_factors(const CgArgs& a, bool on, int i) {
+    return on ? __ldg(a.line_ad + i) : make_float2(0.0f, 1.0f);
+}
+
+// y = B x with the x-line inner preconditioner alone (cg_apply_inner_preconditioner):
+// the same segments and factors the mixed solves use.
+__global__ void line_pc_apply_kernel(int n, const float2* __restrict__ ad, const float* __restrict__ x,
+                                     float* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + threadIdx.x - lane; base < n; base += stride) {
+        const int i = base + lane;
+        const bool on = i < n;
+        const float2 f = on ? ad[i] : make_float2(0.0f, 1.0f);
+        float A[5];
+        warp_line_levels(f.x, A);
+        const float z = warp_line_solve(A, f.y, on ? x[i] : 0.0f);
+        if (on) y[i] = z;
+    }
+}
+
+// The inner preconditioner of this kernel at node i (warp-synchronous: every lane of
+// the warp calls it, `on` false past n): the x-line solve on slab stencils when
+// a.line_pc is set, else Jacobi.
+template <bool SLAB>
+__device__ __forceinline__ float inner_pc32(const CgArgs& a, const SlabShared<float>& s32, int c, int i, bool on,
+                                            float r) {
+    if constexpr (SLAB) {
+        if (a.line_pc) {
+            float A[5];
+            const float2 ad = line_factors(a, on, i);
+            warp_line_levels(ad.x, A);
+            return warp_line_solve(A, ad.y, on ? r : 0.0f);
+        }
+    }
+    return on ? dinv32_of<SLAB>(a, s32, c, i) * r : 0.0f;
+}
+
 template <bool SLAB, int NOFF>
 __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& round) {
     __shared__ SlabShared<double> sh;
@@ -68,7 +173,10 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
     const long long step = *a.step;
     const int n = a.n;
     const int stride = gridDim.x * blockDim.x;
-    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    // warp-uniform grid-stride loops: a warp visits the 32 consecutive nodes
+    // base .. base + 31 together (the x-line preconditioner's segment)
+    const int lane = threadIdx.x & 31;
+    const int w0 = blockIdx.x * blockDim.x + threadIdx.x - lane;
     double* __restrict__ x = a.x;
     float* __restrict__ r32 = a.r32;
     float* __restrict__ z32 = a.z32;
@@ -84,21 +192,27 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
     // ---- FP64 residual r = M z - A x (stored in FP64), its FP32 copy and B r
     {
         double v[4] = {0, 0, 0, 0};
-        for (int i = t0; i < n; i += stride) {
-            const int c = class_of<SLAB>(a, i);
-            const double b = apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs32) + (a.corr ? a.corr[i] : 0.0);
-            const double av = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, x);
-            const double rr = b - av;
-            const double d = dinv_of<SLAB>(a, sh, c, i);
-            const double w = d * b, zz = d * rr;
-            v[0] += fabs(b);
-            v[1] += w * w;
-            v[2] += zz * zz;
-            const float rf = (float)rr;
-            const float zf = dinv32_of<SLAB>(a, s32, c, i) * rf;
-            r[i] = rr;
-            r32[i] = rf;
-            z32[i] = zf;
+        for (int base = w0; base < n; base += stride) {
+            const int i = base + lane;
+            const bool on = i < n;
+            const int c = on ? class_of<SLAB>(a, i) : 0;
+            float rf = 0.0f;
+            if (on) {
+                const double b =
+                    apply_row<SLAB, NOFF, true>(a, sh, soff, c, i, a.zrhs32) + (a.corr ? a.corr[i] : 0.0);
+                const double av = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, x);
+                const double rr = b - av;
+                const double d = dinv_of<SLAB>(a, sh, c, i);
+                const double w = d * b, zz = d * rr;
+                v[0] += fabs(b);
+                v[1] += w * w;
+                v[2] += zz * zz;
+                rf = (float)rr;
+                r[i] = rr;
+                r32[i] = rf;
+            }
+            const float zf = inner_pc32<SLAB>(a, s32, c, i, on, rf);
+            if (on) z32[i] = zf;
             v[3] += (double)rf * (double)zf;
         }
         if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
@@ -134,7 +248,9 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
             const bool first = it == 0;
             {
                 double v[1] = {0};
-                for (int i = t0; i < n; i += stride) {
+                for (int base = w0; base < n; base += stride) {
+                    const int i = base + lane;
+                    if (i >= n) continue;
                     const int c = class_of<SLAB>(a, i);
                     const float az = apply_row32<SLAB, NOFF>(a, s32, soff, c, i, z32);
                     const float qi = first ? az : az + bc * q32[i];
@@ -150,13 +266,18 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
             const float alpha = (float)(beta / dpi);
             {
                 double v[2] = {0, 0};
-                for (int i = t0; i < n; i += stride) {
-                    const int c = class_of<SLAB>(a, i);
-                    e32[i] = first ? alpha * p32[i] : e32[i] + alpha * p32[i];
-                    const float rr = r32[i] - alpha * q32[i];
-                    r32[i] = rr;
-                    const float zz = dinv32_of<SLAB>(a, s32, c, i) * rr;
-                    z32[i] = zz;
+                for (int base = w0; base < n; base += stride) {
+                    const int i = base + lane;
+                    const bool on = i < n;
+                    const int c = on ? class_of<SLAB>(a, i) : 0;
+                    float rr = 0.0f;
+                    if (on) {
+                        e32[i] = first ? alpha * p32[i] : e32[i] + alpha * p32[i];
+                        rr = r32[i] - alpha * q32[i];
+                        r32[i] = rr;
+                    }
+                    const float zz = inner_pc32<SLAB>(a, s32, c, i, on, rr);
+                    if (on) z32[i] = zz;
                     v[0] += (double)zz * (double)zz;
                     v[1] += (double)zz * (double)rr;
                 }
@@ -176,18 +297,23 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
         // ---- refinement in FP64: x += e, r -= A e (e of the neighbours is complete)
         {
             double v[2] = {0, 0};
-            for (int i = t0; i < n; i += stride) {
-                const int c = class_of<SLAB>(a, i);
-                const double ae = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, e32);
-                x[i] += (double)e32[i];
-                const double rr = r[i] - ae;
-                r[i] = rr;
-                const double zz = dinv_of<SLAB>(a, sh, c, i) * rr;
-                const float rf = (float)rr;
-                const float zf = dinv32_of<SLAB>(a, s32, c, i) * rf;
-                r32[i] = rf;
-                z32[i] = zf;
-                v[0] += zz * zz;
+            for (int base = w0; base < n; base += stride) {
+                const int i = base + lane;
+                const bool on = i < n;
+                const int c = on ? class_of<SLAB>(a, i) : 0;
+                float rf = 0.0f;
+                if (on) {
+                    const double ae = apply_row<SLAB, NOFF, false>(a, sh, soff, c, i, e32);
+                    x[i] += (double)e32[i];
+                    const double rr = r[i] - ae;
+                    r[i] = rr;
+                    const double zz = dinv_of<SLAB>(a, sh, c, i) * rr;
+                    rf = (float)rr;
+                    r32[i] = rf;
+                    v[0] += zz * zz;
+                }
+                const float zf = inner_pc32<SLAB>(a, s32, c, i, on, rf);
+                if (on) z32[i] = zf;
                 v[1] += (double)rf * (double)zf;
             }
             if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
@@ -335,71 +461,6 @@ __device__ __forceinline__ float apply_a32_staged(const CgArgs& a, const SlabSha
     return acc;
 }
 
-// Inner preconditioner of the pipelined solve on the slab stencil: T^-1 d, where T is
-// the tridiagonal part of A along x (the direction of the largest conductivity)
-// restricted to the 32 consecutive nodes a warp holds in one register slot (rows cut
-// at the warp's ends and, through the stencil, at the ends of each x-line).  T is a
-// principal block-diagonal part of the SPD matrix A, so it is SPD and fixed, as CG
-// needs.  Solved by parallel cyclic reduction over 5 levels of warp shuffles.  The
-// elimination factors depend on T only, so they are computed once per solve
-// (warp_line_setup) into kLineCoef words of shared memory per slot and thread (the
-// factors in half precision: they only shape the preconditioner, which stays a fixed
-// operator); each application (warp_line_apply) is then 10 shuffles and 10 FMAs.
-// Every lane of the warp takes part; the rows of nodes past n are the identity.
-constexpr int kLineCoef = 6;   // per level the two factors as one half2 word, then 1 / the reduced diagonal
-
-__device__ __forceinline__ void warp_line_setup(float lo, float di, float up, float* cf, int ld) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    if (lane == 0) lo = 0.0f;
-    if (lane == 31) up = 0.0f;
-    int j = 0;
-#pragma unroll
-    for (int s = 1; s < 32; s <<= 1, ++j) {
-        const float am = __shfl_up_sync(full, lo, s), bm = __shfl_up_sync(full, di, s);
-        const float cm = __shfl_up_sync(full, up, s);
-        const float ap = __shfl_down_sync(full, lo, s), bp = __shfl_down_sync(full, di, s);
-        const float cp = __shfl_down_sync(full, up, s);
-        const float k1 = lane >= s ? lo / bm : 0.0f;
-        const float k2 = lane + s < 32 ? up / bp : 0.0f;
-        di = di - k1 * cm - k2 * ap;
-        lo = -k1 * am;
-        up = -k2 * cp;
-        reinterpret_cast<__half2*>(cf)[j * ld] = __floats2half2_rn(k1, k2);
-    }
-    cf[5 * ld] = 1.0f / di;
-}
-
-__device__ __forceinline__ float warp_line_apply(const float* cf, int ld, float d) {
-    const unsigned full = 0xffffffffu;
-    int j = 0;
-#pragma unroll
-    for (int s = 1; s < 32; s <<= 1, ++j) {
-        const float dm = __shfl_up_sync(full, d, s);
-        const float dp = __shfl_down_sync(full, d, s);
-        const float2 k = __half22float2(reinterpret_cast<const __half2*>(cf)[j * ld]);
-        d = d - k.x * dm - k.y * dp;
-    }
-    return d * cf[5 * ld];
-}
-
-// T's three coefficients for a node of stencil class c (identity for nodes past n).
-template <int NOFF>
-__device__ __forceinline__ void line_row(const CgArgs& a, const SlabShared<float>& s32, bool on, int c, float& lo,
-                                         float& di, float& up) {
-    lo = 0.0f, di = 1.0f, up = 0.0f;
-    if (!on) return;
-    if (c == a.slab.interior) {
-        lo = a.slab.ia32[a.xm_slot];
-        di = a.slab.ia32[a.diag_slot];
-        up = a.slab.ia32[a.xp_slot];
-    } else {
-        lo = s32.a[c * NOFF + a.xm_slot];
-        di = s32.a[c * NOFF + a.diag_slot];
-        up = s32.a[c * NOFF + a.xp_slot];
-    }
-}
-
 // B d for register slot k: the x-line solve (a.line_pc) or Jacobi.
 __device__ __forceinline__ float apply_inner_pc(const CgArgs& a, const float* cf, int ld, bool on, float dinv,
                                                 float d) {
@@ -444,11 +505,8 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
     }
     if (a.line_pc) {
 #pragma unroll
-        for (int k = 0; k < KMAX; ++k) {
-            float lo, di, up;
-            line_row<NOFF>(a, s32, on[k], cls[k], lo, di, up);
-            warp_line_setup(lo, di, up, line_cf + k * kLineCoef * ld + threadIdx.x, ld);
-        }
+        for (int k = 0; k < KMAX; ++k)
+            warp_line_setup(line_factors(a, on[k], node[k]), line_cf + k * kLineCoef * ld + threadIdx.x, ld);
     }
     float r[KMAX], u[KMAX], w[KMAX], m[KMAX], zq[KMAX], q[KMAX], sv[KMAX], p[KMAX], e[KMAX];
     double res[4];

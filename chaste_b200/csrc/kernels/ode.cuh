@@ -154,6 +154,9 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
                 y[0] = (T)v;
             }
         } else {
+            // Rush-Larsen: the voltage-only gates' terms once per PDE step (V is clamped)
+            T vinf[S], vfac[S];
+            if (METHOD == 1) rl_freeze_voltage_terms<M, T>(y, p, (T)a.dt_ode, vinf, vfac);
             DevTimeStepper ts(t0, t1, a.dt_ode);
             while (!ts.at_end()) {
                 // cell stimulus in uA/cm^2 = tissue stimulus / Am (GetIntracellularAreaStimulus);
@@ -161,7 +164,7 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
                 const double sv = stimulus_value(st, ts.time);
                 const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
                 if (METHOD == 1) {
-                    rl_step_except_voltage<M, T>(y, s, cm, p, (T)a.dt_ode);
+                    rl_step_except_voltage_frozen<M, T>(y, s, cm, p, (T)a.dt_ode, vinf, vfac);
                 } else if (METHOD == 3) {
                     grl1_step<M, T, false>(y, s, cm, p, (T)(ts.next - ts.time));
                 } else if (METHOD == 4) {

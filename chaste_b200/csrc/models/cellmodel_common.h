@@ -130,6 +130,37 @@ CHB_UNROLL
     }
 }
 
+// The same Rush-Larsen step over the substeps of one PDE step, with the terms of the
+// voltage-only states (Model::rl_voltage_only) taken out of the substep loop: V is
+// clamped, so their inf and exp(rate*dt) are the values rl_step_except_voltage would
+// recompute at every substep.  rl_freeze_voltage_terms forms them once; each substep
+// then evaluates only the terms of the other states.
+template <class Model, typename T>
+CHB_HD void rl_freeze_voltage_terms(const T* y, const T* p, T dt, T* vinf, T* vfac) {
+    T rate[Model::kNumStates];
+    Model::template rl_terms_voltage<T>(y, p, rate, vinf);
+CHB_UNROLL
+    for (int i = 1; i < Model::kNumStates; ++i)
+        if (Model::rl_voltage_only(i)) vfac[i] = m_exp(rate[i] * dt);
+}
+
+template <class Model, typename T>
+CHB_HD void rl_step_except_voltage_frozen(T* y, T stim, T cm, const T* p, T dt, const T* vinf, const T* vfac) {
+    T rate[Model::kNumStates];
+    T inf[Model::kNumStates];
+    Model::template rl_terms_states<T>(y, stim, cm, p, rate, inf);
+CHB_UNROLL
+    for (int i = 1; i < Model::kNumStates; ++i) {
+        if (Model::rl_voltage_only(i)) {
+            y[i] = vinf[i] + (y[i] - vinf[i]) * vfac[i];
+        } else if (Model::rush_larsen(i)) {
+            y[i] = inf[i] + (y[i] - inf[i]) * m_exp(rate[i] * dt);
+        } else {
+            y[i] += dt * rate[i];
+        }
+    }
+}
+
 // Full single-cell steps including the voltage (Compute / SolveAndUpdateState).
 template <class Model, typename T>
 CHB_HD void fe_step(T* y, T stim, T cm, const T* p, T dt) {

@@ -114,6 +114,52 @@ struct LuoRudy1991 {
         rate[7] = (((m_divk((-T(0.0001)), T(1.0), T(1.0)))*v_slow_inward_current__i_si) + (T(0.07)*(T(0.0001) - y[7])));
     }
 
+    // Rush-Larsen states whose (inf, rate) depend on the voltage alone (and the
+    // parameters): with V clamped over a PDE step (ComputeExceptVoltage) their terms,
+    // and so exp(rate*dt), are the same in every substep.
+    static constexpr bool kRlVoltageOnly[8] = {false, true, true, true, true, true, true, false};
+    CHB_HD static constexpr bool rl_voltage_only(int i) { return i == 1 || i == 2 || i == 3 || i == 4 || i == 5 || i == 6; }
+    // rl_terms of the voltage-only Rush-Larsen states (reads y[0] and p only).
+    template <typename T>
+    CHB_HD static void rl_terms_voltage(const T* __restrict__ y, const T* __restrict__ p,
+                                       T* __restrict__ rate, T* __restrict__ inf) {
+        (void)p;
+        const T v_fast_sodium_current_m_gate__alpha_m = (((chb::singularity_offset<T>()*T(10.0)) > fabs((y[0] + T(47.13)))) ? ((m_div((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13))), (T(1.0) - m_exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13))))))) + (m_div((y[0] - (-T(47.13) - (chb::singularity_offset<T>()*T(10.0))))*((m_div((T(0.32)*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13))), (T(1.0) - m_exp(((-T(0.1))*((-T(47.13) + (chb::singularity_offset<T>()*T(10.0))) + T(47.13))))))) - (m_div((T(0.32)*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13))), (T(1.0) - m_exp(((-T(0.1))*((-T(47.13) - (chb::singularity_offset<T>()*T(10.0))) + T(47.13)))))))), (T(2.0)*(chb::singularity_offset<T>()*T(10.0)))))) : (m_div((T(0.32)*(y[0] + T(47.13))), (T(1.0) - m_exp(((-T(0.1))*(y[0] + T(47.13))))))));
+        const T v_fast_sodium_current_m_gate__beta_m = (T(0.08)*m_exp((m_divk((-y[0]), T(11.0), T(0.09090909090909091)))));
+        const T v_fast_sodium_current_h_gate__alpha_h = ((y[0] < (-T(40.0))) ? (T(0.135)*m_exp((m_div((T(80.0) + y[0]), (-T(6.8)))))) : T(0.0));
+        const T v_fast_sodium_current_h_gate__beta_h = ((y[0] < (-T(40.0))) ? ((T(3.56)*m_exp((T(0.079)*y[0]))) + (T(310000.0)*m_exp((T(0.35)*y[0])))) : (m_div(T(1.0), (T(0.13)*(T(1.0) + m_exp((m_div((y[0] + T(10.66)), (-T(11.1))))))))));
+        const T v_fast_sodium_current_j_gate__alpha_j = ((y[0] < (-T(40.0))) ? (m_div(((((-T(127140.0))*m_exp((T(0.2444)*y[0]))) - (T(3.474e-05)*m_exp(((-T(0.04391))*y[0]))))*(y[0] + T(37.78))), (T(1.0) + m_exp((T(0.311)*(y[0] + T(79.23))))))) : T(0.0));
+        const T v_fast_sodium_current_j_gate__beta_j = ((y[0] < (-T(40.0))) ? (m_div((T(0.1212)*m_exp(((-T(0.01052))*y[0]))), (T(1.0) + m_exp(((-T(0.1378))*(y[0] + T(40.14))))))) : (m_div((T(0.3)*m_exp(((-T(2.535e-07))*y[0]))), (T(1.0) + m_exp(((-T(0.1))*(y[0] + T(32.0))))))));
+        const T v_slow_inward_current_d_gate__alpha_d = (m_div((T(0.095)*m_exp(((-T(0.01))*(y[0] - T(5.0))))), (T(1.0) + m_exp(((-T(0.072))*(y[0] - T(5.0)))))));
+        const T v_slow_inward_current_d_gate__beta_d = (m_div((T(0.07)*m_exp(((-T(0.017))*(y[0] + T(44.0))))), (T(1.0) + m_exp((T(0.05)*(y[0] + T(44.0)))))));
+        const T v_slow_inward_current_f_gate__alpha_f = (m_div((T(0.012)*m_exp(((-T(0.008))*(y[0] + T(28.0))))), (T(1.0) + m_exp((T(0.15)*(y[0] + T(28.0)))))));
+        const T v_slow_inward_current_f_gate__beta_f = (m_div((T(0.0065)*m_exp(((-T(0.02))*(y[0] + T(30.0))))), (T(1.0) + m_exp(((-T(0.2))*(y[0] + T(30.0)))))));
+        const T v_time_dependent_potassium_current_X_gate__alpha_X = (m_div((T(0.0005)*m_exp((T(0.083)*(y[0] + T(50.0))))), (T(1.0) + m_exp((T(0.057)*(y[0] + T(50.0)))))));
+        const T v_time_dependent_potassium_current_X_gate__beta_X = (m_div((T(0.0013)*m_exp(((-T(0.06))*(y[0] + T(20.0))))), (T(1.0) + m_exp(((-T(0.04))*(y[0] + T(20.0)))))));
+        inf[1] = (-m_div(v_fast_sodium_current_m_gate__alpha_m, (-v_fast_sodium_current_m_gate__alpha_m - v_fast_sodium_current_m_gate__beta_m)));
+        rate[1] = (-v_fast_sodium_current_m_gate__alpha_m - v_fast_sodium_current_m_gate__beta_m);
+        inf[2] = (-m_div(v_fast_sodium_current_h_gate__alpha_h, (-v_fast_sodium_current_h_gate__alpha_h - v_fast_sodium_current_h_gate__beta_h)));
+        rate[2] = (-v_fast_sodium_current_h_gate__alpha_h - v_fast_sodium_current_h_gate__beta_h);
+        inf[3] = (-m_div(v_fast_sodium_current_j_gate__alpha_j, (-v_fast_sodium_current_j_gate__alpha_j - v_fast_sodium_current_j_gate__beta_j)));
+        rate[3] = (-v_fast_sodium_current_j_gate__alpha_j - v_fast_sodium_current_j_gate__beta_j);
+        inf[4] = (-m_div(v_slow_inward_current_d_gate__alpha_d, (-v_slow_inward_current_d_gate__alpha_d - v_slow_inward_current_d_gate__beta_d)));
+        rate[4] = (-v_slow_inward_current_d_gate__alpha_d - v_slow_inward_current_d_gate__beta_d);
+        inf[5] = (-m_div(v_slow_inward_current_f_gate__alpha_f, (-v_slow_inward_current_f_gate__alpha_f - v_slow_inward_current_f_gate__beta_f)));
+        rate[5] = (-v_slow_inward_current_f_gate__alpha_f - v_slow_inward_current_f_gate__beta_f);
+        inf[6] = (-m_div(v_time_dependent_potassium_current_X_gate__alpha_X, (-v_time_dependent_potassium_current_X_gate__alpha_X - v_time_dependent_potassium_current_X_gate__beta_X)));
+        rate[6] = (-v_time_dependent_potassium_current_X_gate__alpha_X - v_time_dependent_potassium_current_X_gate__beta_X);
+    }
+    // rl_terms of every other non-voltage state (no dV/dt).
+    template <typename T>
+    CHB_HD static void rl_terms_states(const T* __restrict__ y, T stim, T cm,
+                                       const T* __restrict__ p, T* __restrict__ rate,
+                                       T* __restrict__ inf) {
+        (void)stim; (void)cm; (void)p; (void)inf;
+        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*m_log((m_divk(y[7], T(1.0), T(1.0))))));
+        const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
+        rate[7] = (((m_divk((-T(0.0001)), T(1.0), T(1.0)))*v_slow_inward_current__i_si) + (T(0.07)*(T(0.0001) - y[7])));
+    }
+
     // Total ionic current in uA/cm^2 (GetIIonic): the dV/dt currents without
     // the stimulus.
     template <typename T>

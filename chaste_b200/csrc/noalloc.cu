@@ -19,7 +19,9 @@
 // In host code the array's name is only a host-side stand-in, not a device
 // address.  The first call on each device therefore resolves the real address
 // with cudaGetSymbolAddress, with that device current, and caches it; make that
-// first call before any stream capture.
+// first call before any stream capture.  The cached address belongs to the
+// device's primary context: a cudaDeviceReset after the first call on a device
+// is not supported (the module may then load at another address).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -109,6 +111,7 @@ bool class_rows(const SlabGrid& g, const double* sigma, double mass_scale, bool 
     std::memset(m, 0, sizeof(double) * (*n_cls) * no);
     static const int en[6][4] = {{0, 1, 5, 7}, {0, 1, 3, 7}, {0, 2, 3, 7}, {0, 2, 6, 7}, {0, 4, 6, 7}, {0, 4, 5, 7}};
     bool done[kMaxClasses] = {false};
+    double tra[kMaxOffsets], trm[kMaxOffsets];
     // candidate coordinates per axis: both ends and the first two interior
     // positions, which together reach every class (both stagger parities in 2D)
     int cand[3][4], nc[3] = {0, 0, 0};
@@ -120,12 +123,14 @@ bool class_rows(const SlabGrid& g, const double* sigma, double mass_scale, bool 
         for (int cj = 0; cj < nc[1]; ++cj)
             for (int ci = 0; ci < nc[0]; ++ci) {
                     const int i = cand[0][ci], j = cand[1][cj], k = cand[2][ck];
-                    if (done[slab_class(g, i, j, k)]) continue;
-                    done[slab_class(g, i, j, k)] = true;
                     const int cls = slab_class(g, i, j, k);
                     const int node = i + NX * (j + NY * k);
-                    double* ra = a + (size_t)cls * no;
-                    double* rm = m + (size_t)cls * no;
+                    // the row is formed in temporaries; a class met again at another
+                    // candidate node must give the same row (to 1e-12 relative)
+                    double* ra = tra;
+                    double* rm = trm;
+                    std::fill(tra, tra + no, 0.0);
+                    std::fill(trm, trm + no, 0.0);
                     double X[12], Me[16], Ke[16];
                     auto add = [&](const int* v, int nb, int li, const double* sig) {
                         for (int b = 0; b < nb; ++b) {
@@ -180,6 +185,19 @@ bool class_rows(const SlabGrid& g, const double* sigma, double mass_scale, bool 
                                     }
                                 }
                     }
+                    double* ca = a + (size_t)cls * no;
+                    double* cm = m + (size_t)cls * no;
+                    if (!done[cls]) {
+                        std::copy(tra, tra + no, ca);
+                        std::copy(trm, trm + no, cm);
+                        done[cls] = true;
+                        continue;
+                    }
+                    double scale = 0.0;
+                    for (int o = 0; o < no; ++o) scale = std::max({scale, std::fabs(ca[o]), std::fabs(cm[o])});
+                    for (int o = 0; o < no; ++o)
+                        if (std::fabs(tra[o] - ca[o]) > 1e-12 * scale || std::fabs(trm[o] - cm[o]) > 1e-12 * scale)
+                            return false;
                 }
     return true;
 }
@@ -210,6 +228,29 @@ extern "C" int cg_slab_solve_noalloc(const cg_config* cfg, int dim, double h, do
     int no = 0, ncls = 0, offs[27];
     double ta[kMaxClasses * kMaxOffsets], tm[kMaxClasses * kMaxOffsets];
     if (!class_rows(g, sigma, mass_scale, cfg->use_mass_lumping != 0, &no, offs, ta, tm, &ncls)) return CG_ERR_ARG;
+    // drop the offsets whose coefficients vanish in every class (12 of the 27 in 3D,
+    // where the 6-tet cubes leave 15 neighbours), keeping ascending order
+    {
+        int kept = 0;
+        for (int o = 0; o < no; ++o) {
+            bool used = offs[o] == 0;
+            for (int c = 0; c < ncls && !used; ++c)
+                used = ta[(size_t)c * no + o] != 0.0 || tm[(size_t)c * no + o] != 0.0;
+            if (!used) continue;
+            for (int c = 0; c < ncls; ++c) {
+                ta[(size_t)c * no + kept] = ta[(size_t)c * no + o];
+                tm[(size_t)c * no + kept] = tm[(size_t)c * no + o];
+            }
+            offs[kept++] = offs[o];
+        }
+        // re-pack the rows from stride no to stride kept
+        for (int c = 1; c < ncls; ++c)
+            for (int o = 0; o < kept; ++o) {
+                ta[(size_t)c * kept + o] = ta[(size_t)c * no + o];
+                tm[(size_t)c * kept + o] = tm[(size_t)c * no + o];
+            }
+        no = kept;
+    }
     int diag = -1;
     for (int o = 0; o < no; ++o)
         if (offs[o] == 0) diag = o;
@@ -266,9 +307,12 @@ extern "C" int cg_slab_solve_noalloc(const cg_config* cfg, int dim, double h, do
     a.pc = cfg->ksp_preconditioner == CG_PC_JACOBI ? 1 : 0;
     a.diag_slot = diag;
 
-    void (*kernel)(CgArgs) = no == 3 ? cg_fp64_kernel<true, 3>
-                             : no == 9 ? cg_fp64_kernel<true, 9>
-                                       : (no == 27 ? cg_fp64_kernel<true, 0> : cg_fp64_kernel<true, 0>);
+    // the offset count unrolled at compile time where the main path has that instance
+    void (*kernel)(CgArgs) = no == 3    ? cg_fp64_kernel<true, 3>
+                             : no == 7  ? cg_fp64_kernel<true, 7>
+                             : no == 9  ? cg_fp64_kernel<true, 9>
+                             : no == 15 ? cg_fp64_kernel<true, 15>
+                                        : cg_fp64_kernel<true, 0>;
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 512, 0) != cudaSuccess || per_sm < 1) {

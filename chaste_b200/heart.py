@@ -361,6 +361,33 @@ def slab_coordinates(dim, h, width, height=0.0, depth=0.0):
     return np.stack([i.ravel() * h, j.ravel() * h, k.ravel() * h], axis=1)
 
 
+# Transmural cell heterogeneity of the ten Tusscher 2006 model: the scale factors
+# (ScaleFactorGks, ScaleFactorIto, ScaleFactorGkr) of the three layers as Chaste's
+# default parameter file lists them (ChasteParameters.xml:54-92, CellHeterogeneity
+# #1 endo, #2 mid-myocardial, #3 epi), which HeartConfigRelatedCellFactory applies
+# per node (heart/src/problem/cell_factories/HeartConfigRelatedCellFactory.cpp:355-440,
+# layers 0 endo, 1 mid, 2 epi as HeartGeometryInformation::DetermineLayerForEachNode
+# numbers them).
+TRANSMURAL_SCALE_FACTORS = ((0.462, 0.0, 1.0), (1.154, 0.85, 1.0), (1.154, 1.0, 1.0))
+
+
+def transmural_layers(z, depth):
+    """Layer of each node of a slab of the given depth by thirds of z: 0 endo
+    (z < depth/3), 1 mid (z < 2 depth/3), 2 epi."""
+    z = np.asarray(z, dtype=np.float64)
+    third = depth / 3.0
+    return np.where(z < third - 1e-12, 0, np.where(z < 2.0 * third - 1e-12, 1, 2)).astype(np.int32)
+
+
+def transmural_param_table():
+    """Per-layer parameter rows of the TT06 model (cg_set_cells' param_table): the six
+    conductance scales at 1 and ScaleFactorGks, ScaleFactorGkr, ScaleFactorIto of the layer."""
+    rows = []
+    for gks, ito, gkr in TRANSMURAL_SCALE_FACTORS:
+        rows.append([1.0] * 6 + [gks, gkr, ito])
+    return np.asarray(rows)
+
+
 # ---------------------------------------------------------------- problem --
 class MonodomainProblem:
     """MonodomainProblem<DIM> (heart/src/problem/MonodomainProblem.cpp:45-77)."""

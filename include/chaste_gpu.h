@@ -117,6 +117,8 @@ typedef struct {
                                        inner solve runs, keeping this many nodes per thread in registers */
     int cg_blocks;                 /* blocks of the persistent CG kernel (512 threads each; 1024 for a
                                       pipelined solve of a slab that fills every SM with them) */
+    int inner_preconditioner;      /* mixed precision: CG_INNER_PC_* the inner solve uses
+                                      (CG_INNER_PC_JACOBI on CSR meshes); FP64: -1 */
 } cg_stats;
 
 /* Fill cfg with Chaste's defaults (LR91, FE, dt 0.01, Am 1400, Cm 1, Jacobi, atol 2e-4). */
@@ -171,6 +173,13 @@ int cg_get_activation_times(cg_ctx* ctx, double* t /* -1 where not activated */)
 int cg_get_stats(cg_ctx* ctx, cg_stats* stats);
 /* Iteration count of each of the last min(n, steps) solves, oldest first. */
 int cg_get_iteration_history(cg_ctx* ctx, int n, int* iterations);
+
+/* y = B x for the inner preconditioner of a mixed-precision slab solve (the x-line
+ * solve, CG_INNER_PC_LINE), applied on the device in FP32 to a host vector of n
+ * values.  A diagnostic of the mixed solve (B must be symmetric positive definite for
+ * CG); no Chaste counterpart.  CG_ERR_UNSUPPORTED when the context's solve has no
+ * x-line preconditioner (FP64, CSR meshes, CG_INNER_PC_JACOBI). */
+int cg_apply_inner_preconditioner(cg_ctx* ctx, const double* x, double* y);
 
 int cg_num_nodes(cg_ctx* ctx, int* n);
 int cg_num_states(int model, int* n);
@@ -337,10 +346,12 @@ int cg_output_conduction_velocity(cg_ctx* ctx, int origin, const double* distanc
  * reserved on every GPU that loads the library until the process exits and is
  * shared by all calls: calls that overlap on the GPU race, so serialise them.
  * The first call on a device resolves the array's device address and should be
- * made before any stream capture.  stream may be NULL (legacy default stream);
- * the call returns after the solve has completed on it.  cfg supplies
- * pde_time_step, Am, Cm, the KSP tolerance/preconditioner, max_iterations and
- * mass lumping; FP64 only. */
+ * made before any stream capture; a cudaDeviceReset after that first call is not
+ * supported.  sigma is a HOST array of dim conductivities (mS/cm); d_z and d_x
+ * are device pointers on the current device.  stream may be NULL (legacy default
+ * stream) and otherwise must be a stream of the current device; the call returns
+ * after the solve has completed on it.  cfg supplies pde_time_step, Am, Cm, the
+ * KSP tolerance/preconditioner, max_iterations and mass lumping; FP64 only. */
 int cg_slab_solve_noalloc(const cg_config* cfg, int dim, double h, double width, double height,
                           double depth, const double* sigma, const double* d_z, double* d_x,
                           void* stream, int* iterations);

@@ -1,7 +1,7 @@
 """Extract Chaste's own golden vectors for the monodomain path into chaste_kats.json.
 
-Run in a container where the reference tree is mounted (default
-/root/reference); the GPU tests and the benchmark only read the JSON.
+Run where the Chaste source tree is present, passing its root as the first
+argument or in $CHASTE_SOURCE_DIR; the GPU tests and the benchmark only read the JSON.
 Sources:
   heart/test/data/ionicmodels/Lr91DelayedStimValidData.dat   (TestIonicModels.hpp:406-467)
   heart/test/data/ionicmodels/Lr91RegularStimValidData.dat   (TestIonicModels.hpp:469-500)
@@ -18,7 +18,9 @@ import json
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CHASTE_SOURCE_DIR")
+if not REF:
+    sys.exit("usage: make_golden.py <chaste source root>  (or set CHASTE_SOURCE_DIR)")
 
 
 def read_dat(rel):

@@ -6,10 +6,11 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-CELLML = "/root/reference/heart/src/odes/cellml"
+# the Chaste source tree, when present: $CHASTE_SOURCE_DIR (the CellML files are not vendored)
+CELLML = os.path.join(os.environ.get("CHASTE_SOURCE_DIR", ""), "heart", "src", "odes", "cellml")
 
 
-@pytest.mark.skipif(not os.path.isdir(CELLML), reason="CellML sources not mounted")
+@pytest.mark.skipif(not os.path.isdir(CELLML), reason="CHASTE_SOURCE_DIR not set or without the CellML sources")
 def test_generated_headers_are_current(tmp_path):
     from chaste_b200.codegen import emit
 

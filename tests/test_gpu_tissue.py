@@ -83,23 +83,32 @@ def test_tt06_3d_rush_larsen_parity(N, oracle):
     assert np.abs(its_g - its_o).max() <= 1
 
 
-@pytest.mark.parametrize("variant", ["slab", "csr", "slab_two_nodes_per_thread", "slab_jacobi_inner"])
+@pytest.mark.parametrize("variant", ["slab", "csr", "slab_two_nodes_per_thread", "slab_four_nodes_per_thread",
+                                     "slab_jacobi_inner"])
 def test_mixed_precision_against_fp64(N, variant):
     """Mixed mode (FP32 states, FP32 inner CG, FP64 refinement) within 0.5 mV of FP64 and activation within 1 ms.
 
     slab: the pipelined inner solve with one node per thread; csr: the assembled
     operator (two-reduction inner PCG); slab_two_nodes_per_thread: a slab of
     159,681 nodes, more than the co-resident grid has threads, so each thread
-    keeps two nodes' inner vectors in registers."""
+    keeps two nodes' inner vectors in registers; slab_four_nodes_per_thread: a slab
+    of 473,556 nodes, the largest register-resident case (4 per thread on 148 SMs)."""
     case = dict(TC.TT06_3D)
+    pipe = {"slab": 1, "slab_jacobi_inner": 1, "slab_two_nodes_per_thread": 2, "slab_four_nodes_per_thread": 4}
     if variant == "csr":
         case["use_csr"] = True
     elif variant == "slab_two_nodes_per_thread":
         case.update(size=(1.0, 0.5, 0.3), box_hi=(0.1, 0.1, 0.1))
+    elif variant == "slab_four_nodes_per_thread":
+        case.update(size=(2.0, 0.75, 0.3), box_hi=(0.1, 0.1, 0.1))
     elif variant == "slab_jacobi_inner":
         case["inner_pc"] = 1
     a, _ = TC.make_gpu(N, precision=0, **case)
     b, _ = TC.make_gpu(N, precision=1, **case)
+    st = b.stats()
+    assert st.pipelined_nodes_per_thread == pipe.get(variant, 0)
+    assert st.inner_preconditioner == (N.INNER_PC_LINE if variant in pipe and variant != "slab_jacobi_inner"
+                                       else N.INNER_PC_JACOBI)
     worst = 0.0
     for _ in range(20):
         a.step(10)
@@ -128,6 +137,30 @@ def test_line_preconditioned_inner_solve_takes_fewer_iterations(N):
     assert il <= 0.75 * ij, (il, ij)
     assert np.abs(line.voltage() - ref.voltage()).max() <= 0.5
     assert np.abs(line.voltage() - jac.voltage()).max() <= 0.5
+
+
+def test_inner_preconditioner_is_symmetric_and_inverts_the_x_lines(N, oracle):
+    """The mixed solve's x-line inner preconditioner B, applied on the device: <Bx, y> =
+    <x, By> to FP32 rounding, x^T B x > 0, and T B x = x with T the tridiagonal x-part
+    of the assembled A restricted to the 32-node segments B works on."""
+    case = dict(TC.TT06_3D, size=(0.4, 0.1, 0.05))
+    t, _ = TC.make_gpu(N, precision=1, **case)
+    o, _ = TC.make_oracle(oracle, **case)
+    n = t.n
+    rng = np.random.default_rng(3)
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    bx, by = t.apply_inner_preconditioner(x), t.apply_inner_preconditioner(y)
+    assert abs(bx @ y - x @ by) <= 1e-5 * float(np.abs(bx) @ np.abs(y))
+    assert x @ bx > 0 and y @ by > 0
+    rp, cols, vals = o.matrix(0)
+    tbx = np.zeros(n)
+    for i in range(n):
+        for k in range(rp[i], rp[i + 1]):
+            j = cols[k]
+            same_segment = j // 32 == i // 32
+            if j == i or (abs(j - i) == 1 and same_segment):
+                tbx[i] += vals[k] * bx[j]
+    assert np.max(np.abs(tbx - x)) <= 1e-4 * np.max(np.abs(x))
 
 
 @pytest.mark.parametrize("case_name", ["LR91_2D", "TT06_3D"])

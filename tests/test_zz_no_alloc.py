@@ -52,6 +52,7 @@ def _one_solve_from_tissue(N, case, warm_steps):
     cfg.pde_time_step = dt
     cfg.use_absolute_tolerance, cfg.ksp_tolerance = 0, case.get("rel_tol", 1e-8)
     cfg.ksp_preconditioner = N.PC_JACOBI
+    cfg.use_mass_lumping = 1 if case.get("lump") else 0
     sig = np.ascontiguousarray(np.asarray(case["sigma"], dtype=np.float64)[: case["dim"]])
     its = C.c_int(-1)
     rc = N.lib().cg_slab_solve_noalloc(C.byref(cfg), case["dim"], case["h"], *case["size"], N.dptr(sig),
@@ -70,6 +71,21 @@ def test_noalloc_solve_matches_tissue_solve_twice(N):
     err2, its2, ref2 = _one_solve_from_tissue(N, dict(TC.TT06_3D), warm_steps=12)
     assert err2 <= TOL, err2
     assert abs(its2 - ref2) <= 1
+
+
+@pytest.mark.parametrize("name", ["cable_1d", "sheet_2d_lumped_mass", "slab_3d_at_the_limit"])
+def test_noalloc_solve_other_shapes(N, name):
+    """A 1D cable (3 offsets), a lumped-mass sheet, and a 3D slab of exactly the
+    32,768-node limit (64 blocks of the persistent kernel, 15 offsets)."""
+    if name == "cable_1d":
+        case = dict(TC.LR91_2D, dim=1, size=(1.0, 0.0, 0.0), box_hi=(0.0199,))
+    elif name == "sheet_2d_lumped_mass":
+        case = dict(TC.LR91_2D, lump=True)
+    else:
+        case = dict(TC.TT06_3D, size=(0.31, 0.31, 0.31), box_hi=(0.05, 0.05, 0.05))
+    err, its, ref = _one_solve_from_tissue(N, case, warm_steps=6)
+    assert err <= TOL, err
+    assert abs(its - ref) <= 1
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(N):

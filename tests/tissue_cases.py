@@ -17,7 +17,7 @@ def slab_stim_ids(xyz, box_hi):
 
 def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
              abs_tol=None, rel_tol=1e-8, precision=0, use_csr=False, param_set=None, param_table=None,
-             init_states=None, max_iterations=10000, solver=0, svi=0, inner_pc=0):
+             init_states=None, max_iterations=10000, solver=0, svi=0, inner_pc=0, lump=False):
     """A GPU tissue on a regular slab (stencil operator, or CSR through cg_set_mesh when use_csr)."""
     from oracle import pyoracle as O  # mesh generator only: the same node/element order as the library
 
@@ -35,6 +35,7 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
     cfg.solver = solver
     cfg.use_state_variable_interpolation = svi
     cfg.mixed_inner_preconditioner = inner_pc
+    cfg.use_mass_lumping = 1 if lump else 0
     t = N.Tissue(cfg)
     xyz, conn, _ = O.slab_mesh(dim, h, *size)
     if use_csr:
@@ -84,3 +85,19 @@ def niederer_activation(t, n, printing_steps=10, n_prints=400, printing_dt=0.1):
         act[new] = (k - v[new] / (v[new] - last[new])) * printing_dt
         last = np.where(v <= 0, v, last)
     return act
+
+
+# The benchmark configurations at full size (2 and 5)
+C1_SHEET_2D = dict(model=LR91, method=FE, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, size=(1.0, 1.0, 0.0),
+                   sigma=(1.75, 1.75, 1.75), stim=(-5e5, 0.5, 0.0), box_hi=(0.0199, 1e9))
+C2_SLAB_3D = dict(model=TT06, method=RL, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01, size=(2.0, 0.7, 0.3),
+                  sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0), box_hi=(0.1, 0.1, 0.1))
+C5_SLAB_3D = dict(C2_SLAB_3D, h=0.0125, size=(2.0, 2.0, 1.0))
+
+
+def transmural(case):
+    """The case with TT06 endo / mid / epi layers by thirds of z (param_set, param_table)."""
+    from chaste_b200.heart import slab_coordinates, transmural_layers, transmural_param_table
+
+    xyz = slab_coordinates(case["dim"], case["h"], *case["size"])
+    return dict(case, param_set=transmural_layers(xyz[:, 2], case["size"][2]), param_table=transmural_param_table())
