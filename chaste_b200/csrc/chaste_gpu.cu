@@ -14,6 +14,7 @@
 #include "../../include/chaste_gpu.h"
 #include "host/assemble.h"
 #include "kernels/cg.cuh"
+#include "kernels/cg_ilu.cuh"
 #include "kernels/cg_mixed.cuh"
 #include "kernels/ode.cuh"
 #include "kernels/svi.cuh"
@@ -24,6 +25,9 @@ using namespace chb;
 namespace {
 
 constexpr int kRing = 4096;   // iteration-count history per context
+// bjacobi solves of meshes up to this size run as one block (block barriers between
+// the levels of the triangular solves); larger ones on the co-resident grid
+constexpr int kIluOneBlockNodes = 65536;
 
 struct DeviceBuffers {
     std::vector<void*> owned;
@@ -110,6 +114,9 @@ struct cg_ctx {
     int xm_slot = -1, xp_slot = -1;   // stencil slots of offsets -1 and +1
     bool line_pc = false;             // the mixed slab solve uses the x-line inner preconditioner
     float2* d_line_ad = nullptr;      // its factors (a_i, 1/d_i) per node
+    // bjacobi (ILU(0) of the whole matrix): factors, level schedules, b and B b
+    bool ilu = false;
+    IluArgs ilu_args{};
     // stats
     long long steps = 0;
     long long total_iters = 0;
@@ -272,8 +279,11 @@ int cg_create(const cg_config* cfg, cg_ctx** out) {
     if (!(cfg->ode_time_step > 0) || !(cfg->pde_time_step > 0)) return CG_ERR_ARG;
     if (!(cfg->surface_area_to_volume_ratio > 0) || !(cfg->capacitance > 0)) return CG_ERR_ARG;
     if (!(cfg->ksp_tolerance > 0)) return CG_ERR_ARG;
-    if (cfg->ksp_preconditioner == CG_PC_BJACOBI) return CG_ERR_UNSUPPORTED;
-    if (cfg->ksp_preconditioner != CG_PC_NONE && cfg->ksp_preconditioner != CG_PC_JACOBI) return CG_ERR_ARG;
+    if (cfg->ksp_preconditioner != CG_PC_NONE && cfg->ksp_preconditioner != CG_PC_JACOBI &&
+        cfg->ksp_preconditioner != CG_PC_BJACOBI)
+        return CG_ERR_ARG;
+    // bjacobi runs in the FP64 solve only (the mixed solve's outer test is Jacobi-preconditioned)
+    if (cfg->ksp_preconditioner == CG_PC_BJACOBI && cfg->precision != CG_PRECISION_FP64) return CG_ERR_UNSUPPORTED;
     if (cfg->precision != CG_PRECISION_FP64 && cfg->precision != CG_PRECISION_MIXED) return CG_ERR_ARG;
     if (cfg->solver != CG_SOLVER_MONODOMAIN && cfg->solver != CG_SOLVER_OPERATOR_SPLITTING) return CG_ERR_ARG;
     if (cfg->use_state_variable_interpolation != 0 && cfg->use_state_variable_interpolation != 1) return CG_ERR_ARG;
@@ -512,6 +522,16 @@ int alloc_vectors(cg_ctx* c) {
     }
     // the HBM-resident mixed solve takes the x-line preconditioner whenever it is asked for
     if (c->pipe_nodes == 0) c->line_pc = want_line;
+    if (c->ilu) {
+        // one block while the level sweeps are short (block barriers between levels),
+        // else the co-resident grid with grid barriers
+        int per_sm_ilu = 0;
+        CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ilu, cg_ilu_kernel, 1024, 0));
+        if (per_sm_ilu < 1) return CG_ERR_UNSUPPORTED;
+        const long long want_ilu = (long long)n <= kIluOneBlockNodes ? 1 : ((long long)n + 1023) / 1024;
+        c->cg_blocks = (int)std::max(1LL, std::min({want_ilu, (long long)per_sm_ilu * sms, (long long)kMaxGridBlocks}));
+        c->cg_threads = 1024;
+    }
     CG_TRY(dalloc(c, &c->d_partials,
                   (size_t)2 * std::max(blocks_512, c->cg_blocks) * kPartialStride * sizeof(double)));
     c->ode_blocks = (int)std::max(1LL, std::min(((long long)n + 255) / 256, (long long)sms * 16));
@@ -541,6 +561,88 @@ int build_line_factors(cg_ctx* c, const std::vector<uint8_t>& cls) {
     CG_TRY(dalloc(c, &c->d_line_ad, ad.size() * sizeof(float2)));
     CG_CUDA(cudaMemcpyAsync(c->d_line_ad, ad.data(), ad.size() * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
     CG_CUDA(cudaStreamSynchronize(c->stream));
+    return CG_OK;
+}
+
+// ILU(0) of A in natural order with no pivoting, on A's own pattern -- PETSc's
+// bjacobi on one process factors the single diagonal block, the whole matrix,
+// with ILU(0) -- and the level schedules of its two triangular solves (a row's
+// level is one more than the highest level among the rows it reads).
+int setup_ilu(cg_ctx* c) {
+    const HostCsr& A = c->csr;
+    const int n = A.n;
+    std::vector<double> lu(A.a);
+    std::vector<int> diag(n);
+    for (int i = 0; i < n; ++i) {
+        diag[i] = A.find(i, i);
+        if (diag[i] < 0) return CG_ERR_ARG;
+    }
+    for (int i = 1; i < n; ++i) {
+        const int end = A.rowptr[i + 1];
+        for (int kk = A.rowptr[i]; kk < end && A.cols[kk] < i; ++kk) {
+            const int k = A.cols[kk];
+            lu[kk] /= lu[diag[k]];
+            const double lik = lu[kk];
+            // row i -= lik * (row k right of its diagonal), on row i's pattern only
+            int jj = kk + 1;
+            for (int kj = diag[k] + 1; kj < A.rowptr[k + 1]; ++kj) {
+                const int j = A.cols[kj];
+                while (jj < end && A.cols[jj] < j) ++jj;
+                if (jj < end && A.cols[jj] == j) lu[jj] -= lik * lu[kj];
+            }
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (!(lu[diag[i]] != 0.0) || !std::isfinite(lu[diag[i]])) return CG_ERR_ARG;
+    auto schedule = [&](bool forward, std::vector<int>& rows, std::vector<int>& ptr) {
+        std::vector<int> level(n, 0);
+        int top = 0;
+        for (int s = 0; s < n; ++s) {
+            const int i = forward ? s : n - 1 - s;
+            int l = 0;
+            const int b = forward ? A.rowptr[i] : diag[i] + 1;
+            const int e = forward ? diag[i] : A.rowptr[i + 1];
+            for (int k = b; k < e; ++k) l = std::max(l, level[A.cols[k]] + 1);
+            level[i] = l;
+            top = std::max(top, l);
+        }
+        ptr.assign(top + 2, 0);
+        for (int i = 0; i < n; ++i) ptr[level[i] + 1]++;
+        for (int l = 0; l <= top; ++l) ptr[l + 1] += ptr[l];
+        rows.assign(n, 0);
+        std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+        for (int i = 0; i < n; ++i) rows[fill[level[i]]++] = i;   // ascending rows within a level
+        return top + 1;
+    };
+    std::vector<int> frows, fptr, brows, bptr;
+    const int fl = schedule(true, frows, fptr), bl = schedule(false, brows, bptr);
+    cudaStream_t s = c->stream;
+    double* d_lu = nullptr;
+    int *d_diag = nullptr, *d_fr = nullptr, *d_fp = nullptr, *d_br = nullptr, *d_bp = nullptr;
+    CG_TRY(dalloc(c, &d_lu, lu.size() * sizeof(double)));
+    CG_TRY(dalloc(c, &d_diag, n * sizeof(int)));
+    CG_TRY(dalloc(c, &d_fr, n * sizeof(int)));
+    CG_TRY(dalloc(c, &d_fp, fptr.size() * sizeof(int)));
+    CG_TRY(dalloc(c, &d_br, n * sizeof(int)));
+    CG_TRY(dalloc(c, &d_bp, bptr.size() * sizeof(int)));
+    CG_TRY(dalloc(c, &c->ilu_args.bvec, n * sizeof(double)));
+    CG_TRY(dalloc(c, &c->ilu_args.wvec, n * sizeof(double)));
+    CG_CUDA(cudaMemcpyAsync(d_lu, lu.data(), lu.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(d_diag, diag.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(d_fr, frows.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(d_fp, fptr.data(), fptr.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(d_br, brows.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaMemcpyAsync(d_bp, bptr.data(), bptr.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    CG_CUDA(cudaStreamSynchronize(s));
+    c->ilu_args.lu = d_lu;
+    c->ilu_args.diag = d_diag;
+    c->ilu_args.f_rows = d_fr;
+    c->ilu_args.f_ptr = d_fp;
+    c->ilu_args.f_levels = fl;
+    c->ilu_args.b_rows = d_br;
+    c->ilu_args.b_ptr = d_bp;
+    c->ilu_args.b_levels = bl;
+    c->ilu = true;
     return CG_OK;
 }
 
@@ -605,6 +707,7 @@ int upload_operator(cg_ctx* c) {
         CG_CUDA(cudaMemcpyAsync(c->d_aval, m.a.data(), nnz * sizeof(double), cudaMemcpyHostToDevice, s));
         CG_CUDA(cudaMemcpyAsync(c->d_mval, m.m.data(), nnz * sizeof(double), cudaMemcpyHostToDevice, s));
         CG_CUDA(cudaMemcpyAsync(c->d_dinv, dinv.data(), m.n * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (c->cfg.ksp_preconditioner == CG_PC_BJACOBI) CG_TRY(setup_ilu(c));
         std::vector<float> a32, d32;
         if (c->mixed()) {
             a32.assign(m.a.begin(), m.a.end());
@@ -713,7 +816,8 @@ int cg_set_slab_mesh(cg_ctx* c, int dim, double h, double width, double height, 
     if (!assemble(dim, c->n, xyz.data(), n_elems, conn.data(), sig.data(), mass_scale,
                   c->cfg.use_mass_lumping != 0, c->csr))
         return CG_ERR_ARG;
-    c->slab = build_slab_stencil(g, c->csr, c->stencil);
+    // the ILU(0) factors are per row, so bjacobi keeps the assembled CSR
+    c->slab = c->cfg.ksp_preconditioner != CG_PC_BJACOBI && build_slab_stencil(g, c->csr, c->stencil);
     if (c->slab) {
         HostCsr empty;
         std::swap(c->csr, empty);
@@ -913,6 +1017,18 @@ CgArgs make_cg_args(cg_ctx* c) {
 
 cudaError_t launch_cg(cg_ctx* c) {
     CgArgs a = make_cg_args(c);
+    if (c->ilu) {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(c->cg_blocks);
+        lc.blockDim = dim3(c->cg_threads);
+        lc.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        return cudaLaunchKernelEx(&lc, cg_ilu_kernel, a, c->ilu_args);
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->cg_blocks);
     cfg.blockDim = dim3(c->cg_threads);

@@ -55,7 +55,7 @@ class HeartConfig:
         self.sigma = (1.75, 1.75, 1.75)
         self.use_abs_tol = True
         self.tol = 2e-4
-        self.ksp_pc = "jacobi"
+        self.ksp_pc = "bjacobi"       # HeartConfigDefaults.hpp:83
         self.mass_lumping = False
         self.space_dimension = 3
         self.slab = None          # (width, height, depth, h)
@@ -128,8 +128,8 @@ class HeartConfig:
             raise ValueError("the GPU tissue solves with CG (the monodomain matrix is SPD)")
 
     def SetKSPPreconditioner(self, name):
-        if name not in ("jacobi", "none"):
-            raise ValueError(f"unsupported preconditioner {name!r} (jacobi or none)")
+        if name not in ("bjacobi", "jacobi", "none"):
+            raise ValueError(f"unsupported preconditioner {name!r} (bjacobi, jacobi or none)")
         self.ksp_pc = name
 
     def SetUseMassLumping(self, flag=True):
@@ -189,7 +189,9 @@ class HeartConfig:
     def SetSpaceDimension(self, d):
         self.space_dimension = d
 
-    # extension of this library: FP32 states + FP32 inner CG with FP64 refinement
+    # extension of this library: FP32 states + FP32 inner CG with FP64 refinement.  The
+    # mixed solve's FP64 residual test is Jacobi-preconditioned: a bjacobi request is
+    # served by Jacobi in that mode (the converged solution meets the same tolerance).
     def SetPrecision(self, name):
         if name not in ("fp64", "mixed"):
             raise ValueError(name)
@@ -421,7 +423,10 @@ class MonodomainProblem:
         cfg.capacitance = hc.cm
         cfg.use_absolute_tolerance = 1 if hc.use_abs_tol else 0
         cfg.ksp_tolerance = hc.tol
-        cfg.ksp_preconditioner = {"jacobi": N.PC_JACOBI, "none": N.PC_NONE}[hc.ksp_pc]
+        pc = hc.ksp_pc
+        if pc == "bjacobi" and hc.precision == "mixed":
+            pc = "jacobi"
+        cfg.ksp_preconditioner = {"bjacobi": N.PC_BJACOBI, "jacobi": N.PC_JACOBI, "none": N.PC_NONE}[pc]
         cfg.use_mass_lumping = 1 if hc.mass_lumping else 0
         cfg.precision = N.PRECISION_MIXED if hc.precision == "mixed" else N.PRECISION_FP64
         cfg.activation_threshold = hc.activation_threshold

@@ -74,7 +74,8 @@ typedef struct {
     double pde_time_step;      /* ms */
     double surface_area_to_volume_ratio;  /* Am, 1/cm (default 1400) */
     double capacitance;        /* Cm, uF/cm^2 (default 1) */
-    int ksp_preconditioner;    /* CG_PC_*; bjacobi is rejected (CG_ERR_UNSUPPORTED) */
+    int ksp_preconditioner;    /* CG_PC_*; bjacobi (PETSc's on one process: ILU(0) of the whole
+                                  matrix) in FP64 only, CG_ERR_UNSUPPORTED with mixed precision */
     int use_absolute_tolerance;/* 1: KSPSetTolerances(DBL_EPSILON, tol); 0: (tol, default) */
     double ksp_tolerance;
     int use_mass_lumping;

@@ -48,6 +48,7 @@ def test_invalid_configs_are_rejected_before_touching_a_device(native):
     assert e.value.status == 1
     c = native.default_config()
     c.ksp_preconditioner = native.PC_BJACOBI
+    c.precision = native.PRECISION_MIXED   # bjacobi is an FP64 preconditioner here
     with pytest.raises(native.ChasteGpuError) as e:
         native.Tissue(c)
     assert e.value.status == 10

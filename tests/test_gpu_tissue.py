@@ -22,15 +22,18 @@ def _cmp(v_gpu, v_orc):
     return np.max(np.abs(v_gpu - v_orc) / np.maximum(np.abs(v_orc), 1.0))
 
 
-@pytest.mark.parametrize("use_csr", [False, True], ids=["slab_stencil", "csr"])
-def test_chaste_tissue_kats_on_gpu(N, oracle, kats, use_csr):
-    """TestMonodomainProblem.hpp KATs through the GPU path (Jacobi PC), and per-node parity with the oracle."""
+@pytest.mark.parametrize("use_csr,pc", [(False, 1), (True, 1), (False, 2)], ids=["slab_stencil", "csr",
+                                                                                  "bjacobi_ilu0"])
+def test_chaste_tissue_kats_on_gpu(N, oracle, kats, use_csr, pc):
+    """TestMonodomainProblem.hpp KATs through the GPU path (Jacobi on the stencil and CSR
+    operators; bjacobi, Chaste's default, as ILU(0) of the whole matrix), and per-node
+    parity with the oracle, CG iteration counts within one."""
     for case in kats["tissue"]:
         d = case["dim"]
         kw = dict(model=TC.LR91, method=TC.FE, dt_ode=0.01, dt_pde=0.01, dim=d, h=case["h"],
                   size=tuple(case["size"][:3]), sigma=(case["sigma"],) * 3,
                   stim=(case["stim"], case["stim_duration"], 0.0), box_hi=(1e-5,) + (1e9,) * 2,
-                  am=case["am"], cm=case["cm"])
+                  am=case["am"], cm=case["cm"], pc=pc)
         if "abs_tol" in case:
             kw["abs_tol"] = case["abs_tol"]
         else:
@@ -45,7 +48,7 @@ def test_chaste_tissue_kats_on_gpu(N, oracle, kats, use_csr):
         assert _cmp(v, o.voltage()) <= FP64_RTOL, case["name"]
         its_g = g.iteration_history(nsteps)
         assert np.abs(its_g - its_o).max() <= 1, case["name"]
-        assert g.stats().operator_kind == (0 if use_csr else 1)
+        assert g.stats().operator_kind == (0 if use_csr or pc == 2 else 1)
 
 
 def _parity_run(N, oracle, case, t_end, every, precision=0):
@@ -74,6 +77,20 @@ def test_lr91_2d_forward_euler_parity(N, oracle):
     ig, _ = g.caches()
     io, _ = o.caches()
     assert np.max(np.abs(ig - io)) <= 1e-6 * max(1.0, np.abs(io).max())
+
+
+@pytest.mark.parametrize("case_name", ["LR91_2D", "TT06_3D"])
+def test_bjacobi_ilu0_parity(N, oracle, case_name):
+    """bjacobi (ILU(0) of the whole matrix, level-scheduled on the device) against the
+    oracle's ILU(0) on the reduced benchmark slabs: Vm every 1 ms within 1e-6, CG
+    iteration counts within one, and fewer iterations than Jacobi."""
+    case = dict(getattr(TC, case_name), pc=2)
+    g, o, worst, vmax, its_g, its_o = _parity_run(N, oracle, case, 5.0, 1.0)
+    assert worst <= FP64_RTOL, worst
+    assert np.abs(its_g - its_o).max() <= 1
+    j, _ = TC.make_gpu(N, **dict(case, pc=1))
+    j.step(len(its_g))
+    assert its_g.sum() < j.iteration_history(len(its_g)).sum()
 
 
 def test_tt06_3d_rush_larsen_parity(N, oracle):

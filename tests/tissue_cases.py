@@ -17,7 +17,7 @@ def slab_stim_ids(xyz, box_hi):
 
 def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
              abs_tol=None, rel_tol=1e-8, precision=0, use_csr=False, param_set=None, param_table=None,
-             init_states=None, max_iterations=10000, solver=0, svi=0, inner_pc=0, lump=False):
+             init_states=None, max_iterations=10000, solver=0, svi=0, inner_pc=0, lump=False, pc=1):
     """A GPU tissue on a regular slab (stencil operator, or CSR through cg_set_mesh when use_csr)."""
     from oracle import pyoracle as O  # mesh generator only: the same node/element order as the library
 
@@ -25,7 +25,7 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
     cfg.model, cfg.ode_method = model, method
     cfg.ode_time_step, cfg.pde_time_step = dt_ode, dt_pde
     cfg.surface_area_to_volume_ratio, cfg.capacitance = am, cm
-    cfg.ksp_preconditioner = N.PC_JACOBI
+    cfg.ksp_preconditioner = pc
     if abs_tol is not None:
         cfg.use_absolute_tolerance, cfg.ksp_tolerance = 1, abs_tol
     else:
@@ -49,10 +49,11 @@ def make_gpu(N, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box
 
 
 def make_oracle(O, *, model, method, dt_ode, dt_pde, dim, h, size, sigma, stim, box_hi, am=1400.0, cm=1.0,
-                abs_tol=None, rel_tol=1e-8, param_set=None, param_table=None, init_states=None, solver=0, svi=0, **_):
+                abs_tol=None, rel_tol=1e-8, param_set=None, param_table=None, init_states=None, solver=0, svi=0,
+                pc=1, **_):
     xyz, conn, _ = O.slab_mesh(dim, h, *size)
     use_abs = abs_tol is not None
-    cfg = O.Config(model, method, dt_ode, dt_pde, am, cm, O.PC_JACOBI, 1 if use_abs else 0,
+    cfg = O.Config(model, method, dt_ode, dt_pde, am, cm, pc, 1 if use_abs else 0,
                    abs_tol if use_abs else rel_tol, 0, 10000, solver, svi)
     sig = np.tile(np.asarray(sigma[:dim], float), (conn.shape[0], 1))
     sid = slab_stim_ids(xyz, box_hi)
