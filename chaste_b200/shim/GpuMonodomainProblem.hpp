@@ -268,8 +268,11 @@ private:
     unsigned mNumStates;
 
 public:
+    // MonodomainTissue derives virtually from AbstractCardiacTissue, so the most
+    // derived class constructs that base itself
     explicit GpuMonodomainTissue(AbstractCardiacCellFactory<DIM>* pCellFactory)
-        : MonodomainTissue<DIM>(pCellFactory),
+        : AbstractCardiacTissue<DIM>(pCellFactory),
+          MonodomainTissue<DIM>(pCellFactory),
           mpCtx(nullptr),
           mNumStates(0u)
     {

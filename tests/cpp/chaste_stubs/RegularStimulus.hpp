@@ -1,0 +1,2 @@
+#pragma once
+#include "chaste_stub_core.hpp"
