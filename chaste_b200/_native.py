@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libchastegpu.so")
 
 CG_OK = 0
+CG_ERR_CG_MAXIT, CG_ERR_CG_DIVERGED, CG_ERR_NAN = 3, 4, 5
 STATUS_NAMES = {
     0: "CG_OK", 1: "CG_ERR_ARG", 2: "CG_ERR_CUDA", 3: "CG_ERR_CG_MAXIT", 4: "CG_ERR_CG_DIVERGED",
     5: "CG_ERR_NAN", 6: "CG_ERR_STATE_RANGE", 7: "CG_ERR_ORDER", 8: "CG_ERR_TIMEOUT",
@@ -131,6 +132,19 @@ SIGNATURES = {
     "cg_output_get_activation": (C.c_int, [_vp, _dp]),
     "cg_output_cell_properties": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _dp, _ip, _dp, _dp, _ip]),
     "cg_output_conduction_velocity": (C.c_int, [_vp, C.c_int, _dp, C.c_double, C.c_int, _dp, _ip]),
+    "cg_part_create": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp,
+                                 C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "cg_part_rows": (C.c_int, [_vp, _ip, _ip, _ip, _ip]),
+    "cg_part_set_cells": (C.c_int, [_vp, _dp, _ip, _dp, C.c_int]),
+    "cg_part_set_stimulus": (C.c_int, [_vp, _ip, C.POINTER(Stimulus), C.c_int]),
+    "cg_part_ode": (C.c_int, [_vp]),
+    "cg_part_halo_pack": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "cg_part_halo_unpack": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "cg_part_cg_phase": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+    "cg_part_finish_step": (C.c_int, [_vp]),
+    "cg_part_get_voltage": (C.c_int, [_vp, _dp]),
+    "cg_part_config": (C.c_int, [_vp, C.POINTER(Config)]),
+    "cg_part_destroy": (C.c_int, [_vp]),
     "cg_slab_solve_noalloc": (C.c_int, [C.POINTER(Config), C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, _dp, _vp, _vp, _vp, _ip]),
 }

@@ -12,9 +12,9 @@ LIB_DIR = os.path.join(HERE, "lib")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 
-SOURCES = ["chaste_gpu.cu", "noalloc.cu", "batch.cu", "cable.cu", "selftest.cu", "host/assemble.cpp"]
+SOURCES = ["chaste_gpu.cu", "partition.cu", "noalloc.cu", "batch.cu", "cable.cu", "selftest.cu", "host/assemble.cpp"]
 DEPS = SOURCES + [
-    "kernels/common.cuh", "kernels/ops.cuh", "kernels/cg.cuh", "kernels/cg_mixed.cuh",
+    "kernels/common.cuh", "kernels/ops.cuh", "kernels/cg.cuh", "kernels/cg_mixed.cuh", "kernels/cg_ilu.cuh",
     "kernels/ode.cuh", "kernels/batch.cuh", "kernels/cable.cuh", "kernels/svi.cuh", "kernels/output.cuh",
     "models/cellmodel_common.h", "models/lr91.h", "models/tt06.h",
     "host/assemble.h", "../../include/chaste_gpu.h",
@@ -36,11 +36,28 @@ def _stale(target, deps):
 
 
 def build_native(force=False, verbose=False):
-    """Compile libchastegpu.so for sm_100a when it is missing or older than its sources."""
+    """Compile libchastegpu.so for sm_100a when it is missing or older than its sources.
+    The translation units compile in parallel (one nvcc each), then link."""
+    import concurrent.futures
+
     os.makedirs(LIB_DIR, exist_ok=True)
     out = os.path.join(LIB_DIR, "libchastegpu.so")
     if force or _stale(out, DEPS):
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-o", out] + [os.path.join(CSRC, s) for s in SOURCES]
+        obj_dir = os.path.join(LIB_DIR, "obj")
+        os.makedirs(obj_dir, exist_ok=True)
+        compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+        def compile_one(src):
+            obj = os.path.join(obj_dir, src.replace("/", "_") + ".o")
+            cmd = [nvcc()] + ARCH + compile_flags + ["-c", "-o", obj, os.path.join(CSRC, src)]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True, cwd=CSRC)
+            return obj
+
+        with concurrent.futures.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+            objs = list(ex.map(compile_one, SOURCES))
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", out] + objs
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True, cwd=CSRC)

@@ -214,7 +214,7 @@ __device__ void cg_ilu_kernel_body(const CgArgs& a, const IluArgs& f, unsigned& 
     cg_finish(a, step, it, kStatusCgMaxIt);
 }
 
-__global__ void __launch_bounds__(1024, 1) cg_ilu_kernel(CgArgs a, IluArgs f) {
+static __global__ void __launch_bounds__(1024, 1) cg_ilu_kernel(CgArgs a, IluArgs f) {
     unsigned round = 0;
     cg_ilu_kernel_body(a, f, round);
     grid_exit(a.gs);

@@ -126,7 +126,7 @@ __device__ __forceinline__ float2 line_factors(const CgArgs& a, bool on, int i) 
 
 // y = B x with the x-line inner preconditioner alone (cg_apply_inner_preconditioner):
 // the same segments and factors the mixed solves use.
-__global__ void line_pc_apply_kernel(int n, const float2* __restrict__ ad, const float* __restrict__ x,
+static __global__ void line_pc_apply_kernel(int n, const float2* __restrict__ ad, const float* __restrict__ x,
                                      float* __restrict__ y) {
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;

@@ -38,7 +38,7 @@ struct OdeArgs {
 
 // First step with V above the threshold (ActivationOutputModifier::ProcessSolutionAtTimeStep,
 // heart/src/problem/ActivationOutputModifier.cpp:91-101), checked once per PDE step.
-__global__ void activation_kernel(int n, const double* __restrict__ V, double* __restrict__ act,
+static __global__ void activation_kernel(int n, const double* __restrict__ V, double* __restrict__ act,
                                   double threshold, double t) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         if (V[i] > threshold && act[i] < 0.0) act[i] = t;

@@ -331,6 +331,50 @@ int cg_output_cell_properties(cg_ctx* ctx, double percentage, double threshold, 
 int cg_output_conduction_velocity(cg_ctx* ctx, int origin, const double* distances, double threshold, int max_aps,
                                   double* cv, int* n_cv);
 
+/* ------------------------------------------------------ multi-GPU slabs --
+ * One rank's share of a slab tissue, one process per GPU.  Rows are owned in the
+ * contiguous ranges PETSc's PETSC_DECIDE split gives Chaste's
+ * DistributedVectorFactory (global/src/parallel/DistributedVectorFactory.cpp:44-64):
+ * rank r of W owns n/W rows, one more when r < n % W.  With the slab numbering
+ * ((k*NY + j)*NX + i) a range is a block of z-planes, and the stencil reaches
+ * `halo` = NX*NY + NX + 1 rows on each side.  The ODE step is local
+ * (AbstractCardiacTissue::SolveCellSystems over the rank's cells); the diffusion
+ * solve is PETSc's CG with Jacobi (KSPSolve_CG, linalg/src/LinearSystem.cpp:1099)
+ * split at its two inner-product reductions into phases that the caller
+ * sequences, all-reducing each phase's four partial sums across the ranks and
+ * exchanging halos before each operator application (chaste_b200/partition.py
+ * does both with torch.distributed):
+ *   phase 0: b = M z, r = b - A x, z' = B r; sums sum|b|, |B b|^2, |z'|^2, (r, z')
+ *            (needs the V and z halos)
+ *   phase 1: zero guess for a tiny right-hand side (LinearSystem.cpp:984-994):
+ *            x = 0, r = b, z' = B b; sums |z'|^2, (b, z')
+ *   phase 2: q = A z' + s0 q, p = z' + s0 p (s1 != 0: first iteration, no old p);
+ *            sum (p, q) (needs the z' halo)
+ *   phase 3: x += s0 p, r -= s0 q, z' = B r; sums |z'|^2, (z', r)
+ * cg_part_halo_pack copies the `halo` rows next to the lower and upper neighbour
+ * of vector `which` (0 V, 1 z, 2 z') into lo_out / hi_out; _unpack writes the
+ * neighbours' rows into the halos; buffers may be host or device memory.  Global
+ * arrays (init_states n x S, param_set, stim_id) are indexed by global row; the
+ * rank keeps its own rows.  FP64, Jacobi or no preconditioner, the default solver;
+ * a rank of a multi-rank run must own at least `halo` rows.  No counterpart in
+ * the reference beyond the distributed PETSc objects it stands in for. */
+typedef struct cg_part cg_part;
+int cg_part_create(const cg_config* cfg, int dim, double h, double width, double height, double depth,
+                   const double* sigma, int rank, int world, cg_part** out);
+int cg_part_rows(const cg_part* part, int* lo, int* hi, int* halo, int* n_global);
+int cg_part_set_cells(cg_part* part, const double* init_states, const int* param_set, const double* param_table,
+                      int n_param_sets);
+int cg_part_set_stimulus(cg_part* part, const int* stim_id, const cg_stimulus* stims, int n_stims);
+int cg_part_ode(cg_part* part);
+int cg_part_halo_pack(cg_part* part, int which, void* lo_out, void* hi_out);
+int cg_part_halo_unpack(cg_part* part, int which, const void* lo_in, const void* hi_in);
+int cg_part_cg_phase(cg_part* part, int phase, const double* scalars /* 2 */, double* sums /* 4 */);
+/* ends the PDE step (the ODE step of the next call is at the next time) */
+int cg_part_finish_step(cg_part* part);
+int cg_part_get_voltage(cg_part* part, double* v /* the rank's rows */);
+int cg_part_config(const cg_part* part, cg_config* cfg);
+int cg_part_destroy(cg_part* part);
+
 /* Allocation-free diffusion solve of one PDE step on a regular slab.
  *
  * No counterpart in the reference: Chaste always owns its PETSc vectors.  This
