@@ -479,12 +479,26 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--t-start-ms", type=float, default=10.0,
                     help="simulated time reached, untimed, before the warm-up and timed steps")
-    ap.add_argument("--profile", choices=["fp64", "mixed"],
+    ap.add_argument("--profile", choices=["fp64", "mixed", "population"],
                     help="only build the workload's tissue in this precision, advance it to --t-start-ms and "
                          "take --steps steps with an L2 flush before each (the program the ncu captures in "
                          "profiles/ run)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.profile == "population":
+        # the C3 population's launch shapes for --steps steps each (cg_batch_autotune), the
+        # program the batch-kernel ncu capture runs
+        from chaste_b200 import _native as N
+        from chaste_b200.build import build_native
+
+        build_native()
+        rng = np.random.default_rng(20261203)
+        params = np.ones((8192, 9))
+        params[:, :6] = np.exp(rng.normal(0.0, 0.2, size=(8192, 6)))
+        b = N.CellBatch(N.MODEL_TT06, rng.integers(1, 21, size=8192).astype(np.int32), params)
+        tpb = b.autotune(steps=args.steps)
+        print(json.dumps({"profile": "population", "threads_per_block": tpb, "shape": b.launch_shape()}), flush=True)
+        return
     if args.profile:
         import torch
 

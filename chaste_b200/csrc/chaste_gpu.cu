@@ -114,6 +114,9 @@ struct cg_ctx {
     int xm_slot = -1, xp_slot = -1;   // stencil slots of offsets -1 and +1
     bool line_pc = false;             // the mixed slab solve uses the x-line inner preconditioner
     float2* d_line_ad = nullptr;      // its factors (a_i, 1/d_i) per node
+    bool want_line = false;           // mixed slab solve asked for the x-line preconditioner
+    int line_segment = 0;             // nodes per x-line segment of the factors (32 or a block)
+    std::vector<uint8_t> cls_host;    // slab class of every node (kept for the factors)
     // bjacobi (ILU(0) of the whole matrix): factors, level schedules, b and B b
     bool ilu = false;
     IluArgs ilu_args{};
@@ -431,6 +434,8 @@ bool plan_stage(cg_ctx* c, int threads) {
     return true;
 }
 
+int build_line_factors(cg_ctx* c, const std::vector<uint8_t>& cls, int segment);
+
 int alloc_vectors(cg_ctx* c) {
     const size_t n = (size_t)c->n;
     CG_TRY(dalloc_haloed(c, &c->d_V, n));
@@ -474,7 +479,7 @@ int alloc_vectors(cg_ctx* c) {
     c->cg_threads = 512;
     const int blocks_512 = c->cg_blocks;
     c->pipe_nodes = 0;
-    const bool want_line = c->d_line_ad != nullptr;
+    const bool want_line = c->want_line;
     c->line_pc = want_line;
     if (c->mixed() && c->slab && pick_pipe(c, 1)) {
         // one block of kPipeThreads per SM when the slab fills every SM with them (fewer
@@ -488,7 +493,9 @@ int alloc_vectors(cg_ctx* c) {
             // the x-line factors live after the staged windows; without room for both
             // the inner solve keeps Jacobi
             auto smem_of = [&](long long k) {
-                return (size_t)k * ((size_t)c->stage.cap + (c->line_pc ? (size_t)kLineCoef * pt : 0)) * sizeof(float);
+                return (size_t)k *
+                       ((size_t)c->stage.cap + (c->line_pc ? (size_t)kBlockLineCoef * pt + kBlockLineWords : 0)) *
+                       sizeof(float);
             };
             // the dynamic shared-memory limit is a property of the kernel for the whole
             // process, so it is raised once to the device's maximum (contexts with other
@@ -520,8 +527,13 @@ int alloc_vectors(cg_ctx* c) {
             }
         }
     }
-    // the HBM-resident mixed solve takes the x-line preconditioner whenever it is asked for
+    // the HBM-resident mixed solve takes the x-line preconditioner whenever it is asked for,
+    // on warp segments; the pipelined one on its blocks' segments
     if (c->pipe_nodes == 0) c->line_pc = want_line;
+    if (c->line_pc) {
+        CG_TRY(build_line_factors(c, c->cls_host, c->pipe_nodes > 0 ? c->cg_threads : 32));
+        std::vector<uint8_t>().swap(c->cls_host);
+    }
     if (c->ilu) {
         // one block while the level sweeps are short (block barriers between levels),
         // else the co-resident grid with grid barriers
@@ -540,18 +552,20 @@ int alloc_vectors(cg_ctx* c) {
 }
 
 // Factors of the mixed solve's x-line inner preconditioner (kernels/cg_mixed.cuh):
-// T = L D L^T on each segment of 32 nodes aligned on a multiple of 32, T the
-// tridiagonal x part of A (sub-diagonal = the coefficient of offset -1, cut at the
+// T = L D L^T on each segment of `segment` nodes aligned on a multiple of it (32 for
+// the warp solve of the HBM-resident kernel, the block size for the pipelined one), T
+// the tridiagonal x part of A (sub-diagonal = the coefficient of offset -1, cut at the
 // segment start), in FP64; stored per node as (a_i = -T_{i,i-1} / d_{i-1}, 1 / d_i).
-int build_line_factors(cg_ctx* c, const std::vector<uint8_t>& cls) {
+int build_line_factors(cg_ctx* c, const std::vector<uint8_t>& cls, int segment) {
     const SlabStencil& st = c->stencil;
+    c->line_segment = segment;
     const int no = st.n_offsets;
     std::vector<float2> ad((size_t)c->n);
     double dprev = 1.0;
     for (int i = 0; i < c->n; ++i) {
         const double* row = &st.a[(size_t)cls[i] * no];
         const double di = row[c->diag_slot];
-        const double lo = (i % 32 == 0) ? 0.0 : row[c->xm_slot];
+        const double lo = (i % segment == 0) ? 0.0 : row[c->xm_slot];
         const double l = lo / dprev;
         const double d = di - l * lo;
         if (!(d > 0.0)) return CG_ERR_ARG;   // A is SPD, so every pivot is positive
@@ -685,8 +699,8 @@ int upload_operator(cg_ctx* c) {
             if (st.offsets[o] == 1) c->xp_slot = o;
         }
         if (c->diag_slot < 0) return CG_ERR_ARG;
-        if (c->mixed() && c->cfg.mixed_inner_preconditioner == CG_INNER_PC_LINE && c->xm_slot >= 0)
-            CG_TRY(build_line_factors(c, cls));
+        c->want_line = c->mixed() && c->cfg.mixed_inner_preconditioner == CG_INNER_PC_LINE && c->xm_slot >= 0;
+        if (c->want_line) c->cls_host = cls;
         CG_CUDA(cudaStreamSynchronize(s));
     } else {
         const HostCsr& m = c->csr;
@@ -1386,6 +1400,7 @@ int cg_get_stats(cg_ctx* c, cg_stats* s) {
     s->pipelined_nodes_per_thread = c->pipe_nodes;
     s->cg_blocks = c->cg_blocks;
     s->inner_preconditioner = !c->mixed() ? -1 : (c->line_pc ? CG_INNER_PC_LINE : CG_INNER_PC_JACOBI);
+    s->inner_line_segment = c->line_pc ? c->line_segment : 0;
     if (c->have_cells && c->steps > 0) {
         CG_CUDA(cudaSetDevice(c->device));
         CG_CUDA(cudaMemcpy(&s->last_cg_iterations, c->d_ring + ((c->steps - 1) % kRing), sizeof(int),
@@ -1413,8 +1428,15 @@ int cg_apply_inner_preconditioner(cg_ctx* c, const double* x, double* y) {
     if (cudaMemcpyAsync(d, h.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
         rc = CG_ERR_CUDA;
     } else {
-        const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)c->ode_blocks);
-        line_pc_apply_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->n, c->d_line_ad, d, d + n);
+        if (c->line_segment > 32) {
+            // the pipelined solve's block segments: one block per segment
+            const int L = c->line_segment;
+            const size_t smem = ((size_t)kBlockLineCoef * L + kBlockLineWords) * sizeof(float);
+            line_pc_block_apply_kernel<<<(int)((n + L - 1) / L), L, smem, c->stream>>>(c->n, c->d_line_ad, d, d + n);
+        } else {
+            const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)c->ode_blocks);
+            line_pc_apply_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->n, c->d_line_ad, d, d + n);
+        }
         if (cudaGetLastError() != cudaSuccess ||
             cudaMemcpyAsync(h.data(), d + n, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
             cudaStreamSynchronize(c->stream) != cudaSuccess)

@@ -120,6 +120,8 @@ typedef struct {
                                       pipelined solve of a slab that fills every SM with them) */
     int inner_preconditioner;      /* mixed precision: CG_INNER_PC_* the inner solve uses
                                       (CG_INNER_PC_JACOBI on CSR meshes); FP64: -1 */
+    int inner_line_segment;        /* x-line preconditioner: nodes per segment its x-lines are cut
+                                      to (a block of the pipelined solve, else 32); 0 without it */
 } cg_stats;
 
 /* Fill cfg with Chaste's defaults (LR91, FE, dt 0.01, Am 1400, Cm 1, Jacobi, atol 2e-4). */

@@ -159,11 +159,14 @@ def test_line_preconditioned_inner_solve_takes_fewer_iterations(N):
 def test_inner_preconditioner_is_symmetric_and_inverts_the_x_lines(N, oracle):
     """The mixed solve's x-line inner preconditioner B, applied on the device: <Bx, y> =
     <x, By> to FP32 rounding, x^T B x > 0, and T B x = x with T the tridiagonal x-part
-    of the assembled A restricted to the 32-node segments B works on."""
+    of the assembled A restricted to the segments B works on (a block of the pipelined
+    solve: 512 nodes here, so the 41-node x-lines are mostly whole)."""
     case = dict(TC.TT06_3D, size=(0.4, 0.1, 0.05))
     t, _ = TC.make_gpu(N, precision=1, **case)
     o, _ = TC.make_oracle(oracle, **case)
     n = t.n
+    seg = t.stats().inner_line_segment
+    assert seg == 512
     rng = np.random.default_rng(3)
     x, y = rng.standard_normal(n), rng.standard_normal(n)
     bx, by = t.apply_inner_preconditioner(x), t.apply_inner_preconditioner(y)
@@ -174,7 +177,7 @@ def test_inner_preconditioner_is_symmetric_and_inverts_the_x_lines(N, oracle):
     for i in range(n):
         for k in range(rp[i], rp[i + 1]):
             j = cols[k]
-            same_segment = j // 32 == i // 32
+            same_segment = j // seg == i // seg
             if j == i or (abs(j - i) == 1 and same_segment):
                 tbx[i] += vals[k] * bx[j]
     assert np.max(np.abs(tbx - x)) <= 1e-4 * np.max(np.abs(x))
