@@ -28,6 +28,7 @@ PRECISION_FP64, PRECISION_MIXED = 0, 1
 STIM_NONE, STIM_SIMPLE, STIM_REGULAR = 0, 1, 2
 SOLVER_MONODOMAIN, SOLVER_OPERATOR_SPLITTING = 0, 1
 INNER_PC_LINE, INNER_PC_JACOBI = 0, 1
+BATCH_PER_BEAT, BATCH_PERSISTENT = 0, 1
 
 
 class ChasteGpuError(RuntimeError):
@@ -119,6 +120,8 @@ SIGNATURES = {
     "cg_batch_set_launch_shape": (C.c_int, [_vp, C.c_int, C.c_int]),
     "cg_batch_results": (C.c_int, [_vp, _dp, _dp, _ip, _ip, C.POINTER(C.c_float), _dp, _dp]),
     "cg_batch_destroy": (C.c_int, [_vp]),
+    "cg_batch_set_engine": (C.c_int, [_vp, C.c_int]),
+    "cg_batch_engine": (C.c_int, [_vp, _ip]),
     "cg_cable_default_config": (None, [C.POINTER(CableConfig)]),
     "cg_cable_create": (C.c_int, [C.POINTER(CableConfig), _ip, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "cg_cable_forward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp]),
@@ -412,6 +415,14 @@ class CellBatch:
         tpb, cpt = C.c_int(), C.c_int()
         check(lib().cg_batch_launch_shape(self.h, C.byref(tpb), C.byref(cpt)), "cg_batch_launch_shape")
         return tpb.value, cpt.value
+
+    def set_engine(self, engine):
+        check(lib().cg_batch_set_engine(self.h, int(engine)), "cg_batch_set_engine")
+
+    def engine(self):
+        e = C.c_int()
+        check(lib().cg_batch_engine(self.h, C.byref(e)), "cg_batch_engine")
+        return e.value
 
     def run(self):
         ms = C.c_double()

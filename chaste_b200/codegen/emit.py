@@ -655,6 +655,7 @@ class ModelEmitter:
         A("    // and so exp(rate*dt), are the same in every substep.")
         A(f"    static constexpr bool kRlVoltageOnly[{n}] = {{{vflags}}};")
         A(f"    CHB_HD static constexpr bool rl_voltage_only(int i) {{ return {vidx}; }}")
+        A(f"    static constexpr int kNumVoltageGates = {len(vonly)};")
         A("    // rl_terms of the voltage-only Rush-Larsen states (reads y[0] and p only).")
         A("    template <typename T>")
         A("    CHB_HD static void rl_terms_voltage(const T* __restrict__ y, const T* __restrict__ p,")
@@ -670,20 +671,20 @@ class ModelEmitter:
             A(f"        inf[{i}] = {pr(self._fold_expr(inf))};")
             A(f"        rate[{i}] = {pr(self._fold_expr(h))};")
         A("    }")
-        A("    // rl_terms of every other non-voltage state (no dV/dt).")
+        A("    // rl_terms of every state but the voltage-only gates (dV/dt in rate[0]).")
         A("    template <typename T>")
         A("    CHB_HD static void rl_terms_states(const T* __restrict__ y, T stim, T cm,")
         A("                                       const T* __restrict__ p, T* __restrict__ rate,")
         A("                                       T* __restrict__ inf) {")
         A("        (void)stim; (void)cm; (void)p; (void)inf;")
         r_exprs = []
-        for s_ in self.states[1:]:
+        for s_ in self.states:
             if s_ in vonly:
                 continue
             r_exprs += list(self.rl[s_]) if s_ in self.rl else [self.odes[s_]]
         lines.extend(self._body(r_exprs, pr))
         for i, s_ in enumerate(self.states):
-            if i == 0 or s_ in vonly:
+            if s_ in vonly:
                 continue
             if s_ in self.rl:
                 inf, h = self.rl[s_]

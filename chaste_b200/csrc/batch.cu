@@ -1,6 +1,10 @@
-// Batched single-cell populations (include/chaste_gpu.h, cg_batch_*): one
-// CUDA graph holding the persistent FP64+FP32 kernel, the per-beat error
-// kernel and the beat counter, replayed once per beat.
+// Batched single-cell populations (include/chaste_gpu.h, cg_batch_*).  Two engines:
+//   persistent (default): one CUDA graph holding ONE launch of population_kernel that
+//     runs every beat of every cell from a work queue (kernels/population.cuh);
+//   per beat: one CUDA graph holding batch_kernel, the per-beat error kernel and the
+//     beat counter, replayed once per beat (kernels/batch.cuh).
+// cg_batch_autotune times both (and the per-beat kernel's launch shapes) and keeps
+// the fastest.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -10,7 +14,7 @@
 #include <vector>
 
 #include "../../include/chaste_gpu.h"
-#include "kernels/batch.cuh"
+#include "kernels/population.cuh"
 
 using namespace chb;
 
@@ -18,6 +22,8 @@ struct cg_batch {
     int model = 0, n = 0, S = 0, P = 0, max_beats = 0, max_aps = 0, sample_every = 10, device = 0;
     int tpb = 64;
     int cpt = 1;            // cells per thread
+    int engine = CG_BATCH_PERSISTENT;
+    int pop_blocks = 1;     // persistent engine: co-resident blocks of kPopThreads
     long long steps_per_beat = 0;
     double dt = 0.01;
     DevStimulus stim{};
@@ -34,6 +40,8 @@ struct cg_batch {
     float* d_maxdv = nullptr;
     long long* d_launch = nullptr;
     int* d_status = nullptr;
+    int* d_order = nullptr;   // cells by decreasing beat count (the persistent engine's queue)
+    int* d_next = nullptr;    // its work-queue counter
     std::vector<double> y0;   // initial states, SoA
     ~cg_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -97,6 +105,32 @@ cudaError_t launch_beat(cg_batch* b, long long steps_override, bool with_error) 
     batch_beat_error_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(a, b->d_maxdv);
     batch_advance_kernel<<<1, 1, 0, b->stream>>>(b->d_launch);
     return cudaGetLastError();
+}
+
+PopArgs pop_args(const cg_batch* b, long long steps_override) {
+    PopArgs pa;
+    std::memset(&pa, 0, sizeof(pa));
+    pa.b = batch_args(b, steps_override);
+    pa.order = b->d_order;
+    pa.n_groups = (b->n + 31) / 32;
+    pa.next_group = b->d_next;
+    pa.max_dv = b->d_maxdv;
+    return pa;
+}
+
+cudaError_t launch_population(cg_batch* b, long long steps_override) {
+    cudaError_t e = cudaMemsetAsync(b->d_next, 0, sizeof(int), b->stream);
+    if (e != cudaSuccess) return e;
+    const PopArgs pa = pop_args(b, steps_override);
+    if (b->model == CG_MODEL_TT06) population_kernel<TenTusscher2006Epi><<<b->pop_blocks, kPopThreads, 0, b->stream>>>(pa);
+    else population_kernel<LuoRudy1991><<<b->pop_blocks, kPopThreads, 0, b->stream>>>(pa);
+    return cudaGetLastError();
+}
+
+// A run (or, with steps_override, the first steps of one) of the current engine.
+cudaError_t launch_engine(cg_batch* b, long long steps_override) {
+    return b->engine == CG_BATCH_PERSISTENT ? launch_population(b, steps_override)
+                                            : launch_beat(b, steps_override, false);
 }
 
 int reset_states(cg_batch* b) {
@@ -169,7 +203,8 @@ int cg_batch_create(int model, int n_cells, const int* beats, const double* para
         !balloc(b, &b->d_trk, 2 * n * sizeof(ApdTracker)) || !balloc(b, &b->d_apd, 2 * n * max_aps * sizeof(double)) ||
         !balloc(b, &b->d_vsamp, 2 * (size_t)nsamp * n * sizeof(float)) ||
         !balloc(b, &b->d_maxdv, n * b->max_beats * sizeof(float)) || !balloc(b, &b->d_launch, sizeof(long long)) ||
-        !balloc(b, &b->d_status, sizeof(int))) {
+        !balloc(b, &b->d_status, sizeof(int)) || !balloc(b, &b->d_order, n * sizeof(int)) ||
+        !balloc(b, &b->d_next, sizeof(int))) {
         cudaGetLastError();
         delete b;
         return CG_ERR_NOMEM;
@@ -180,7 +215,20 @@ int cg_batch_create(int model, int n_cells, const int* beats, const double* para
     b->y0.resize(n * b->S);
     for (int k = 0; k < b->S; ++k)
         for (size_t i = 0; i < n; ++i) b->y0[k * n + i] = init[k];
-    if (cudaMemcpy(b->d_beats, beats, n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+    // the persistent engine's queue: longest runs first (ties by cell index), so each
+    // group of 32 cells has about one length and the long runs start at once
+    std::vector<int> order(n);
+    for (size_t i = 0; i < n; ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return beats[x] > beats[y]; });
+    int sms = 1, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (model == CG_MODEL_TT06)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, population_kernel<TenTusscher2006Epi>, kPopThreads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, population_kernel<LuoRudy1991>, kPopThreads, 0);
+    b->pop_blocks = (int)std::max(1LL, std::min((long long)(n + 31) / 32, (long long)std::max(per_sm, 1) * sms));
+    if (cudaMemcpy(b->d_order, order.data(), n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->d_beats, beats, n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->d_params, p.data(), p.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaGetLastError();
         delete b;
@@ -204,14 +252,17 @@ int cg_batch_autotune(cg_batch* b, int steps, int* threads_per_block) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int cand = 0; cand < 8; ++cand) {
+    int best_engine = b->engine;
+    for (int cand = 0; cand < 9; ++cand) {
+        // candidates 0-7: the per-beat kernel's shapes; 8: the persistent engine
         const int c = cands[cand % 4];
-        b->tpb = c;
-        b->cpt = cand < 4 ? 1 : 2;
+        b->engine = cand < 8 ? CG_BATCH_PER_BEAT : CG_BATCH_PERSISTENT;
+        b->tpb = cand < 8 ? c : best_tpb;
+        b->cpt = cand < 8 ? (cand < 4 ? 1 : 2) : best_cpt;
         int rc = reset_states(b);
         if (rc != CG_OK) return rc;
         cudaEventRecord(e0, b->stream);
-        if (launch_beat(b, steps, false) != cudaSuccess) {
+        if (launch_engine(b, steps) != cudaSuccess) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
             return CG_ERR_CUDA;
@@ -222,12 +273,16 @@ int cg_batch_autotune(cg_batch* b, int steps, int* threads_per_block) {
         cudaEventElapsedTime(&ms, e0, e1);
         if (ms < best) {
             best = ms;
-            best_tpb = c;
-            best_cpt = b->cpt;
+            best_engine = b->engine;
+            if (cand < 8) {
+                best_tpb = c;
+                best_cpt = b->cpt;
+            }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    b->engine = best_engine;
     b->tpb = best_tpb;
     b->cpt = best_cpt;
     if (b->graph) {
@@ -244,6 +299,7 @@ int cg_batch_set_launch_shape(cg_batch* b, int threads_per_block, int cells_per_
         return CG_ERR_ARG;
     b->tpb = threads_per_block;
     b->cpt = cells_per_thread;
+    b->engine = CG_BATCH_PER_BEAT;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -258,6 +314,22 @@ int cg_batch_launch_shape(const cg_batch* b, int* threads_per_block, int* cells_
     return CG_OK;
 }
 
+int cg_batch_set_engine(cg_batch* b, int engine) {
+    if (!b || (engine != CG_BATCH_PER_BEAT && engine != CG_BATCH_PERSISTENT)) return CG_ERR_ARG;
+    b->engine = engine;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return CG_OK;
+}
+
+int cg_batch_engine(const cg_batch* b, int* engine) {
+    if (!b || !engine) return CG_ERR_ARG;
+    *engine = b->engine;
+    return CG_OK;
+}
+
 int cg_batch_run(cg_batch* b, double* ms) {
     if (!b) return CG_ERR_ARG;
     cudaSetDevice(b->device);
@@ -267,7 +339,7 @@ int cg_batch_run(cg_batch* b, double* ms) {
             cudaGetLastError();
             return CG_ERR_CUDA;
         }
-        const cudaError_t le = launch_beat(b, 0, true);
+        const cudaError_t le = b->engine == CG_BATCH_PERSISTENT ? launch_population(b, 0) : launch_beat(b, 0, true);
         const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (le != cudaSuccess || ce != cudaSuccess || cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) {
             cudaGetLastError();
@@ -282,7 +354,8 @@ int cg_batch_run(cg_batch* b, double* ms) {
     cudaEventCreate(&e1);
     cudaEventRecord(e0, b->stream);
     bool ok = true;
-    for (int k = 0; k < b->max_beats && ok; ++k) ok = cudaGraphLaunch(b->graph, b->stream) == cudaSuccess;
+    const int replays = b->engine == CG_BATCH_PERSISTENT ? 1 : b->max_beats;
+    for (int k = 0; k < replays && ok; ++k) ok = cudaGraphLaunch(b->graph, b->stream) == cudaSuccess;
     cudaEventRecord(e1, b->stream);
     ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
     float t = 0.f;

@@ -493,9 +493,7 @@ int alloc_vectors(cg_ctx* c) {
             // the x-line factors live after the staged windows; without room for both
             // the inner solve keeps Jacobi
             auto smem_of = [&](long long k) {
-                return (size_t)k *
-                       ((size_t)c->stage.cap + (c->line_pc ? (size_t)kBlockLineCoef * pt + kBlockLineWords : 0)) *
-                       sizeof(float);
+                return (size_t)k * ((size_t)c->stage.cap + (c->line_pc ? (size_t)kLineCoef * pt : 0)) * sizeof(float);
             };
             // the dynamic shared-memory limit is a property of the kernel for the whole
             // process, so it is raised once to the device's maximum (contexts with other
@@ -527,11 +525,11 @@ int alloc_vectors(cg_ctx* c) {
             }
         }
     }
-    // the HBM-resident mixed solve takes the x-line preconditioner whenever it is asked for,
-    // on warp segments; the pipelined one on its blocks' segments
+    // the HBM-resident mixed solve takes the x-line preconditioner whenever it is asked for;
+    // both solves cut the x-lines into the 32-node segments of a warp
     if (c->pipe_nodes == 0) c->line_pc = want_line;
     if (c->line_pc) {
-        CG_TRY(build_line_factors(c, c->cls_host, c->pipe_nodes > 0 ? c->cg_threads : 32));
+        CG_TRY(build_line_factors(c, c->cls_host, 32));
         std::vector<uint8_t>().swap(c->cls_host);
     }
     if (c->ilu) {
@@ -552,10 +550,10 @@ int alloc_vectors(cg_ctx* c) {
 }
 
 // Factors of the mixed solve's x-line inner preconditioner (kernels/cg_mixed.cuh):
-// T = L D L^T on each segment of `segment` nodes aligned on a multiple of it (32 for
-// the warp solve of the HBM-resident kernel, the block size for the pipelined one), T
-// the tridiagonal x part of A (sub-diagonal = the coefficient of offset -1, cut at the
-// segment start), in FP64; stored per node as (a_i = -T_{i,i-1} / d_{i-1}, 1 / d_i).
+// T = L D L^T on each segment of `segment` nodes aligned on a multiple of it (32: the
+// nodes a warp holds in one register slot or grid-stride step), T the tridiagonal x
+// part of A (sub-diagonal = the coefficient of offset -1, cut at the segment start),
+// in FP64; stored per node as (a_i = -T_{i,i-1} / d_{i-1}, 1 / d_i).
 int build_line_factors(cg_ctx* c, const std::vector<uint8_t>& cls, int segment) {
     const SlabStencil& st = c->stencil;
     c->line_segment = segment;
@@ -1428,15 +1426,8 @@ int cg_apply_inner_preconditioner(cg_ctx* c, const double* x, double* y) {
     if (cudaMemcpyAsync(d, h.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
         rc = CG_ERR_CUDA;
     } else {
-        if (c->line_segment > 32) {
-            // the pipelined solve's block segments: one block per segment
-            const int L = c->line_segment;
-            const size_t smem = ((size_t)kBlockLineCoef * L + kBlockLineWords) * sizeof(float);
-            line_pc_block_apply_kernel<<<(int)((n + L - 1) / L), L, smem, c->stream>>>(c->n, c->d_line_ad, d, d + n);
-        } else {
-            const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)c->ode_blocks);
-            line_pc_apply_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->n, c->d_line_ad, d, d + n);
-        }
+        const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)c->ode_blocks);
+        line_pc_apply_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->n, c->d_line_ad, d, d + n);
         if (cudaGetLastError() != cudaSuccess ||
             cudaMemcpyAsync(h.data(), d + n, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
             cudaStreamSynchronize(c->stream) != cudaSuccess)

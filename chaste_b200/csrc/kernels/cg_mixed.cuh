@@ -72,6 +72,7 @@ __device__ __forceinline__ float apply_row32(const CgArgs& a, const SlabShared<f
 // five A^(s) from a_i by four shuffle levels (warp_line_levels); an application is
 // then 10 shuffles and 11 multiply-adds.  Every lane of the warp takes part; the rows
 // of nodes past n are the identity (a = 0, 1/d = 1).
+constexpr int kLineCoef = 6;   // A^(1), A^(2), A^(4), A^(8), A^(16), 1 / d
 
 __device__ __forceinline__ void warp_line_levels(float a, float (&A)[5]) {
     const unsigned full = 0xffffffffu;
@@ -102,133 +103,20 @@ __device__ __forceinline__ float warp_line_solve(const float (&A)[5], float dinv
     return z;
 }
 
-// The same preconditioner on segments of a whole block's consecutive nodes (1024
-// or 512; CgArgs::line_pc == 2), so that most x-lines are solved whole: the warp
-// scan above handles each warp's 32 nodes, and the carries between the warps of the
-// block are a second scan over the warps, done by warp 0 through shared memory:
-//   y = v + P (.) C(extract(S v)),   S = the in-warp levels, extract = the value at
-//   each warp's last lane, C = Y -> (the affine scan Y_w += G_w Y_{w-1} over the
-//   warps, shifted by one warp), P_i = a_{first lane}..a_i within the warp,
-//   G_w = the P of warp w's last lane.
-// The backward pass F^T is the literal transpose of those steps with the same stored
-// coefficients (P-weighted warp sums, the transposed warp scan, added at each warp's
-// last lane, then the transposed in-warp levels), so B stays exactly symmetric.
-// Shared memory: kBlockLineCoef words per slot and thread (the five A^(s), P, 1/d),
-// the five warp-scan levels of G per slot, and two carry vectors per slot.
-constexpr int kBlockLineCoef = 7;
-constexpr int kBlockLineWords = 5 * 32 + 2 * 32;   // per slot, after the per-thread words
-
-// Per-slot set-up: cf points at this thread's word 0 of the slot (stride ld), lw at the
-// slot's kBlockLineWords (its forward carry vector is the scratch here).  All threads
-// of the block.
-__device__ __forceinline__ void block_line_setup(float2 ad, float* cf, int ld, float* lw) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// Per-slot factors kept in shared memory by the pipelined solve.
+__device__ __forceinline__ void warp_line_setup(float2 ad, float* cf, int ld) {
     float A[5];
     warp_line_levels(ad.x, A);
-    float P = ad.x;   // inclusive prefix product of a within the warp
-#pragma unroll
-    for (int s = 1; s < 32; s <<= 1) {
-        const float Pm = __shfl_up_sync(full, P, s);
-        if (lane >= s) P *= Pm;
-    }
 #pragma unroll
     for (int j = 0; j < 5; ++j) cf[j * ld] = A[j];
-    cf[5 * ld] = P;
-    cf[6 * ld] = ad.y;
-    if (lane == 31) lw[160 + w] = P;
-    __syncthreads();
-    if (w == 0) {
-        float G[5];
-        warp_line_levels(lane < nw ? lw[160 + lane] : 0.0f, G);
-#pragma unroll
-        for (int j = 0; j < 5; ++j) lw[j * 32 + lane] = G[j];
-    }
-    __syncthreads();
+    cf[5 * ld] = ad.y;
 }
 
-// v[k] <- B v[k] for the KMAX slots of this thread; cf + k * slot_stride = this
-// thread's word 0 of slot k; lw + k * kBlockLineWords = slot k's warp-scan levels
-// (5 x 32) and its forward and backward carry vectors (32 each).  Every thread of the
-// block calls it (four block barriers).
-template <int KMAX>
-__device__ __forceinline__ void block_line_apply(float (&v)[KMAX], const float* cf, int slot_stride, int ld,
-                                                 float* lw) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    // forward: in-warp levels, then the carries between the warps
+__device__ __forceinline__ float warp_line_apply(const float* cf, int ld, float v) {
+    float A[5];
 #pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-        const float* c = cf + k * slot_stride;
-#pragma unroll
-        for (int j = 0; j < 5; ++j) v[k] += c[j * ld] * __shfl_up_sync(full, v[k], 1 << j);
-        if (lane == 31) lw[k * kBlockLineWords + 160 + w] = v[k];
-    }
-    __syncthreads();
-    if (w == 0) {
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k) {
-            float* h = lw + k * kBlockLineWords;
-            float Y = lane < nw ? h[160 + lane] : 0.0f;
-#pragma unroll
-            for (int j = 0; j < 5; ++j) Y += h[j * 32 + lane] * __shfl_up_sync(full, Y, 1 << j);
-            const float C = __shfl_up_sync(full, Y, 1);
-            h[160 + lane] = lane == 0 ? 0.0f : C;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-        const float* c = cf + k * slot_stride;
-        const float P = c[5 * ld];
-        v[k] = (v[k] + P * lw[k * kBlockLineWords + 160 + w]) * c[6 * ld];
-        // backward, the transpose: P-weighted warp sums first
-        const float d = warp_sum_f(P * v[k]);
-        if (lane == 0) lw[k * kBlockLineWords + 192 + w] = d;
-    }
-    __syncthreads();
-    if (w == 0) {
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k) {
-            float* h = lw + k * kBlockLineWords;
-            const float D = lane < nw ? h[192 + lane] : 0.0f;
-            float x = __shfl_down_sync(full, D, 1);
-            if (lane + 1 >= nw) x = 0.0f;
-#pragma unroll
-            for (int j = 4; j >= 0; --j) {
-                const int s = 1 << j;
-                const float t = __shfl_down_sync(full, h[j * 32 + lane] * x, s);
-                if (lane + s < 32) x += t;
-            }
-            h[192 + lane] = x;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-        const float* c = cf + k * slot_stride;
-        if (lane == 31) v[k] += lw[k * kBlockLineWords + 192 + w];
-#pragma unroll
-        for (int j = 4; j >= 0; --j) {
-            const int s = 1 << j;
-            const float t = __shfl_down_sync(full, c[j * ld] * v[k], s);
-            if (lane + s < 32) v[k] += t;
-        }
-    }
-}
-
-// y = B x with the block x-line solve (segments of blockDim nodes, one block each).
-static __global__ void line_pc_block_apply_kernel(int n, const float2* __restrict__ ad, const float* __restrict__ x,
-                                                  float* __restrict__ y) {
-    extern __shared__ float lsm[];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool on[1] = {i < n};
-    float* cf = lsm + threadIdx.x;
-    float* lw = lsm + kBlockLineCoef * blockDim.x;
-    block_line_setup(on[0] ? ad[i] : make_float2(0.0f, 1.0f), cf, blockDim.x, lw);
-    float v[1] = {on[0] ? x[i] : 0.0f};
-    block_line_apply<1>(v, cf, kBlockLineCoef * blockDim.x, blockDim.x, lw);
-    if (on[0]) y[i] = v[0];
+    for (int j = 0; j < 5; ++j) A[j] = cf[j * ld];
+    return warp_line_solve(A, cf[5 * ld], v);
 }
 
 // (a_i, 1/d_i) of node i, identity for nodes past n.
@@ -573,20 +461,11 @@ __device__ __forceinline__ float apply_a32_staged(const CgArgs& a, const SlabSha
     return acc;
 }
 
-// v <- B v for the KMAX register slots: the block x-line solve (a.line_pc) or Jacobi.
-// Every thread of the block calls it.
-template <int KMAX>
-__device__ __forceinline__ void inner_pc_slots(const CgArgs& a, float (&v)[KMAX], const float (&dinv)[KMAX],
-                                               const bool (&on)[KMAX], const float* cf, int ld, float* lw) {
-    if (!a.line_pc) {
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k) v[k] *= dinv[k];
-        return;
-    }
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k)
-        if (!on[k]) v[k] = 0.0f;
-    block_line_apply<KMAX>(v, cf, kBlockLineCoef * ld, ld, lw);
+// B d for register slot k: the x-line solve (a.line_pc) or Jacobi.
+__device__ __forceinline__ float apply_inner_pc(const CgArgs& a, const float* cf, int ld, bool on, float dinv,
+                                                float d) {
+    if (!a.line_pc) return dinv * d;
+    return warp_line_apply(cf, ld, on ? d : 0.0f);
 }
 
 template <int NOFF, int KMAX>
@@ -597,12 +476,9 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
     extern __shared__ float4 stage4[];
     float* stage = reinterpret_cast<float*>(stage4);
     // x-line factors after the staged windows: slot k, word j of thread t at
-    // line_cf[(k * kBlockLineCoef + j) * blockDim.x + t]; then each slot's warp-scan
-    // levels and carry vectors (kBlockLineWords) at line_w
-    const int ld = blockDim.x;
+    // line_cf[(k * kLineCoef + j) * blockDim.x + t]
     float* line_cf = stage + KMAX * a.stage.cap;
-    float* line_w = line_cf + KMAX * kBlockLineCoef * ld;
-    float* my_cf = line_cf + threadIdx.x;
+    const int ld = blockDim.x;
     __shared__ __align__(8) unsigned long long stage_bar;
     unsigned stage_parity = 0;
     if (threadIdx.x == 0) mbar_init(&stage_bar);
@@ -630,8 +506,7 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
     if (a.line_pc) {
 #pragma unroll
         for (int k = 0; k < KMAX; ++k)
-            block_line_setup(line_factors(a, on[k], node[k]), my_cf + k * kBlockLineCoef * ld, ld,
-                             line_w + k * kBlockLineWords);
+            warp_line_setup(line_factors(a, on[k], node[k]), line_cf + k * kLineCoef * ld + threadIdx.x, ld);
     }
     float r[KMAX], u[KMAX], w[KMAX], m[KMAX], zq[KMAX], q[KMAX], sv[KMAX], p[KMAX], e[KMAX];
     double res[4];
@@ -656,12 +531,9 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
                 r64[i] = rr;
                 r[k] = (float)rr;
             }
-            u[k] = r[k];
-        }
-        inner_pc_slots<KMAX>(a, u, dinv, on, my_cf, ld, line_w);
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k)
+            u[k] = apply_inner_pc(a, line_cf + k * kLineCoef * ld + threadIdx.x, ld, on[k], dinv[k], r[k]);
             if (on[k]) z32[node[k]] = u[k];
+        }
         if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
     }
     double rnorm0 = sqrt(res[1]);
@@ -697,12 +569,9 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
             for (int k = 0; k < KMAX; ++k) {
                 v[0] += (double)r[k] * (double)u[k];
                 v[1] += (double)w[k] * (double)u[k];
-                m[k] = w[k];
-            }
-            inner_pc_slots<KMAX>(a, m, dinv, on, my_cf, ld, line_w);
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k)
+                m[k] = apply_inner_pc(a, line_cf + k * kLineCoef * ld + threadIdx.x, ld, on[k], dinv[k], w[k]);
                 if (on[k]) mb[node[k]] = m[k];
+            }
             if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
             const double gamma = res[0], delta = res[1];
             if (it == 0) g0 = gamma;
@@ -765,12 +634,9 @@ __device__ __forceinline__ void cg_mixed_pipe_kernel_body(const CgArgs& a, unsig
                     v[0] += zz * zz;
                     r[k] = (float)rr;
                 }
-                u[k] = r[k];
-            }
-            inner_pc_slots<KMAX>(a, u, dinv, on, my_cf, ld, line_w);
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k)
+                u[k] = apply_inner_pc(a, line_cf + k * kLineCoef * ld + threadIdx.x, ld, on[k], dinv[k], r[k]);
                 if (on[k]) z32[node[k]] = u[k];
+            }
             if (!grid_reduce<1>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }
         dp = sqrt(res[0]);

@@ -100,12 +100,6 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__device__ __forceinline__ float warp_sum_f(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
 // One thread waits until *counter >= target (acquire), for at most limit_ns of
 // %globaltimer.  On timeout, or when another waiter has already timed out, it sets
 // kStatusBarrierTimeout and returns false: every wait of a kernel ends.

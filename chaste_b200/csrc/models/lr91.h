@@ -119,6 +119,7 @@ struct LuoRudy1991 {
     // and so exp(rate*dt), are the same in every substep.
     static constexpr bool kRlVoltageOnly[8] = {false, true, true, true, true, true, true, false};
     CHB_HD static constexpr bool rl_voltage_only(int i) { return i == 1 || i == 2 || i == 3 || i == 4 || i == 5 || i == 6; }
+    static constexpr int kNumVoltageGates = 6;
     // rl_terms of the voltage-only Rush-Larsen states (reads y[0] and p only).
     template <typename T>
     CHB_HD static void rl_terms_voltage(const T* __restrict__ y, const T* __restrict__ p,
@@ -149,14 +150,28 @@ struct LuoRudy1991 {
         inf[6] = (-m_div(v_time_dependent_potassium_current_X_gate__alpha_X, (-v_time_dependent_potassium_current_X_gate__alpha_X - v_time_dependent_potassium_current_X_gate__beta_X)));
         rate[6] = (-v_time_dependent_potassium_current_X_gate__alpha_X - v_time_dependent_potassium_current_X_gate__beta_X);
     }
-    // rl_terms of every other non-voltage state (no dV/dt).
+    // rl_terms of every state but the voltage-only gates (dV/dt in rate[0]).
     template <typename T>
     CHB_HD static void rl_terms_states(const T* __restrict__ y, T stim, T cm,
                                        const T* __restrict__ p, T* __restrict__ rate,
                                        T* __restrict__ inf) {
         (void)stim; (void)cm; (void)p; (void)inf;
+        const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
+        const T v_fast_sodium_current__i_Na = ((T(23.0)*p[0])*(y[1]*y[1]*y[1])*y[2]*y[3]*(y[0] - T(54.79446393509185)));
+        const T v_membrane__I_stim = stim;
+        const T v_plateau_potassium_current__Kp = (m_div(T(1.0), (T(1.0) + m_exp((m_divk((T(7.488) - y[0]), T(5.98), T(0.16722408026755853)))))));
+        const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*v_plateau_potassium_current__Kp*(y[0] - (-T(87.8929017138025))));
         const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*m_log((m_divk(y[7], T(1.0), T(1.0))))));
         const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
+        const T v_time_dependent_potassium_current_Xi_gate__Xi = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? ((m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0))))))) + (m_div((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*((m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0))))))) - (m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))), (T(2.0)*(chb::singularity_offset<T>()*T(1.0)))))) : (m_div((T(2.837)*(m_exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0))), ((y[0] + T(77.0))*m_exp((T(0.04)*(y[0] + T(35.0)))))))) : T(1.0));
+        const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
+        const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*v_time_dependent_potassium_current_Xi_gate__Xi*(y[0] - (-T(77.56758438531939))));
+        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (m_div(T(1.02), (T(1.0) + m_exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215)))))));
+        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (m_div(((T(0.49124)*m_exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*m_exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31))))))), (T(1.0) + m_exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753)))))));
+        const T v_time_independent_potassium_current_K1_gate__K1_infinity = (m_div(v_time_independent_potassium_current_K1_gate__alpha_K1, (v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1)));
+        const T v_time_independent_potassium_current__g_K1__scaled = (T(0.6047)*p[3]);
+        const T v_time_independent_potassium_current__i_K1 = (v_time_independent_potassium_current__g_K1__scaled*v_time_independent_potassium_current_K1_gate__K1_infinity*(y[0] - (-T(87.8929017138025))));
+        rate[0] = ((m_divk((-T(1.0)), T(1.0), T(1.0)))*(v_membrane__I_stim + v_fast_sodium_current__i_Na + v_slow_inward_current__i_si + v_time_dependent_potassium_current__i_K + v_time_independent_potassium_current__i_K1 + v_plateau_potassium_current__i_Kp + v_background_current__i_b));
         rate[7] = (((m_divk((-T(0.0001)), T(1.0), T(1.0)))*v_slow_inward_current__i_si) + (T(0.07)*(T(0.0001) - y[7])));
     }
 

@@ -121,7 +121,7 @@ typedef struct {
     int inner_preconditioner;      /* mixed precision: CG_INNER_PC_* the inner solve uses
                                       (CG_INNER_PC_JACOBI on CSR meshes); FP64: -1 */
     int inner_line_segment;        /* x-line preconditioner: nodes per segment its x-lines are cut
-                                      to (a block of the pipelined solve, else 32); 0 without it */
+                                      to (32, a warp's nodes); 0 without it */
 } cg_stats;
 
 /* Fill cfg with Chaste's defaults (LR91, FE, dt 0.01, Am 1400, Cm 1, Jacobi, atol 2e-4). */
@@ -209,16 +209,28 @@ const char* cg_status_string(int status);
 typedef struct cg_batch cg_batch;
 int cg_batch_create(int model, int n_cells, const int* beats, const double* params, const cg_stimulus* stim,
                     double dt, double beat_length, int max_aps, int device, cg_batch** out);
-/* Times each candidate launch shape -- threads per block (32, 64, 128, 256) x
- * cells advanced together by each thread (1, 2) -- on `steps` steps and keeps the
- * fastest; the population is reset to its initial state afterwards. */
+/* Times each candidate -- the per-beat kernel's launch shapes, threads per block
+ * (32, 64, 128, 256) x cells advanced together by each thread (1, 2), and the
+ * persistent engine -- on `steps` steps and keeps the fastest; the population is
+ * reset to its initial state afterwards. */
 int cg_batch_autotune(cg_batch* b, int steps, int* threads_per_block);
-/* Set the launch shape (threads per block a multiple of 32 up to 1024, cells per
- * thread 1 or 2) without timing; results do not depend on it. */
+/* Set the per-beat engine's launch shape (threads per block a multiple of 32 up to
+ * 1024, cells per thread 1 or 2) without timing, and select that engine; results do
+ * not depend on it. */
 int cg_batch_set_launch_shape(cg_batch* b, int threads_per_block, int cells_per_thread);
 /* The launch shape in use (after cg_batch_autotune, or the default 64 x 1). */
 int cg_batch_launch_shape(const cg_batch* b, int* threads_per_block, int* cells_per_thread);
-/* Runs every beat (one CUDA-graph replay per beat); ms = device time. */
+/* Engines: CG_BATCH_PERSISTENT (default) runs the whole population in ONE launch
+ * inside a CUDA graph -- blocks of 4 warps draw groups of 32 cells from a work queue
+ * ordered by decreasing beat count, and each cell's step is split over a gate thread
+ * (the voltage-only gates) and a state thread (currents, V, other states), with the
+ * FP64 and FP32 copies in lockstep; CG_BATCH_PER_BEAT replays a graph of one launch
+ * per beat.  cg_batch_autotune times both and keeps the faster; the results do not
+ * depend on the engine. */
+enum { CG_BATCH_PER_BEAT = 0, CG_BATCH_PERSISTENT = 1 };
+int cg_batch_set_engine(cg_batch* b, int engine);
+int cg_batch_engine(const cg_batch* b, int* engine);
+/* Runs every beat of every cell; ms = device time. */
 int cg_batch_run(cg_batch* b, double* ms);
 /* apd64/apd32: n_cells x max_aps (-1 where no AP), n_ap: APs completed per cell,
  * max_dv: n_cells x max_beats largest |V32 - V64| per beat (0.1 ms samples),

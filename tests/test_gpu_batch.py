@@ -24,14 +24,22 @@ def population(n, seed=20261203, max_beats=3):
     return params, beats
 
 
-def test_population_matches_oracle_cells(N, oracle):
+@pytest.mark.parametrize("engine", ["autotuned", "per_beat", "persistent"])
+def test_population_matches_oracle_cells(N, oracle, engine):
     O = oracle
     n = 64
     params, beats = population(n)
     beats[:2] = 2
     b = N.CellBatch(N.MODEL_TT06, beats, params)
-    tpb = b.autotune(steps=500)
-    assert tpb in (32, 64, 128, 256)
+    if engine == "autotuned":
+        tpb = b.autotune(steps=500)
+        assert tpb in (32, 64, 128, 256)
+        assert b.engine() in (N.BATCH_PER_BEAT, N.BATCH_PERSISTENT)
+    elif engine == "per_beat":
+        b.set_launch_shape(64, 1)
+        assert b.engine() == N.BATCH_PER_BEAT
+    else:
+        b.set_engine(N.BATCH_PERSISTENT)
     b.run()
     r = b.results()
     stim = O.regular(-52.0, 1.0, 1000.0, 50.0)
@@ -66,3 +74,24 @@ def test_cells_per_thread_do_not_change_results(N):
         out.append(b.results())
     for key in ("apd64", "apd32", "states64", "states32", "max_dv", "n_ap64", "n_ap32"):
         assert np.array_equal(out[0][key], out[1][key]), key
+
+
+@pytest.mark.parametrize("model", ["TT06", "LR91"])
+def test_persistent_engine_equals_per_beat_launches(N, model):
+    """The persistent engine (one launch, work queue, each cell split over a gate
+    thread and a state thread) gives bitwise the states, APDs and per-beat errors of
+    the per-beat launches, for an odd population with uneven beat counts."""
+    params, beats = population(45, seed=11, max_beats=3)
+    m = getattr(N, f"MODEL_{model}")
+    if model == "LR91":
+        params = params[:, :6]
+    out = []
+    for engine in (N.BATCH_PER_BEAT, N.BATCH_PERSISTENT):
+        b = N.CellBatch(m, beats, params)
+        b.set_engine(engine)
+        b.run()
+        out.append(b.results())
+    for key in ("states64", "states32", "n_ap64", "n_ap32", "max_dv"):
+        assert np.array_equal(out[0][key], out[1][key]), key
+    for key in ("apd64", "apd32"):
+        assert np.max(np.abs(out[0][key] - out[1][key])) <= 1e-9, key

@@ -159,14 +159,13 @@ def test_line_preconditioned_inner_solve_takes_fewer_iterations(N):
 def test_inner_preconditioner_is_symmetric_and_inverts_the_x_lines(N, oracle):
     """The mixed solve's x-line inner preconditioner B, applied on the device: <Bx, y> =
     <x, By> to FP32 rounding, x^T B x > 0, and T B x = x with T the tridiagonal x-part
-    of the assembled A restricted to the segments B works on (a block of the pipelined
-    solve: 512 nodes here, so the 41-node x-lines are mostly whole)."""
+    of the assembled A restricted to the 32-node segments B works on."""
     case = dict(TC.TT06_3D, size=(0.4, 0.1, 0.05))
     t, _ = TC.make_gpu(N, precision=1, **case)
     o, _ = TC.make_oracle(oracle, **case)
     n = t.n
     seg = t.stats().inner_line_segment
-    assert seg == 512
+    assert seg == 32
     rng = np.random.default_rng(3)
     x, y = rng.standard_normal(n), rng.standard_normal(n)
     bx, by = t.apply_inner_preconditioner(x), t.apply_inner_preconditioner(y)
