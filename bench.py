@@ -331,8 +331,9 @@ def cpu_baseline(wl, start_steps, seconds=15.0, threads=None):
 
 def run_population(args):
     """8192 TT06 cells, six conductances scaled by lognormal(0, 0.2), 1-20 beats
-    (uniform) at BCL 1000 ms, stimulus -52 uA/uF for 1 ms, Rush-Larsen dt 0.01 ms, FP64 and FP32 in one
-    launch per beat (CUDA graph).  Metric: cell-steps/s over both precisions' shared launches."""
+    (uniform) at BCL 1000 ms, stimulus -52 uA/uF for 1 ms, Rush-Larsen dt 0.01 ms, FP64 and FP32 side by
+    side, the engine the autotuner picks (one persistent launch in a CUDA graph, or one launch per beat).
+    Metric: cell-steps/s over both precisions."""
     from chaste_b200 import _native as N
     from chaste_b200.build import build_native
 
@@ -345,6 +346,7 @@ def run_population(args):
     b = N.CellBatch(N.MODEL_TT06, beats, params)
     b.autotune(steps=2000)
     tpb, cpt = b.launch_shape()
+    engine = "persistent" if b.engine() == N.BATCH_PERSISTENT else "per_beat"
     ms = b.run()
     r = b.results()
     steps = int(beats.sum()) * 100000
@@ -357,8 +359,12 @@ def run_population(args):
             "higher_is_better": True, "dtype": "f64+f32", "data": "synthetic",
             "config": {"workload": "8192 TT06-epi cells, lognormal(0,0.2) conductance scales, 1-20 beats at "
                                    "BCL 1000 ms, RL dt 0.01 ms", "cell_steps_per_precision": steps,
-                       "threads_per_block": tpb, "cells_per_thread": cpt,
-                       "launch_shape": "autotuned over threads per block x cells per thread"},
+                       "engine": engine,
+                       "threads_per_block": tpb if engine == "per_beat" else 128,
+                       "cells_per_thread": cpt if engine == "per_beat" else 0.5,
+                       "launch_shape": "autotuned over the per-beat kernel's threads per block x cells per "
+                                       "thread and the persistent engine (one launch, work queue, two threads "
+                                       "per cell)"},
             "apd90_fp32_vs_fp64_ms": {"max": max(d_apd), "mean": float(np.mean(d_apd)), "n": len(d_apd)},
             "per_beat_max_vm_error_mv": {"max": max(dv), "median": float(np.median(dv))}}
 

@@ -12,8 +12,9 @@
 //                        CellProperties bookkeeping and the samples.
 //
 // Both start a step from the same state, as the reference step does (every term from
-// the step's start values, then V, then the gates), so the result equals the
-// single-thread step bit for bit.  They meet once per step at a block barrier:
+// the step's start values, then V, then the gates), so the step is the single-thread
+// step's arithmetic (to the compiler's choice of fused multiply-adds, which may differ
+// between the two code paths).  They meet once per step at a block barrier:
 // the state thread publishes V(t+dt), the gate thread the gates at t+dt, in
 // double-buffered shared memory.  A block has four warps: FP64 state, FP64 gates,
 // FP32 state, FP32 gates -- lane l of each holds cell l of the group -- so the two

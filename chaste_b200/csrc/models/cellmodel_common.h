@@ -36,10 +36,27 @@ namespace chb {
 #ifndef CHB_FAST_FP32
 #define CHB_FAST_FP32 1
 #endif
+// On the device the double-precision functions are called, not inlined
+// (CHB_FP64_CALLS, default 1): a cell model evaluates dozens of them per step, and one
+// shared copy of each keeps the straight-line model code small enough for the
+// instruction cache -- inlined, the FP64 kernels stalled on instruction fetch.  The
+// values are those of the inlined library functions.
+#ifndef CHB_FP64_CALLS
+#define CHB_FP64_CALLS 1
+#endif
+#if defined(__CUDA_ARCH__) && CHB_FP64_CALLS
+__device__ __noinline__ double m_exp_call(double x) { return ::exp(x); }
+__device__ __noinline__ double m_log_call(double x) { return ::log(x); }
+__device__ __noinline__ double m_pow_call(double x, double y) { return ::pow(x, y); }
+CHB_HD double m_exp(double x) { return m_exp_call(x); }
+CHB_HD double m_log(double x) { return m_log_call(x); }
+CHB_HD double m_pow(double x, double y) { return m_pow_call(x, y); }
+#else
 CHB_HD double m_exp(double x) { return ::exp(x); }
 CHB_HD double m_log(double x) { return ::log(x); }
-CHB_HD double m_sqrt(double x) { return ::sqrt(x); }
 CHB_HD double m_pow(double x, double y) { return ::pow(x, y); }
+#endif
+CHB_HD double m_sqrt(double x) { return ::sqrt(x); }
 CHB_HD float m_exp(float x) {
 #if defined(__CUDA_ARCH__) && CHB_FAST_FP32
     return __expf(x);
