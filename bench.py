@@ -443,6 +443,72 @@ def run_cable(args):
     return line
 
 
+def mixed_population_runs(N, F, rng):
+    """4096 LR91 single cells (Rush-Larsen dt 0.01 ms, 1-10 beats at BCL 500 ms, six conductances scaled by
+    lognormal(0, 0.2), V sampled every 1 ms) and 64 LR91 cables (100-1000 nodes, 50-400 ms, 1-4 regions x 7
+    lognormal(0, 0.2) scales, 5 probes sampled every 0.1 ms), every run of its own length."""
+    cells, cables = [], []
+    stim = N.stimulus(N.STIM_REGULAR, -25.5, 2.0, 5.0, 500.0)
+    for _ in range(4096):
+        cells.append((int(rng.integers(1, 11)) * 50000, np.exp(rng.normal(0.0, 0.2, size=6))))
+    for _ in range(64):
+        cfg = F.default_cable_config()
+        cfg.n_nodes = int(rng.integers(100, 1001))
+        cfg.n_steps = int(rng.integers(5, 41)) * 1000
+        cfg.n_regions = int(rng.integers(1, 5))
+        cables.append((cfg, np.exp(rng.normal(0.0, 0.2, size=(cfg.n_regions, 7))), F.even_probes(cfg.n_nodes, 5)))
+    return stim, cells, cables
+
+
+def run_mixed(args):
+    """Single-cell and cable runs of LR91 with uneven lengths and their own parameters in ONE persistent
+    launch (cg_runs_*), launch shape autotuned.  Metric: node-steps/s, a single cell counting as one node."""
+    from chaste_b200 import _native as N
+    from chaste_b200 import fitting as F
+    from chaste_b200.build import build_native
+
+    build_native()
+    stim, cells, cables = mixed_population_runs(N, F, np.random.default_rng(20261204))
+    pop = N.RunPopulation(N.MODEL_LR91)
+    for steps, p in cells:
+        pop.add_cell(N.ODE_RUSH_LARSEN, steps, 0.01, 100, p, stim)
+    cids = [pop.add_cable(cfg, p, pr, 10) for cfg, p, pr in cables]
+    tpb, cpt = pop.autotune(steps=2000)
+    pop.run()                                   # warm-up
+    ms = pop.run()
+    cell_steps = sum(s for s, _ in cells)
+    cable_steps = sum(cfg.n_nodes * cfg.n_steps for cfg, _, _ in cables)
+    its = sum(pop.result(i)[2] for i in cids)
+    line = {"metric": "mixed single-cell + cable population node-steps/s (one persistent launch)",
+            "value": (cell_steps + cable_steps) / (ms / 1e3), "unit": "node-steps/s", "n_gpus": 1,
+            "ms_total": ms, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "4096 LR91 cells RL dt 0.01 ms 1-10 beats of 500 ms + 64 LR91 cables of "
+                                   "100-1000 nodes x 50-400 ms, dt 0.01 ms, CG+Jacobi rtol 1e-8",
+                       "cell_steps": cell_steps, "cable_node_steps": cable_steps,
+                       "cable_cg_iterations": int(its), "threads_per_block": tpb, "cells_per_thread": cpt}}
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+
+        from tests import cable_cases as CC
+
+        # a bounded sample: 8 cells for one beat each and the first 2000 steps of 2 cables
+        t0 = time.perf_counter()
+        n_cell = 0
+        for steps, p in cells[:8]:
+            y = O.initial_states(O.LR91)
+            O.cell_compute(O.LR91, O.RL, y, 0.0, 500.0, 0.01, 1.0, O.regular(-25.5, 2.0, 500.0, 5.0), params=p)
+            n_cell += 50000
+        n_cab = 0
+        for cfg, p, pr in cables[:2]:
+            cc = CC.PlainCableConfig(n_nodes=cfg.n_nodes, n_steps=2000, n_regions=cfg.n_regions)
+            O.cable_run(CC.oracle_config(O, cc), p, pr, traces=True)
+            n_cab += cfg.n_nodes * 2000
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": (n_cell + n_cab) / dt, "unit": "node-steps/s", "cores": 1, "kind": "port",
+                                "sample": f"8 cells x 1 beat and 2 cables x 2000 steps of the population, {dt:.1f} s"}
+    return line
+
+
 def aggregate(dist, device, ms_step, e2e_s, n, steps, world):
     """Whole-job figures of N replicas: the max over ranks of the device step time and of
     the end-to-end time (a collective on `device`: cuda for NCCL, cpu for gloo), then
@@ -480,7 +546,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tt06_slab_3d",
-                    choices=sorted(WORKLOADS) + ["tt06_population", "lr91_cable_adjoint"])
+                    choices=sorted(WORKLOADS) + ["tt06_population", "lr91_cable_adjoint", "lr91_mixed_population"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--t-start-ms", type=float, default=10.0,
@@ -530,6 +596,9 @@ def main():
         return
     if args.workload == "lr91_cable_adjoint":
         print(json.dumps(run_cable(args)), flush=True)
+        return
+    if args.workload == "lr91_mixed_population":
+        print(json.dumps(run_mixed(args)), flush=True)
         return
     rank, world, local, dist = dist_setup(args)
     wl = WORKLOADS[args.workload]

@@ -127,6 +127,15 @@ SIGNATURES = {
     "cg_cable_forward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp]),
     "cg_cable_backward": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
     "cg_cable_destroy": (C.c_int, [_vp]),
+    "cg_runs_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "cg_runs_add_cell": (C.c_int, [_vp, C.c_int, _dp, C.POINTER(Stimulus), C.c_double, C.c_int, C.c_int, _ip]),
+    "cg_runs_add_cable": (C.c_int, [_vp, C.POINTER(CableConfig), _dp, _ip, C.c_int, C.c_int, _ip]),
+    "cg_runs_autotune": (C.c_int, [_vp, C.c_int, _ip, _ip]),
+    "cg_runs_set_shape": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "cg_runs_shape": (C.c_int, [_vp, _ip, _ip]),
+    "cg_runs_run": (C.c_int, [_vp, _dp]),
+    "cg_runs_result": (C.c_int, [_vp, C.c_int, _dp, _dp, _ip, C.POINTER(C.c_longlong)]),
+    "cg_runs_destroy": (C.c_int, [_vp]),
     "cg_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_double, _ip, _dp]),
     "cg_output_configure": (C.c_int, [_vp, C.c_int, C.c_int, _ip, C.c_int]),
     "cg_output_frames": (C.c_int, [_vp, _ip, _dp]),
@@ -443,6 +452,81 @@ class CellBatch:
     def close(self):
         if getattr(self, "h", None):
             lib().cg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+class RunPopulation:
+    """Single-cell and cable runs of one cell model in one persistent launch (cg_runs)."""
+
+    def __init__(self, model, device=0):
+        self.model = model
+        self.n_states = num_states(model)
+        self.n_params = num_params(model)
+        self._cables = {}
+        h = C.c_void_p()
+        check(lib().cg_runs_create(model, device, C.byref(h)), "cg_runs_create")
+        self.h = h
+
+    def add_cell(self, method, n_steps, dt=0.01, sample_every=1, params=None, stim=None):
+        """Returns the run id; params: n_params scale factors (None: all 1)."""
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        i = C.c_int()
+        check(lib().cg_runs_add_cell(self.h, method, dptr(p), C.byref(stim) if stim is not None else None, dt,
+                                     int(n_steps), int(sample_every), C.byref(i)), "cg_runs_add_cell")
+        return i.value
+
+    def add_cable(self, cfg, params, probes, sample_every=1):
+        """cfg: CableConfig; params: n_regions x (n_params + 1); probes: node indices."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        pr = np.ascontiguousarray(probes, dtype=np.int32)
+        i = C.c_int()
+        check(lib().cg_runs_add_cable(self.h, C.byref(cfg), dptr(p), iptr(pr), pr.size, int(sample_every),
+                                      C.byref(i)), "cg_runs_add_cable")
+        self._cables[i.value] = (cfg.n_nodes, pr.size)
+        return i.value
+
+    def autotune(self, steps=200):
+        tpb, cpt = C.c_int(), C.c_int()
+        check(lib().cg_runs_autotune(self.h, steps, C.byref(tpb), C.byref(cpt)), "cg_runs_autotune")
+        return tpb.value, cpt.value
+
+    def set_shape(self, threads_per_block, cells_per_thread):
+        check(lib().cg_runs_set_shape(self.h, threads_per_block, cells_per_thread), "cg_runs_set_shape")
+
+    def shape(self):
+        tpb, cpt = C.c_int(), C.c_int()
+        check(lib().cg_runs_shape(self.h, C.byref(tpb), C.byref(cpt)), "cg_runs_shape")
+        return tpb.value, cpt.value
+
+    def run(self):
+        ms = C.c_double()
+        check(lib().cg_runs_run(self.h, C.byref(ms)), "cg_runs_run")
+        return ms.value
+
+    def result(self, run_id):
+        """Cell: (states (n_states,), trace (n_samples,)); cable: (states (n_nodes, n_states),
+        trace (n_samples, n_probes), cg_iterations)."""
+        ns = C.c_int()
+        check(lib().cg_runs_result(self.h, run_id, None, None, C.byref(ns), None), "cg_runs_result")
+        it = C.c_longlong()
+        if run_id in self._cables:
+            n, npr = self._cables[run_id]
+            st, tr = np.zeros((n, self.n_states)), np.zeros((ns.value, npr))
+            check(lib().cg_runs_result(self.h, run_id, dptr(st), dptr(tr), None, C.byref(it)), "cg_runs_result")
+            return st, tr, it.value
+        st, tr = np.zeros(self.n_states), np.zeros(ns.value)
+        check(lib().cg_runs_result(self.h, run_id, dptr(st), dptr(tr), None, None), "cg_runs_result")
+        return st, tr
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cg_runs_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -12,13 +12,22 @@ LIB_DIR = os.path.join(HERE, "lib")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 
-SOURCES = ["chaste_gpu.cu", "partition.cu", "noalloc.cu", "batch.cu", "cable.cu", "selftest.cu", "host/assemble.cpp"]
-DEPS = SOURCES + [
-    "kernels/common.cuh", "kernels/ops.cuh", "kernels/cg.cuh", "kernels/cg_mixed.cuh", "kernels/cg_ilu.cuh",
-    "kernels/ode.cuh", "kernels/batch.cuh", "kernels/cable.cuh", "kernels/svi.cuh", "kernels/output.cuh",
-    "models/cellmodel_common.h", "models/lr91.h", "models/tt06.h",
-    "host/assemble.h", "../../include/chaste_gpu.h",
-]
+SOURCES = ["chaste_gpu.cu", "partition.cu", "noalloc.cu", "batch.cu", "runs.cu", "cable.cu", "selftest.cu",
+           "host/assemble.cpp"]
+
+
+def _deps():
+    """Every source and header under csrc/ plus the public header: a change to any
+    of them rebuilds the library."""
+    out = ["../../include/chaste_gpu.h"]
+    for root, _, files in os.walk(CSRC):
+        for f in files:
+            if f.endswith((".cu", ".cuh", ".h", ".cpp")):
+                out.append(os.path.relpath(os.path.join(root, f), CSRC))
+    return sorted(out)
+
+
+DEPS = _deps()
 
 
 def nvcc():

@@ -213,7 +213,7 @@ __global__ void batch_kernel(BatchArgs a) {
 }
 
 // Largest |V32 - V64| over this beat's samples, per cell; then the beat counter.
-__global__ void batch_beat_error_kernel(BatchArgs a, float* max_dv) {
+static __global__ void batch_beat_error_kernel(BatchArgs a, float* max_dv) {
     const long long beat = *a.launch;
     const long long nsamp = (a.steps_per_beat + a.sample_every - 1) / a.sample_every;
     for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < a.n_cells; cell += gridDim.x * blockDim.x) {
@@ -228,6 +228,6 @@ __global__ void batch_beat_error_kernel(BatchArgs a, float* max_dv) {
     }
 }
 
-__global__ void batch_advance_kernel(long long* launch) { *launch += 1; }
+static __global__ void batch_advance_kernel(long long* launch) { *launch += 1; }
 
 }  // namespace chb

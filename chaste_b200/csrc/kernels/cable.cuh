@@ -73,7 +73,7 @@ struct CableShared {
 
 // Tridiagonal A and M, rows summed element by element in ascending order
 // (row i gets element i-1, then element i), consistent P1 mass h/6 [2 1; 1 2].
-__device__ void cable_assemble(const CableArgs& a, const double* prm, int stride, CableShared& s) {
+static __device__ void cable_assemble(const CableArgs& a, const double* prm, int stride, CableShared& s) {
     const int n = a.n, i = threadIdx.x;
     if (i < n) {
         const double ms = a.am * a.cm / a.dt;
@@ -113,7 +113,7 @@ __device__ __forceinline__ double tri(const double* d, const double* o, const do
 // solution.  b_norm: measure the tolerance against ||B b|| (nonzero initial
 // guess) instead of the initial residual.  Returns the iteration count, or -1
 // when maxit was reached.
-__device__ int cable_cg(const CableArgs& a, CableShared& s, double bi, bool b_norm) {
+static __device__ int cable_cg(const CableArgs& a, CableShared& s, double bi, bool b_norm) {
     const int n = a.n, i = threadIdx.x;
     const bool on = i < n;
     __syncthreads();

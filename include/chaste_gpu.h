@@ -294,6 +294,45 @@ int cg_cable_backward(cg_cable* c, int n_sets, const double* d_params, const dou
                       void* stream);
 int cg_cable_destroy(cg_cable* c);
 
+/* ---------------------------------------------- mixed run populations --
+ * Single-cell runs and cable runs of ONE cell model, each with its own length,
+ * time step, parameters and stimulus, run together in ONE persistent launch
+ * replayed from a CUDA graph: blocks draw jobs -- a group of single cells of about
+ * one length, or one whole cable -- from a queue ordered by decreasing estimated
+ * cost.  FP64.  A single-cell run is AbstractCardiacCell::Compute(0, t_end, tsamp)
+ * with forward Euler (AbstractOneStepIvpOdeSolver::Solve,
+ * ode/src/solver/AbstractOneStepIvpOdeSolver.cpp:41-91) or Rush-Larsen
+ * (AbstractRushLarsenCardiacCell::Compute, heart/src/odes/AbstractRushLarsenCardiacCell.cpp:57-104),
+ * Cm = 1; a cable run takes the cg_cable forward step.  Host pointers throughout. */
+typedef struct cg_runs cg_runs;
+int cg_runs_create(int model, int device, cg_runs** out);
+/* A single-cell run of n_steps steps of dt (method CG_ODE_FORWARD_EULER or
+ * CG_ODE_RUSH_LARSEN) sampled every sample_every steps (tsamp = sample_every * dt;
+ * n_steps a multiple of sample_every).  params: cg_num_params(model) scale factors
+ * (NULL: all 1); stim may be NULL.  *id receives the run's id. */
+int cg_runs_add_cell(cg_runs* r, int method, const double* params, const cg_stimulus* stim, double dt, int n_steps,
+                     int sample_every, int* id);
+/* A cable run: cfg as for cg_cable_create (cfg->model must be the population's;
+ * checkpoint_every is ignored), params n_regions x (n_params + 1), V at the probes
+ * recorded after every sample_every-th step (cfg->n_steps a multiple of it). */
+int cg_runs_add_cable(cg_runs* r, const cg_cable_config* cfg, const double* params, const int* probes, int n_probes,
+                      int sample_every, int* id);
+/* Times each launch shape -- threads per block (64, 128, 256) x single cells per
+ * thread (1, 2); a cable's nodes are spread over the block's threads -- on the first
+ * `steps` steps of every run and keeps the fastest.  Results do not depend on it
+ * beyond the order of the cables' block sums. */
+int cg_runs_autotune(cg_runs* r, int steps, int* threads_per_block, int* cells_per_thread);
+int cg_runs_set_shape(cg_runs* r, int threads_per_block, int cells_per_thread);
+int cg_runs_shape(const cg_runs* r, int* threads_per_block, int* cells_per_thread);
+/* Runs every run from its initial state; ms = device time of the launch. */
+int cg_runs_run(cg_runs* r, double* ms);
+/* Results of run `id` after cg_runs_run.  Cell: states (n_states), trace
+ * (n_samples = n_steps / sample_every + 1 voltages, the first at t = 0).  Cable:
+ * states (n_nodes x n_states), trace (n_samples = n_steps / sample_every rows of
+ * n_probes voltages), cg_iterations (summed over its steps).  Any pointer may be NULL. */
+int cg_runs_result(cg_runs* r, int id, double* states, double* trace, int* n_samples, long long* cg_iterations);
+int cg_runs_destroy(cg_runs* r);
+
 /* Self-test of the device-side failure path, no counterpart in the reference:
  * launches a small kernel whose blocks wait, through the same bounded wait the
  * CG kernels' grid reductions use, for an arrival that never comes.  The wait
