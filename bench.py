@@ -491,21 +491,22 @@ def run_mixed(args):
 
         from tests import cable_cases as CC
 
-        # a bounded sample: 8 cells for one beat each and the first 2000 steps of 2 cables
+        # a bounded sample (about 10 s on one core): 150 cells for one beat each and the
+        # first 10,000 steps of 4 cables
         t0 = time.perf_counter()
         n_cell = 0
-        for steps, p in cells[:8]:
+        for steps, p in cells[:150]:
             y = O.initial_states(O.LR91)
             O.cell_compute(O.LR91, O.RL, y, 0.0, 500.0, 0.01, 1.0, O.regular(-25.5, 2.0, 500.0, 5.0), params=p)
             n_cell += 50000
         n_cab = 0
-        for cfg, p, pr in cables[:2]:
-            cc = CC.PlainCableConfig(n_nodes=cfg.n_nodes, n_steps=2000, n_regions=cfg.n_regions)
+        for cfg, p, pr in cables[:4]:
+            cc = CC.PlainCableConfig(n_nodes=cfg.n_nodes, n_steps=10000, n_regions=cfg.n_regions)
             O.cable_run(CC.oracle_config(O, cc), p, pr, traces=True)
-            n_cab += cfg.n_nodes * 2000
+            n_cab += cfg.n_nodes * 10000
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": (n_cell + n_cab) / dt, "unit": "node-steps/s", "cores": 1, "kind": "port",
-                                "sample": f"8 cells x 1 beat and 2 cables x 2000 steps of the population, {dt:.1f} s"}
+                                "sample": f"150 cells x 1 beat and 4 cables x 10,000 steps of the population, {dt:.1f} s"}
     return line
 
 

@@ -89,7 +89,7 @@ __device__ __forceinline__ double dinv_of(const CgArgs& a, const SlabShared<doub
 // y_i = (A x)_i or (M x)_i for the row of node i (class c)
 template <bool SLAB, int NOFF, bool MASS, typename X>
 __device__ __forceinline__ double apply_row(const CgArgs& a, const SlabShared<double>& sh, const int* soff,
-                                            int c, int i, const X* __restrict__ x) {
+                                            int c, int i, const X* x) {
     if constexpr (!SLAB) {
         return csr_row<double, double>(a.csr.rowptr, a.csr.cols, MASS ? a.csr.m : a.csr.a, i, x);
     } else if constexpr (NOFF > 0) {
@@ -202,16 +202,35 @@ __device__ __forceinline__ void cg_fp64_kernel_body(const CgArgs& a, unsigned& r
         const double alpha = beta / dpi;
         // ---- phase B: x += alpha p ; r -= alpha A p ; z = B r ; z.z, z.r
         {
+            // two grid-stride steps per loop trip, every load before the first store
+            // (the nodes and the order of the sums are the plain loop's)
             double v[2] = {0, 0};
-            for (int i = t0; i < n; i += stride) {
-                const int c = class_of<SLAB>(a, i);
-                x[i] += alpha * p[i];
-                const double rr = r[i] - alpha * q[i];
-                r[i] = rr;
-                const double zz = dinv_of<SLAB>(a, sh, c, i) * rr;
-                zp[i] = zz;
-                v[0] += zz * zz;
-                v[1] += zz * rr;
+            for (int i0 = t0; i0 < n; i0 += 2 * stride) {
+                double xo[2], po[2], ro[2], qo[2], dv[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int i = i0 + u * stride;
+                    xo[u] = po[u] = ro[u] = qo[u] = dv[u] = 0.0;
+                    if (i < n) {
+                        dv[u] = dinv_of<SLAB>(a, sh, class_of<SLAB>(a, i), i);
+                        xo[u] = x[i];
+                        po[u] = p[i];
+                        ro[u] = r[i];
+                        qo[u] = q[i];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int i = i0 + u * stride;
+                    if (i >= n) continue;
+                    x[i] = xo[u] + alpha * po[u];
+                    const double rr = ro[u] - alpha * qo[u];
+                    r[i] = rr;
+                    const double zz = dv[u] * rr;
+                    zp[i] = zz;
+                    v[0] += zz * zz;
+                    v[1] += zz * rr;
+                }
             }
             if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }

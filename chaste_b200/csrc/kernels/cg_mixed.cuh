@@ -39,7 +39,7 @@ __device__ __forceinline__ float dinv32_of(const CgArgs& a, const SlabShared<flo
 
 template <bool SLAB, int NOFF>
 __device__ __forceinline__ float apply_row32(const CgArgs& a, const SlabShared<float>& s32, const int* soff,
-                                             int c, int i, const float* __restrict__ x) {
+                                             int c, int i, const float* x) {
     if constexpr (!SLAB) {
         return csr_row<float, float>(a.csr.rowptr, a.csr.cols, a.csr.a32, i, x);
     } else if constexpr (NOFF > 0) {
@@ -158,6 +158,35 @@ __device__ __forceinline__ float inner_pc32(const CgArgs& a, const SlabShared<fl
     return on ? dinv32_of<SLAB>(a, s32, c, i) * r : 0.0f;
 }
 
+// The same in two parts, so a loop can load the x-line factors together with its
+// other operands: inner_pc_factors (a load, or the identity when there is no line
+// solve), then inner_pc32_with.
+template <bool SLAB>
+__device__ __forceinline__ float2 inner_pc_factors(const CgArgs& a, bool on, int i) {
+    if constexpr (SLAB) {
+        if (a.line_pc) return line_factors(a, on, i);
+    }
+    return make_float2(0.0f, 1.0f);
+}
+
+template <bool SLAB>
+__device__ __forceinline__ float inner_pc32_with(const CgArgs& a, const SlabShared<float>& s32, int c, int i,
+                                                 bool on, float r, float2 ad) {
+    if constexpr (SLAB) {
+        if (a.line_pc) {
+            float A[5];
+            warp_line_levels(ad.x, A);
+            return warp_line_solve(A, ad.y, on ? r : 0.0f);
+        }
+    }
+    return on ? dinv32_of<SLAB>(a, s32, c, i) * r : 0.0f;
+}
+
+// Grid-stride steps of the HBM-resident inner loops taken per loop trip (loads of all
+// of them issued before the first store).
+constexpr int kInnerUnroll = 2;
+constexpr int kStencilUnroll = 1;
+
 template <bool SLAB, int NOFF>
 __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& round) {
     __shared__ SlabShared<double> sh;
@@ -247,17 +276,36 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
             const float bc = it == 0 ? 0.0f : (float)(beta / betaold);
             const bool first = it == 0;
             {
+                // kInnerUnroll grid-stride steps per loop trip: every load of the group
+                // is issued before any store, so their latencies overlap (the nodes and
+                // the order of the sums are those of the plain grid-stride loop)
                 double v[1] = {0};
-                for (int base = w0; base < n; base += stride) {
-                    const int i = base + lane;
-                    if (i >= n) continue;
-                    const int c = class_of<SLAB>(a, i);
-                    const float az = apply_row32<SLAB, NOFF>(a, s32, soff, c, i, z32);
-                    const float qi = first ? az : az + bc * q32[i];
-                    const float pi = first ? z32[i] : z32[i] + bc * p32[i];
-                    q32[i] = qi;
-                    p32[i] = pi;
-                    v[0] += (double)pi * (double)qi;
+                for (int base = w0; base < n; base += kStencilUnroll * stride) {
+                    float az[kStencilUnroll], zo[kStencilUnroll], qo[kStencilUnroll], po[kStencilUnroll];
+#pragma unroll
+                    for (int u = 0; u < kStencilUnroll; ++u) {
+                        const int i = base + u * stride + lane;
+                        az[u] = zo[u] = qo[u] = po[u] = 0.0f;
+                        if (i < n) {
+                            const int c = class_of<SLAB>(a, i);
+                            az[u] = apply_row32<SLAB, NOFF>(a, s32, soff, c, i, z32);
+                            zo[u] = z32[i];
+                            if (!first) {
+                                qo[u] = q32[i];
+                                po[u] = p32[i];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kStencilUnroll; ++u) {
+                        const int i = base + u * stride + lane;
+                        if (i >= n) continue;
+                        const float qi = first ? az[u] : az[u] + bc * qo[u];
+                        const float pi = first ? zo[u] : zo[u] + bc * po[u];
+                        q32[i] = qi;
+                        p32[i] = pi;
+                        v[0] += (double)pi * (double)qi;
+                    }
                 }
                 if (!grid_reduce<1>(v, red, a.gs, a.partials, res, a.status, round)) return;
             }
@@ -266,20 +314,39 @@ __device__ __forceinline__ void cg_mixed_kernel_body(const CgArgs& a, unsigned& 
             const float alpha = (float)(beta / dpi);
             {
                 double v[2] = {0, 0};
-                for (int base = w0; base < n; base += stride) {
-                    const int i = base + lane;
-                    const bool on = i < n;
-                    const int c = on ? class_of<SLAB>(a, i) : 0;
-                    float rr = 0.0f;
-                    if (on) {
-                        e32[i] = first ? alpha * p32[i] : e32[i] + alpha * p32[i];
-                        rr = r32[i] - alpha * q32[i];
-                        r32[i] = rr;
+                for (int base = w0; base < n; base += kInnerUnroll * stride) {
+                    float pv[kInnerUnroll], qv[kInnerUnroll], rv[kInnerUnroll], eo[kInnerUnroll];
+                    int cl[kInnerUnroll];
+                    float2 ad[kInnerUnroll];
+#pragma unroll
+                    for (int u = 0; u < kInnerUnroll; ++u) {
+                        const int i = base + u * stride + lane;
+                        const bool on = i < n;
+                        pv[u] = qv[u] = rv[u] = eo[u] = 0.0f;
+                        cl[u] = on ? class_of<SLAB>(a, i) : 0;
+                        ad[u] = inner_pc_factors<SLAB>(a, on, i);
+                        if (on) {
+                            pv[u] = p32[i];
+                            qv[u] = q32[i];
+                            rv[u] = r32[i];
+                            if (!first) eo[u] = e32[i];
+                        }
                     }
-                    const float zz = inner_pc32<SLAB>(a, s32, c, i, on, rr);
-                    if (on) z32[i] = zz;
-                    v[0] += (double)zz * (double)zz;
-                    v[1] += (double)zz * (double)rr;
+#pragma unroll
+                    for (int u = 0; u < kInnerUnroll; ++u) {
+                        const int i = base + u * stride + lane;
+                        const bool on = i < n;
+                        float rr = 0.0f;
+                        if (on) {
+                            e32[i] = first ? alpha * pv[u] : eo[u] + alpha * pv[u];
+                            rr = rv[u] - alpha * qv[u];
+                            r32[i] = rr;
+                        }
+                        const float zz = inner_pc32_with<SLAB>(a, s32, cl[u], i, on, rr, ad[u]);
+                        if (on) z32[i] = zz;
+                        v[0] += (double)zz * (double)zz;
+                        v[1] += (double)zz * (double)rr;
+                    }
                 }
                 if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
             }

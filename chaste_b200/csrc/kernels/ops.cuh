@@ -64,9 +64,13 @@ __device__ void slab_load_shared(const SlabOp& op, SlabShared<T>& sh, int diag_s
 }
 
 // sum_o coef[o] * x[i + off[o]]; NOFF > 0 unrolls a fixed offset count, 0 loops n_off.
+// x is not declared __restrict__: the persistent solves apply the operator to vectors
+// that other blocks of the same launch write between grid reductions, so its loads must
+// be ordinary coherent loads (ordered by the reductions' acquire), never the read-only
+// path a restrict-qualified const pointer allows the compiler to choose.
 template <int NOFF, typename T, typename Acc, typename X>
 __device__ __forceinline__ Acc slab_row(const T* coef, const int* __restrict__ off, int n_off, int i,
-                                        const X* __restrict__ x) {
+                                        const X* x) {
     Acc acc = Acc(0);
     if constexpr (NOFF > 0) {
 #pragma unroll
@@ -90,7 +94,7 @@ struct CsrOp {
 
 template <typename T, typename Acc, typename X>
 __device__ __forceinline__ Acc csr_row(const int* __restrict__ rp, const int* __restrict__ ci,
-                                       const T* __restrict__ v, int i, const X* __restrict__ x) {
+                                       const T* __restrict__ v, int i, const X* x) {
     Acc acc = Acc(0);
     const int e = rp[i + 1];
     for (int k = rp[i]; k < e; ++k) acc += (Acc)v[k] * (Acc)x[ci[k]];

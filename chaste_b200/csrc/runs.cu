@@ -97,15 +97,21 @@ double cable_cost(const RunCable& c, int tpb) {
     return (double)c.n_steps * (12.0 + npt);
 }
 
-// Jobs (cells grouped by length, cables one each), longest first.
-void make_jobs(const cg_runs* r, std::vector<RunJob>& jobs, std::vector<int>& order) {
+// Jobs (cells grouped by length, cables one each), longest first.  A run's steps
+// are one dependent chain, so the population ends no sooner than its longest run:
+// groups are cut small enough (down to one warp) that the cells spread over every
+// block the GPU holds instead of crowding the threads of a few SMs.
+void make_jobs(const cg_runs* r, int blocks_available, std::vector<RunJob>& jobs, std::vector<int>& order) {
     const int n_cells = (int)r->cells.size();
     order.resize(n_cells);
     for (int i = 0; i < n_cells; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(),
                      [&](int x, int y) { return r->cells[x].n_steps > r->cells[y].n_steps; });
     std::vector<std::pair<double, RunJob>> cost;
-    const int group = r->tpb * r->cpt;
+    const int n_cables = (int)r->cables.size();
+    const int for_cells = std::max(blocks_available - n_cables, std::max(1, blocks_available / 2));
+    const int spread = (n_cells + for_cells - 1) / for_cells;
+    const int group = std::min(r->tpb * r->cpt, std::max(32, (spread + 31) / 32 * 32));
     for (int f = 0; f < n_cells; f += group) {
         RunJob j{0, f, std::min(group, n_cells - f), 0};
         cost.push_back({(double)r->cells[order[f]].n_steps * r->cpt, j});
@@ -116,13 +122,11 @@ void make_jobs(const cg_runs* r, std::vector<RunJob>& jobs, std::vector<int>& or
     for (auto& c : cost) jobs.push_back(c.second);
 }
 
-int configure(cg_runs* r) {
+// Shared memory of the launch shape and the blocks that fit on the GPU at once.
+int configure(cg_runs* r, int smem_nodes, int* resident) {
     const void* k = kernel_for(r->model, r->cpt);
-    r->smem = r->max_cable_nodes > 0
-                  ? ((size_t)kRunsCableArrays * r->args.smem_nodes + 3 * 32) * sizeof(double)
-                  : 0;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smem) !=
-        cudaSuccess) {
+    r->smem = r->max_cable_nodes > 0 ? ((size_t)kRunsCableArrays * smem_nodes + 3 * 32) * sizeof(double) : 0;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smem) != cudaSuccess) {
         cudaGetLastError();
         return CG_ERR_CUDA;
     }
@@ -132,7 +136,7 @@ int configure(cg_runs* r) {
         cudaGetLastError();
         return CG_ERR_UNSUPPORTED;
     }
-    r->blocks = (int)std::max(1LL, std::min((long long)r->args.n_jobs, (long long)per_sm * sms));
+    *resident = per_sm * sms;
     return CG_OK;
 }
 
@@ -145,13 +149,18 @@ int prepare(cg_runs* r) {
     r->y0_cells.resize((size_t)r->S * n_cells);
     for (int k = 0; k < r->S; ++k)
         for (size_t i = 0; i < n_cells; ++i) r->y0_cells[k * n_cells + i] = init[k];
+    const int smem_nodes = (r->max_cable_nodes + 31) / 32 * 32;
+    int resident = 1;
+    int rc = configure(r, smem_nodes, &resident);
+    if (rc != CG_OK) return rc;
     std::vector<RunJob> jobs;
     std::vector<int> order;
-    make_jobs(r, jobs, order);
+    make_jobs(r, resident, jobs, order);
+    r->blocks = (int)std::max(1LL, std::min((long long)jobs.size(), (long long)resident));
     RunsArgs a;
     std::memset(&a, 0, sizeof(a));
     a.n_jobs = (int)jobs.size();
-    a.smem_nodes = (r->max_cable_nodes + 31) / 32 * 32;
+    a.smem_nodes = smem_nodes;
     a.n_cells = (int)r->cells.size();
     RunJob* d_jobs = nullptr;
     RunCell* d_cells = nullptr;
@@ -176,11 +185,6 @@ int prepare(cg_runs* r) {
     a.cable_params = d_kp;
     a.probes = d_probes;
     r->args = a;
-    const int rc = configure(r);
-    if (rc != CG_OK) {
-        r->release();
-        return rc;
-    }
     r->dirty = false;
     return CG_OK;
 }
