@@ -94,6 +94,7 @@ SIGNATURES = {
     "cg_set_cells": (C.c_int, [_vp, _dp, _ip, _dp, C.c_int]),
     "cg_set_stimulus": (C.c_int, [_vp, _ip, C.POINTER(Stimulus), C.c_int]),
     "cg_step": (C.c_int, [_vp, C.c_int]),
+    "cg_step_host": (C.c_int, [_vp, _dp, C.c_int, _dp, C.c_int]),
     "cg_step_profiled": (C.c_int, [_vp, C.c_int, _dp, _dp]),
     "cg_get_voltage": (C.c_int, [_vp, _dp]),
     "cg_set_voltage": (C.c_int, [_vp, _dp]),
@@ -258,6 +259,17 @@ class Tissue:
     # -- stepping
     def step(self, n=1):
         check(lib().cg_step(self.h, int(n)), "cg_step")
+
+    def step_host(self, v_in, n=1, v_out=None, keep_history=True):
+        """n steps from the host voltage v_in (None: the device's), V after them into
+        v_out (None: not read back); one synchronisation (cg_step_host)."""
+        vi = None if v_in is None else np.ascontiguousarray(v_in, dtype=np.float64)
+        if vi is not None and vi.size != self.n:
+            raise ValueError("v_in must hold one value per node")
+        if v_out is not None and (v_out.dtype != np.float64 or not v_out.flags.c_contiguous or v_out.size != self.n):
+            raise ValueError("v_out must be a contiguous float64 array of one value per node")
+        check(lib().cg_step_host(self.h, dptr(vi), int(n), dptr(v_out), 1 if keep_history else 0), "cg_step_host")
+        return v_out
 
     def step_profiled(self, n=1):
         """Returns (ms in the ODE kernel, ms in the RHS+CG kernel) over n steps."""

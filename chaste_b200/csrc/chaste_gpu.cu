@@ -25,6 +25,16 @@ using namespace chb;
 namespace {
 
 constexpr int kRing = 4096;   // iteration-count history per context
+constexpr int kHostChunks = 8;   // cg_step_host: pieces of V copied in while the ODE runs on the earlier ones
+
+// Status word, step counter and iteration ring read back after each call, copied
+// together into page-locked memory so one synchronisation covers them.
+struct HostControl {
+    int status;
+    int pad;
+    long long step;
+    int ring[kRing];
+};
 // bjacobi solves of meshes up to this size run as one block (block barriers between
 // the levels of the triangular solves); larger ones on the co-resident grid
 constexpr int kIluOneBlockNodes = 65536;
@@ -126,6 +136,10 @@ struct cg_ctx {
     int max_iters = 0;
     double ms_last = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // cg_step_host: a copy stream, one event per chunk of V, and page-locked control words
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t chunk_ev[kHostChunks] = {};
+    HostControl* h_ctl = nullptr;
 
     bool mixed() const { return cfg.precision == CG_PRECISION_MIXED; }
     size_t real_size() const { return mixed() ? sizeof(float) : sizeof(double); }
@@ -330,6 +344,10 @@ int cg_destroy(cg_ctx* c) {
     c->mem.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (cudaEvent_t e : c->chunk_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CG_OK;
@@ -925,9 +943,13 @@ int upload_cells_t(cg_ctx* c, const double* init, const int* pset, const double*
 }
 
 template <class M, typename T>
-void launch_ode(cg_ctx* c, int half = 0) {
+void launch_ode(cg_ctx* c, int half = 0, int lo = 0, int hi = -1, bool reset_history = false) {
     OdeArgs<T> a;
     a.n = c->n;
+    a.lo = lo;
+    a.hi = hi < 0 ? c->n : hi;
+    a.reset_history = reset_history ? 1 : 0;
+    const int blocks = (int)std::max(1LL, std::min((long long)c->ode_blocks, ((long long)a.hi - a.lo + 255) / 256));
     a.V = c->d_V;
     // the extrapolated guess replaces V^n in place, which splitting and SVI still need
     a.vprev = (c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING || c->svi) ? nullptr : c->d_Vprev;
@@ -949,15 +971,15 @@ void launch_ode(cg_ctx* c, int half = 0) {
     a.act = c->d_act;
     a.act_threshold = c->cfg.activation_threshold;
     if (c->cfg.ode_method == CG_ODE_RUSH_LARSEN)
-        ode_kernel<M, T, 1><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+        ode_kernel<M, T, 1><<<blocks, 256, 0, c->stream>>>(a);
     else if (c->cfg.ode_method == CG_ODE_BACKWARD_EULER)
-        ode_kernel<M, T, 2><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+        ode_kernel<M, T, 2><<<blocks, 256, 0, c->stream>>>(a);
     else if (c->cfg.ode_method == CG_ODE_GRL1)
-        ode_kernel<M, T, 3><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+        ode_kernel<M, T, 3><<<blocks, 256, 0, c->stream>>>(a);
     else if (c->cfg.ode_method == CG_ODE_GRL2)
-        ode_kernel<M, T, 4><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+        ode_kernel<M, T, 4><<<blocks, 256, 0, c->stream>>>(a);
     else
-        ode_kernel<M, T, 0><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+        ode_kernel<M, T, 0><<<blocks, 256, 0, c->stream>>>(a);
 }
 
 CgArgs make_cg_args(cg_ctx* c) {
@@ -1055,15 +1077,16 @@ cudaError_t launch_cg(cg_ctx* c) {
 }
 
 // The ODE launch of a step: the whole step with V clamped (half 0), or one half of
-// the operator-splitting step including V (half 1, 2).
-void launch_odes(cg_ctx* c, int half) {
+// the operator-splitting step including V (half 1, 2); half 0 may cover the nodes
+// [lo, hi) only.
+void launch_odes(cg_ctx* c, int half, int lo = 0, int hi = -1, bool reset_history = false) {
     const bool tt = c->cfg.model == CG_MODEL_TT06;
     if (c->mixed()) {
-        if (tt) launch_ode<TenTusscher2006Epi, float>(c, half);
-        else launch_ode<LuoRudy1991, float>(c, half);
+        if (tt) launch_ode<TenTusscher2006Epi, float>(c, half, lo, hi, reset_history);
+        else launch_ode<LuoRudy1991, float>(c, half, lo, hi, reset_history);
     } else {
-        if (tt) launch_ode<TenTusscher2006Epi, double>(c, half);
-        else launch_ode<LuoRudy1991, double>(c, half);
+        if (tt) launch_ode<TenTusscher2006Epi, double>(c, half, lo, hi, reset_history);
+        else launch_ode<LuoRudy1991, double>(c, half, lo, hi, reset_history);
     }
 }
 
@@ -1160,6 +1183,26 @@ cudaError_t launch_step(cg_ctx* c) {
     return cudaGetLastError();
 }
 
+// The copy stream, chunk events and page-locked control words, made on first use.
+int ensure_host_path(cg_ctx* c) {
+    if (c->h_ctl) return CG_OK;
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return CG_ERR_CUDA;
+    }
+    for (cudaEvent_t& e : c->chunk_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return CG_ERR_CUDA;
+        }
+    if (cudaMallocHost(&c->h_ctl, sizeof(HostControl)) != cudaSuccess) {
+        cudaGetLastError();
+        c->h_ctl = nullptr;
+        return CG_ERR_NOMEM;
+    }
+    return CG_OK;
+}
+
 int build_graph(cg_ctx* c) {
     if (c->graph) {
         cudaGraphExecDestroy(c->graph);
@@ -1235,18 +1278,49 @@ int cg_set_stimulus(cg_ctx* c, const int* stim_id, const cg_stimulus* stims, int
     return CG_OK;
 }
 
-int cg_step(cg_ctx* c, int n_steps) {
+int cg_step(cg_ctx* c, int n_steps) { return cg_step_host(c, nullptr, n_steps, nullptr, 1); }
+
+int cg_step_host(cg_ctx* c, const double* v_in, int n_steps, double* v_out, int keep_history) {
     if (!c || n_steps < 0) return CG_ERR_ARG;
     if (!c->have_mesh || !c->have_cells) return CG_ERR_ORDER;
-    if (n_steps == 0) return CG_OK;
+    if (n_steps == 0 && !v_in && !v_out) return CG_OK;
     CG_CUDA(cudaSetDevice(c->device));
     if (c->graph_dirty) {
         if (build_graph(c) != CG_OK) c->graph = nullptr;   // plain launches instead
         c->graph_dirty = false;
     }
     if (c->out_max && c->out_count + out_frames_added(c, n_steps) > c->out_max) return CG_ERR_NOMEM;
+    CG_TRY(ensure_host_path(c));
+    const size_t n = (size_t)c->n;
     CG_CUDA(cudaEventRecord(c->ev0, c->stream));
-    for (int k = 0; k < n_steps; ++k) {
+    int k0 = 0;
+    if (v_in) {
+        if (n_steps > 0 && !split(c) && !c->svi) {
+            // the first step's ODE runs on each piece of V as soon as it has arrived
+            CG_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev0, 0));
+            const int per = (int)((n + kHostChunks - 1) / kHostChunks);
+            for (int k = 0; k < kHostChunks; ++k) {
+                const int lo = k * per, hi = (int)std::min(n, (size_t)lo + per);
+                if (lo >= hi) break;
+                CG_CUDA(cudaMemcpyAsync(c->d_V + lo, v_in + lo, (size_t)(hi - lo) * sizeof(double),
+                                        cudaMemcpyHostToDevice, c->copy_stream));
+                CG_CUDA(cudaEventRecord(c->chunk_ev[k], c->copy_stream));
+                CG_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[k], 0));
+                launch_odes(c, 0, lo, hi, keep_history == 0);
+            }
+            if (cudaGetLastError() != cudaSuccess || launch_cg(c) != cudaSuccess) {
+                cudaGetLastError();
+                return CG_ERR_CUDA;
+            }
+            out_after_step(c, c->steps + 1);
+            k0 = 1;
+        } else {
+            CG_CUDA(cudaMemcpyAsync(c->d_V, v_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            if (!keep_history && c->d_Vprev)
+                CG_CUDA(cudaMemcpyAsync(c->d_Vprev, c->d_V, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        }
+    }
+    for (int k = k0; k < n_steps; ++k) {
         const cudaError_t e = c->graph ? cudaGraphLaunch(c->graph, c->stream) : launch_step(c);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -1255,26 +1329,24 @@ int cg_step(cg_ctx* c, int n_steps) {
         out_after_step(c, c->steps + k + 1);
     }
     CG_CUDA(cudaEventRecord(c->ev1, c->stream));
+    if (v_out) CG_CUDA(cudaMemcpyAsync(v_out, c->d_V, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HostControl* h = c->h_ctl;
+    CG_CUDA(cudaMemcpyAsync(&h->status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CG_CUDA(cudaMemcpyAsync(&h->step, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    CG_CUDA(cudaMemcpyAsync(h->ring, c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CG_CUDA(cudaStreamSynchronize(c->stream));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->ms_last = ms;
-    int bits = 0;
-    long long dstep = 0;
-    CG_CUDA(cudaMemcpy(&bits, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    CG_CUDA(cudaMemcpy(&dstep, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost));
+    const long long dstep = h->step;
     const long long from = std::max(c->steps, dstep - kRing);
-    if (dstep > from) {
-        std::vector<int> ring(kRing);
-        CG_CUDA(cudaMemcpy(ring.data(), c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost));
-        for (long long s = from; s < dstep; ++s) {
-            const int it = ring[s % kRing];
-            c->total_iters += it;
-            c->max_iters = std::max(c->max_iters, it);
-        }
+    for (long long s = from; s < dstep; ++s) {
+        const int it = h->ring[s % kRing];
+        c->total_iters += it;
+        c->max_iters = std::max(c->max_iters, it);
     }
     c->steps = dstep;
-    return status_from_bits(bits);
+    return status_from_bits(h->status);
 }
 
 }  // extern "C"

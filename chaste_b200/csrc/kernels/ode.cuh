@@ -34,6 +34,8 @@ struct OdeArgs {
     double act_threshold;
     int half;                           // 0: ComputeExceptVoltage over the step; 1, 2: first or second
                                         // half step including V (operator splitting)
+    int lo, hi;                         // half 0: the nodes [lo, hi) of this launch
+    int reset_history;                  // with vprev: V^n has no predecessor (guess V^n, no extrapolation)
 };
 
 // First step with V above the threshold (ActivationOutputModifier::ProcessSolutionAtTimeStep,
@@ -114,14 +116,14 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
         return;
     }
     const double dtinv = 1.0 / a.dt_pde;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int i = a.lo + blockIdx.x * blockDim.x + threadIdx.x; i < a.hi; i += gridDim.x * blockDim.x) {
         T y[S];
         const double v = a.V[i];
         // mixed precision: the diffusion solve starts from the linear extrapolation
         // 2 V^n - V^{n-1} (FP64 mode keeps Chaste's guess V^n, LinearSystem.cpp:833-837);
         // the right-hand side below still uses V^n
         if (a.vprev) {
-            const double vp = a.vprev[i];
+            const double vp = a.reset_history ? v : a.vprev[i];
             a.vprev[i] = v;
             a.V[i] = 2.0 * v - vp;
         }

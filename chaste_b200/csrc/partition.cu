@@ -422,6 +422,8 @@ int cg_part_ode(cg_part* c) {
     OdeArgs<double> a;
     std::memset(&a, 0, sizeof(a));
     a.n = c->nloc;
+    a.lo = 0;
+    a.hi = c->nloc;
     a.V = c->x + c->halo;
     a.vprev = nullptr;
     a.half = 0;

@@ -14,7 +14,7 @@
  *
  *   InitialiseForSolve(V0)          -- the device tissue receives V0; the linear system
  *                                      is set to the identity once
- *   PrepareForSetupLinearSystem(V)  -- cg_step(ctx, 1): the cells' ODEs, b = M z and the
+ *   PrepareForSetupLinearSystem(V)  -- cg_step_host(ctx, NULL, 1, V_host, 1): the cells' ODEs, b = M z and the
  *                                      CG solve, on the device (MonodomainSolver's
  *                                      SolveCellSystems + SetupLinearSystem + KSPSolve)
  *   SetupLinearSystem(V, ...)       -- the right-hand side becomes the device solution,
@@ -514,18 +514,18 @@ public:
         }
     }
 
-    /* The whole monodomain step on the device: ODEs, b = M z, CG. */
+    /* The whole monodomain step on the device (ODEs, b = M z, CG) and the new V copied
+     * back, one call and one synchronisation. */
     void PrepareForSetupLinearSystem(Vec currentSolution)
     {
-        chaste_gpu_shim::Check(cg_step(mpTissue->GetContext(), 1), "cg_step");
+        mHostV.resize(this->mpMesh->GetNumNodes());
+        chaste_gpu_shim::Check(cg_step_host(mpTissue->GetContext(), nullptr, 1, mHostV.data(), 1), "cg_step_host");
     }
 
     /* b = the device solution; the identity system returns it as the next solution. */
     void SetupLinearSystem(Vec currentSolution, bool computeMatrix)
     {
         using namespace chaste_gpu_shim;
-        mHostV.resize(this->mpMesh->GetNumNodes());
-        Check(cg_get_voltage(mpTissue->GetContext(), mHostV.data()), "cg_get_voltage");
         PetscInt lo, hi;
         this->mpLinearSystem->GetOwnershipRange(lo, hi);
         for (PetscInt i = lo; i < hi; ++i)

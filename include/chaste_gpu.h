@@ -158,6 +158,17 @@ int cg_set_stimulus(cg_ctx* ctx, const int* stim_id, const cg_stimulus* stims, i
 
 /* Advance n PDE steps (ODE -> RHS -> CG each), launched as a CUDA graph. */
 int cg_step(cg_ctx* ctx, int n_steps);
+/* The same with the voltage in host memory, for a caller that keeps V on the host
+ * between steps (AbstractDynamicLinearPdeSolver::Solve hands the solution Vec back
+ * every step, pde/src/solver/AbstractDynamicLinearPdeSolver.hpp:233-272): v_in
+ * (n_nodes, may be NULL) is copied in before the first step -- in pieces, the first
+ * step's ODE starting on each piece as it arrives -- and V after the last step is
+ * copied to v_out (may be NULL), with one synchronisation for the whole call.
+ * keep_history = 1 declares that v_in continues the trajectory (the caller passes
+ * back what the previous call returned), so the mixed solve keeps its extrapolated
+ * initial guess; 0 treats v_in as new (as cg_set_voltage does).  Page-locked host
+ * buffers make the copies DMA transfers. */
+int cg_step_host(cg_ctx* ctx, const double* v_in, int n_steps, double* v_out, int keep_history);
 
 /* cg_step with device-side event timing per phase, launched kernel by kernel
  * (no graph): ms_solve_odes accumulates the ODE kernel (HeartEventHandler

@@ -433,3 +433,37 @@ def test_monodomain_problem_api_on_gpu(N, kats):
     cell = p.GetTissue().GetCardiacCell(3)
     assert abs(cell.GetVoltage() - v[3]) == 0.0
     hc.Reset()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_host_buffer_steps_match_device_steps(N, precision):
+    """cg_step_host (V copied in piece by piece under the first step's ODE, V copied
+    out, one synchronisation) reproduces the device-resident steps bit for bit when
+    the caller passes back what it got (keep_history), and set_voltage + step when it
+    declares the voltage new (no history: the mixed solve's guess is V itself)."""
+    case = dict(TC.TT06_3D)
+    dev, _ = TC.make_gpu(N, precision=precision, **case)
+    host, _ = TC.make_gpu(N, precision=precision, **case)
+    dev.step(5)
+    host.step(5)
+    v = host.voltage()
+    out = np.empty_like(v)
+    for _ in range(15):
+        dev.step(1)
+        host.step_host(v, 1, out, keep_history=True)
+        v, out = out, v
+        assert np.array_equal(v, dev.voltage())
+    assert host.stats().steps == dev.stats().steps == 20
+    # a voltage declared new: the same as cg_set_voltage followed by cg_step (the two
+    # tissues hold bitwise the same states here)
+    w = v.copy()
+    w[::7] += 0.25
+    dev.set_voltage(w)
+    dev.step(3)
+    host.step_host(w, 3, out, keep_history=False)
+    assert np.array_equal(out, dev.voltage())
+    # reading back only, and writing only
+    host.step_host(None, 2, out)
+    assert np.array_equal(out, host.voltage())
+    host.step_host(out, 0, None)
+    assert np.array_equal(out, host.voltage())
