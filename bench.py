@@ -266,7 +266,7 @@ def run_ours(args, rank, world, device):
 # --t-start-ms), `bench.py --profile <precision> --steps 5`, summarised in
 # profiles/cg_kernels_tt06_slab_3d.md.  None where no such capture exists.
 NCU_TRAFFIC = {
-    ("tt06_slab_3d", "mixed", "cg_kernel"): 10.84e6,   # 10.23 MB read + 0.61 MB written, 179 us
+    ("tt06_slab_3d", "mixed", "cg_kernel"): 11.07e6,   # 10.21 MB read + 0.86 MB written, 163 us
 }
 
 
