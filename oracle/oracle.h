@@ -108,6 +108,15 @@ double orc_tissue_time(const orc_tissue* t);
 void orc_tissue_get_voltage(const orc_tissue* t, double* v);
 void orc_tissue_get_states(const orc_tissue* t, double* states /* n_nodes*n_states */);
 void orc_tissue_get_caches(const orc_tissue* t, double* iion, double* istim);
+/* Bidomain without a bath (BidomainProblem, BidomainSolver, BidomainAssembler): the
+ * tissue's unknowns become the interleaved (V, phi_e) pairs of every node.  Call once,
+ * before the first step, with the mesh again and both conductivities (n_elems*dim
+ * each); fixed: nodes whose phi_e is held at 0 (SetFixedExtracellularPotentialNodes),
+ * none for the singular system with the null space of constant phi_e.  Steps are
+ * taken by orc_tissue_step; Jacobi or no preconditioner.  Returns 0 or -4. */
+int orc_tissue_set_bidomain(orc_tissue* t, const double* xyz, int n_elems, const int* conn, const double* sigma_i,
+                            const double* sigma_e, const int* fixed, int n_fixed);
+void orc_tissue_get_extracellular(const orc_tissue* t, double* phi);
 /* CSR of A = Am*Cm/dt*M + K and of M (for tests): returns nnz. */
 int orc_tissue_matrix(const orc_tissue* t, int which /*0 A, 1 M*/, int* rowptr, int* cols, double* vals);
 void orc_set_threads(int n);

@@ -239,6 +239,11 @@ struct Tissue {
     std::vector<double> detj;                 // |det J| per element
     double t = 0.0;
     long long steps = 0;
+    // bidomain (orc_tissue_set_bidomain): the interleaved system of (V, phi_e)
+    bool bido = false;
+    bool nullspace = true;                    // no fixed phi_e: PETSc null space of constant phi_e
+    Csr B;                                    // 2n x 2n, row 2i the V equation, 2i+1 the phi_e one
+    std::vector<double> bdinv, u, bb, br, bz, bp, bw, bmz;
 };
 
 static void ilu0_factor(const Csr& A, std::vector<double>& lu, std::vector<int>& diag) {
@@ -302,15 +307,15 @@ static double dot(int n, const double* a, const double* b) {
 // nonzero initial guess rnorm0 = ||B b||, ttol = max(rtol*rnorm0, abstol);
 // converged when ||B r_k|| <= ttol (checked from iteration 0), diverged when
 // ||B r_k|| >= dtol*rnorm0 (dtol 1e5) or the iteration count reaches max_it.
-static int cg_solve(Tissue& T, double* xv, const double* bv, int* iters) {
-    const int n = T.n;
-    double* R = T.r.data();
-    double* Z = T.z.data();
-    double* P = T.p.data();
-    const double rtol = T.cfg.use_abs_tol ? DBL_EPSILON : T.cfg.tol;
-    const double abstol = T.cfg.use_abs_tol ? T.cfg.tol : 1e-50;
+// `pc` is KSP_PCApply: the preconditioner followed, when the operator has a null
+// space, by its removal from the result.
+template <class Mv, class Pc>
+static int cg_core(const orc_config& cfg, int n, double* xv, const double* bv, double* R, double* Z, double* P,
+                   double* W, Mv matvec, Pc pc, int* iters) {
+    const double rtol = cfg.use_abs_tol ? DBL_EPSILON : cfg.tol;
+    const double abstol = cfg.use_abs_tol ? cfg.tol : 1e-50;
     const double dtol = 1e5;
-    const int maxit = T.cfg.max_iterations > 0 ? T.cfg.max_iterations : 10000;
+    const int maxit = cfg.max_iterations > 0 ? cfg.max_iterations : 10000;
     // LinearSystem::Solve: small nonzero RHS -> zero guess (LinearSystem.cpp:984-994)
     double rhs1 = parallel_sum(n, [&](int i) { return std::fabs(bv[i]); });
     bool guess_zero = false;
@@ -319,16 +324,16 @@ static int cg_solve(Tissue& T, double* xv, const double* bv, int* iters) {
         guess_zero = true;
     }
     // r = b - A x
-    T.A.matvec(xv, R);
+    matvec(xv, R);
     parallel_for(n, [&](int b, int e) {
         for (int i = b; i < e; ++i) R[i] = bv[i] - R[i];
     });
-    pc_apply(T, R, Z);
+    pc(R, Z);
     double dp = std::sqrt(dot(n, Z, Z));
     double rnorm0;
     if (!guess_zero) {
-        pc_apply(T, bv, T.w.data());
-        double snorm = std::sqrt(dot(n, T.w.data(), T.w.data()));
+        pc(bv, W);
+        double snorm = std::sqrt(dot(n, W, W));
         rnorm0 = snorm != 0.0 ? snorm : dp;
     } else {
         rnorm0 = dp;
@@ -351,7 +356,7 @@ static int cg_solve(Tissue& T, double* xv, const double* bv, int* iters) {
                 for (int k = b; k < e; ++k) P[k] = Z[k] + bb * P[k];
             });
         }
-        T.A.matvec(P, Z);                       // Z = A p
+        matvec(P, Z);                           // Z = A p
         const double dpi = dot(n, P, Z);
         if (dpi <= 0.0) return -2;              // indefinite matrix
         const double a = beta / dpi;
@@ -361,7 +366,7 @@ static int cg_solve(Tissue& T, double* xv, const double* bv, int* iters) {
                 R[k] -= a * Z[k];
             }
         });
-        pc_apply(T, R, Z);
+        pc(R, Z);
         dp = std::sqrt(dot(n, Z, Z));
         if (std::isnan(dp) || std::isinf(dp)) return -3;
         if (dp <= ttol) return 0;
@@ -371,6 +376,13 @@ static int cg_solve(Tissue& T, double* xv, const double* bv, int* iters) {
         i++;
     } while (i < maxit);
     return -1;
+}
+
+static int cg_solve(Tissue& T, double* xv, const double* bv, int* iters) {
+    return cg_core(
+        T.cfg, T.n, xv, bv, T.r.data(), T.z.data(), T.p.data(), T.w.data(),
+        [&](const double* x, double* y) { T.A.matvec(x, y); },
+        [&](const double* r, double* z) { pc_apply(T, r, z); }, iters);
 }
 
 template <class Mdl>
@@ -528,7 +540,68 @@ static void svi_correction(Tissue& T, double* b) {
     }
 }
 
+// ------------------------------------------------------------- bidomain --
+// BidomainProblem without a bath: BidomainSolver::SetupLinearSystem
+// (heart/src/solver/electrics/bidomain/BidomainSolver.cpp:63-190) on the interleaved
+// unknowns (V_0, phi_0, V_1, phi_1, ...) with the blocks of BidomainAssembler
+// (BidomainAssembler.cpp:41-89) and BidomainMassMatrixAssembler (mass in the V-V block
+// only), b = M z with z = (Am Cm V/dt - Am Iion - Istim, 0); then PETSc CG.  With no
+// fixed phi_e the system is singular and the solve carries the null space of constant
+// phi_e (AbstractBidomainSolver::FinaliseLinearSystem / GenerateNullBasis,
+// AbstractBidomainSolver.cpp:112-186): KSP_PCApply removes it from every
+// preconditioned vector.  Fixed phi_e nodes are Dirichlet rows and columns
+// (BoundaryConditionsContainer::ApplyDirichletToLinearProblem on a symmetric matrix,
+// pde/src/common/BoundaryConditionsContainerImplementation.hpp:257-417) with value 0.
+static void bido_pc(Tissue& T, const double* r, double* z) {
+    const int n2 = 2 * T.n;
+    if (T.cfg.pc == ORC_PC_JACOBI) {
+        const double* d = T.bdinv.data();
+        parallel_for(n2, [&](int b, int e) {
+            for (int i = b; i < e; ++i) z[i] = r[i] * d[i];
+        });
+    } else {
+        std::memcpy(z, r, sizeof(double) * n2);
+    }
+    if (T.nullspace) {
+        // MatNullSpaceRemove: z -= (z . e) e, e = (0, 1/sqrt(n), 0, 1/sqrt(n), ...)
+        const double inv = 1.0 / std::sqrt((double)T.n);
+        const double alpha = parallel_sum(T.n, [&](int i) { return z[2 * i + 1] * inv; });
+        parallel_for(T.n, [&](int b, int e) {
+            for (int i = b; i < e; ++i) z[2 * i + 1] -= alpha * inv;
+        });
+    }
+}
+
+static int step_bido(Tissue& T, int* iters) {
+    const double t0 = T.t;
+    const double t1 = (double)(T.steps + 1) * T.cfg.dt_pde;
+    if (T.cfg.model == ORC_TT06) solve_cells<chb::TenTusscher2006Epi>(T, t0, t1);
+    else solve_cells<chb::LuoRudy1991>(T, t0, t1);
+    const double am = T.cfg.am, cm = T.cfg.cm;
+    const double dtinv = 1.0 / T.cfg.dt_pde;
+    double* zz = T.w.data();
+    parallel_for(T.n, [&](int b, int e) {
+        for (int i = b; i < e; ++i) zz[i] = am * cm * T.V[i] * dtinv + (-am * T.iion[i] - T.istim[i]);
+    });
+    T.M.matvec(zz, T.bmz.data());
+    for (int i = 0; i < T.n; ++i) {
+        T.bb[2 * i] = T.bmz[i];
+        T.bb[2 * i + 1] = 0.0;   // phi_e rows of M z are zero; fixed rows hold the value 0
+    }
+    for (int i = 0; i < T.n; ++i) T.u[2 * i] = T.V[i];
+    const int rc = cg_core(
+        T.cfg, 2 * T.n, T.u.data(), T.bb.data(), T.br.data(), T.bz.data(), T.bp.data(), T.bw.data(),
+        [&](const double* x, double* y) { T.B.matvec(x, y); }, [&](const double* r, double* z) { bido_pc(T, r, z); },
+        iters);
+    if (rc != 0) return rc;
+    for (int i = 0; i < T.n; ++i) T.V[i] = T.u[2 * i];
+    T.steps++;
+    T.t = t1;
+    return 0;
+}
+
 static int step_once(Tissue& T, int* iters) {
+    if (T.bido) return step_bido(T, iters);
     if (T.cfg.solver == ORC_SOLVER_OPERATOR_SPLITTING) return step_split(T, iters);
     const double t0 = T.t;
     const double t1 = (double)(T.steps + 1) * T.cfg.dt_pde;
@@ -735,6 +808,74 @@ orc_tissue* orc_tissue_create(const orc_config* cfg, int dim, int n_nodes, const
     T.w.assign(T.n, 0.0);
     T.x.assign(T.n, 0.0);
     return h;
+}
+
+int orc_tissue_set_bidomain(orc_tissue* h, const double* xyz, int n_elems, const int* conn, const double* sigma_i,
+                            const double* sigma_e, const int* fixed, int n_fixed) {
+    Tissue& T = h->T;
+    if (T.bido || T.steps != 0 || T.cfg.solver != ORC_SOLVER_MONODOMAIN || T.cfg.svi || T.cfg.mass_lumping ||
+        T.cfg.pc == ORC_PC_BJACOBI || n_fixed < 0 || (n_fixed > 0 && !fixed))
+        return -4;
+    const int n = T.n, dim = T.dim, nb = dim + 1;
+    for (int k = 0; k < n_fixed; ++k)
+        if (fixed[k] < 0 || fixed[k] >= n) return -4;
+    // pattern: rows 2i and 2i+1 both hold columns 2j, 2j+1 for every j of A's row i
+    Csr& B = T.B;
+    B.n = 2 * n;
+    B.rp.assign(2 * n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        const int len = 2 * (T.A.rp[i + 1] - T.A.rp[i]);
+        B.rp[2 * i + 1] = B.rp[2 * i] + len;
+        B.rp[2 * i + 2] = B.rp[2 * i + 1] + len;
+    }
+    B.ci.resize(B.rp[2 * n]);
+    for (int i = 0; i < n; ++i)
+        for (int r = 0; r < 2; ++r) {
+            int q = B.rp[2 * i + r];
+            for (int k = T.A.rp[i]; k < T.A.rp[i + 1]; ++k) {
+                B.ci[q++] = 2 * T.A.ci[k];
+                B.ci[q++] = 2 * T.A.ci[k] + 1;
+            }
+        }
+    B.v.assign(B.ci.size(), 0.0);
+    const double ms = T.cfg.am * T.cfg.cm / T.cfg.dt_pde;
+    for (int e = 0; e < n_elems; ++e) {
+        double X[4 * 3];
+        for (int a = 0; a < nb; ++a)
+            for (int c = 0; c < 3; ++c) X[a * 3 + c] = xyz[(size_t)conn[e * nb + a] * 3 + c];
+        double Me[16], Ki[16], Me2[16], Ke[16];
+        if (!element_matrices(dim, X, sigma_i + (size_t)e * dim, false, Me, Ki) ||
+            !element_matrices(dim, X, sigma_e + (size_t)e * dim, false, Me2, Ke))
+            return -4;
+        for (int a = 0; a < nb; ++a)
+            for (int c = 0; c < nb; ++c) {
+                const int i = conn[e * nb + a], j = conn[e * nb + c];
+                const double ki = Ki[a * nb + c];
+                B.v[B.find(2 * i, 2 * j)] += ms * Me[a * nb + c] + ki;
+                B.v[B.find(2 * i, 2 * j + 1)] += ki;
+                B.v[B.find(2 * i + 1, 2 * j)] += ki;
+                B.v[B.find(2 * i + 1, 2 * j + 1)] += ki + Ke[a * nb + c];
+            }
+    }
+    // fixed phi_e = 0: zero the row and the column, 1 on the diagonal
+    std::vector<char> is_fixed(2 * n, 0);
+    for (int k = 0; k < n_fixed; ++k) is_fixed[2 * fixed[k] + 1] = 1;
+    for (int r = 0; r < 2 * n; ++r)
+        for (int k = B.rp[r]; k < B.rp[r + 1]; ++k)
+            if (is_fixed[r] || is_fixed[B.ci[k]]) B.v[k] = (B.ci[k] == r) ? 1.0 : 0.0;
+    T.nullspace = n_fixed == 0;
+    T.bdinv.resize(2 * n);
+    for (int r = 0; r < 2 * n; ++r) T.bdinv[r] = 1.0 / B.v[B.find(r, r)];
+    for (auto* v : {&T.bb, &T.br, &T.bz, &T.bp, &T.bw}) v->assign(2 * n, 0.0);
+    T.bmz.assign(n, 0.0);
+    T.u.assign(2 * n, 0.0);
+    for (int i = 0; i < n; ++i) T.u[2 * i] = T.V[i];
+    T.bido = true;
+    return 0;
+}
+
+void orc_tissue_get_extracellular(const orc_tissue* h, double* phi) {
+    for (int i = 0; i < h->T.n; ++i) phi[i] = h->T.bido ? h->T.u[2 * i + 1] : 0.0;
 }
 
 void orc_tissue_destroy(orc_tissue* t) { delete t; }

@@ -113,6 +113,9 @@ def lib():
         L.orc_tissue_matrix.restype = C.c_int
         L.orc_tissue_matrix.argtypes = [C.c_void_p, C.c_int, ip, ip, dp]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_tissue_set_bidomain.restype = C.c_int
+        L.orc_tissue_set_bidomain.argtypes = [C.c_void_p, dp, C.c_int, ip, dp, dp, ip, C.c_int]
+        L.orc_tissue_get_extracellular.argtypes = [C.c_void_p, dp]
         L.orc_cable_run.restype = C.c_int
         L.orc_cable_run.argtypes = [C.POINTER(CableConfig), dp, ip, C.c_int, dp, dp, dp, dp]
         L.orc_cable_tangent_gradient.restype = C.c_int
@@ -216,6 +219,24 @@ class Tissue:
         v = np.zeros(self.n)
         lib().orc_tissue_get_voltage(self.h, _dp(v))
         return v
+
+    def set_bidomain(self, xyz, conn, sigma_i, sigma_e, fixed=None):
+        """orc_tissue_set_bidomain: (V, phi_e) unknowns; fixed phi_e = 0 at `fixed` nodes, else the
+        null space of constant phi_e."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        conn = np.ascontiguousarray(conn, dtype=np.int32)
+        si = np.ascontiguousarray(sigma_i, dtype=np.float64)
+        se = np.ascontiguousarray(sigma_e, dtype=np.float64)
+        fx = None if fixed is None else np.ascontiguousarray(fixed, dtype=np.int32)
+        rc = lib().orc_tissue_set_bidomain(self.h, _dp(xyz), conn.shape[0], _ip(conn), _dp(si), _dp(se), _ip(fx),
+                                           0 if fx is None else fx.size)
+        if rc != 0:
+            raise RuntimeError(f"orc_tissue_set_bidomain failed with code {rc}")
+
+    def extracellular(self):
+        phi = np.zeros(self.n)
+        lib().orc_tissue_get_extracellular(self.h, _dp(phi))
+        return phi
 
     def states(self):
         s = np.zeros((self.n, self.ns))

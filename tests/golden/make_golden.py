@@ -89,6 +89,24 @@ out = {
          "midway": {"end": 1.0, "nodes": [0, 665, 1330], "V": [48.0637, 26.5404, -55.3058],
                     "tolerance": 1e-3}},
     ],
+    # BidomainProblem<1> with PlaneStimulusCellFactory<LR91> (SimpleStimulus(-600, 0.5) at x = 0),
+    # sigma_i = sigma_e = 0.0005, Am = Cm = 1, dt 0.01 ms, HeartConfig's default KSP tolerance
+    # (absolute 2e-4); solution entries interleaved as (V_0, phi_0, V_1, phi_1, ...)
+    "bidomain": [
+        {"name": "TestSimpleBidomain1D", "source": "heart/test/bidomain/TestBidomainProblem.hpp:1006-1040",
+         "h": 0.01, "size": 0.1, "sigma_i": 0.0005, "sigma_e": 0.0005, "am": 1.0, "cm": 1.0, "end": 2.0,
+         "abs_tol": 2e-4, "fixed": [], "solution_index": [1, 2, 3, 5, 7, 9, 10],
+         "solution": [-16.4861, 22.8117, -16.4893, -16.5617, -16.6761, -16.8344, 25.3148], "tolerance": 5e-3},
+        {"name": "TestBidomainDg01DPinned", "source": "heart/test/bidomain/TestBidomainProblem.hpp:240-331",
+         "h": 0.01, "size": 1.0, "sigma_i": 0.0005, "sigma_e": 0.0005, "am": 1.0, "cm": 1.0, "end": 1.0,
+         "abs_tol": 2e-4, "fixed": [100], "voltage_nodes": [0, 1, 2, 3, 4, 5],
+         "voltage": [31.0335, 28.9214, 20.0279, -3.92649, -57.9395, -79.7754], "tolerance": 7e-3,
+         "rest_from_node": 51, "rest": -83.85, "rest_tolerance": 0.1},
+        {"name": "TestCompareBidomainProblemWithMonodomain",
+         "source": "heart/test/bidomain/TestBidomainProblem.hpp:475-556",
+         "h": 0.01, "size": 1.0, "sigma_i": 0.0005, "sigma_e": 1.0, "am": 1.0, "cm": 1.0, "end": 1.0,
+         "abs_tol": 2e-4, "fixed": [], "max_v_difference_from_monodomain": 0.4, "max_abs_phi_e": 0.06},
+    ],
 }
 here = os.path.dirname(os.path.abspath(__file__))
 with open(os.path.join(here, "chaste_kats.json"), "w") as f:
