@@ -92,6 +92,9 @@ SIGNATURES = {
     "cg_set_mesh": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_int, _ip, _dp]),
     "cg_set_slab_mesh": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _ip]),
     "cg_set_cells": (C.c_int, [_vp, _dp, _ip, _dp, C.c_int]),
+    "cg_set_bidomain_mesh": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_int, _ip, _dp, _dp]),
+    "cg_set_fixed_extracellular_nodes": (C.c_int, [_vp, _ip, C.c_int]),
+    "cg_get_extracellular_potential": (C.c_int, [_vp, _dp]),
     "cg_set_stimulus": (C.c_int, [_vp, _ip, C.POINTER(Stimulus), C.c_int]),
     "cg_step": (C.c_int, [_vp, C.c_int]),
     "cg_step_host": (C.c_int, [_vp, _dp, C.c_int, _dp, C.c_int]),
@@ -236,6 +239,27 @@ class Tissue:
         check(lib().cg_set_mesh(self.h, xyz.shape[0], dim, dptr(xyz), conn.shape[0], iptr(conn), dptr(sigma)),
               "cg_set_mesh")
         self.n = xyz.shape[0]
+
+    def set_bidomain_mesh(self, xyz, conn, sigma_i, sigma_e):
+        """cg_set_bidomain_mesh: the tissue solves for (V, phi_e); sigma_* per element (or broadcast)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        conn = np.ascontiguousarray(conn, dtype=np.int32)
+        dim = conn.shape[1] - 1
+        si, se = (np.ascontiguousarray(np.broadcast_to(np.asarray(s, dtype=np.float64), (conn.shape[0], dim)))
+                  for s in (sigma_i, sigma_e))
+        check(lib().cg_set_bidomain_mesh(self.h, xyz.shape[0], dim, dptr(xyz), conn.shape[0], iptr(conn), dptr(si),
+                                         dptr(se)), "cg_set_bidomain_mesh")
+        self.n = xyz.shape[0]
+
+    def fix_extracellular_potential(self, nodes):
+        nodes = np.ascontiguousarray(nodes, dtype=np.int32)
+        check(lib().cg_set_fixed_extracellular_nodes(self.h, iptr(nodes), nodes.size),
+              "cg_set_fixed_extracellular_nodes")
+
+    def extracellular_potential(self):
+        phi = np.empty(self.n)
+        check(lib().cg_get_extracellular_potential(self.h, dptr(phi)), "cg_get_extracellular_potential")
+        return phi
 
     def set_slab_mesh(self, dim, h, width, height=0.0, depth=0.0, sigma=(1.75, 1.75, 1.75)):
         sig = np.ascontiguousarray(np.asarray(sigma, dtype=np.float64)[:dim])

@@ -14,6 +14,7 @@
 #include "../../include/chaste_gpu.h"
 #include "host/assemble.h"
 #include "kernels/cg.cuh"
+#include "kernels/cg_bidomain.cuh"
 #include "kernels/cg_ilu.cuh"
 #include "kernels/cg_mixed.cuh"
 #include "kernels/ode.cuh"
@@ -130,6 +131,19 @@ struct cg_ctx {
     // bjacobi (ILU(0) of the whole matrix): factors, level schedules, b and B b
     bool ilu = false;
     IluArgs ilu_args{};
+    // bidomain (cg_set_bidomain_mesh): the interleaved (V, phi_e) operator B, on the host
+    // for fixing phi_e nodes and on the device, and the solve's vectors
+    bool bido = false;
+    bool bido_nullspace = true;
+    std::vector<int> b_rp, b_ci;
+    std::vector<double> b_val;
+    int* d_brp = nullptr;
+    int* d_bci = nullptr;
+    double* d_bval = nullptr;
+    double* d_bdinv = nullptr;
+    double* d_u = nullptr;
+    double* d_bvec[4] = {};   // r, z, p, q
+    int bido_blocks = 0;
     // stats
     long long steps = 0;
     long long total_iters = 0;
@@ -803,9 +817,138 @@ int setup_svi(cg_ctx* c, int dim, int n, const double* xyz, int n_elems, const i
     return CG_OK;
 }
 
+// B's values and Jacobi inverse on the device (after assembly and after fixing nodes).
+int upload_bidomain_values(cg_ctx* c) {
+    const size_t n2 = 2 * (size_t)c->n;
+    std::vector<double> dinv(n2);
+    for (size_t r = 0; r < n2; ++r) {
+        double d = 0.0;
+        for (int k = c->b_rp[r]; k < c->b_rp[r + 1]; ++k)
+            if (c->b_ci[k] == (int)r) d = c->b_val[k];
+        if (d == 0.0) return CG_ERR_ARG;
+        dinv[r] = 1.0 / d;
+    }
+    CG_CUDA(cudaMemcpyAsync(c->d_bval, c->b_val.data(), c->b_val.size() * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    CG_CUDA(cudaMemcpyAsync(c->d_bdinv, dinv.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CG_CUDA(cudaStreamSynchronize(c->stream));
+    c->graph_dirty = true;
+    return CG_OK;
+}
+
+// The bidomain operator B on the interleaved unknowns (BidomainAssembler.cpp:41-89):
+// rows 2i and 2i+1 carry node i's pattern twice (columns 2j, 2j+1), and element e adds
+// Am Cm/dt M_e + K_i,e to the V-V block, K_i,e to both off-diagonal blocks and
+// K_i,e + K_e,e to the phi_e-phi_e block, in ascending element order.
+int setup_bidomain(cg_ctx* c, const double* xyz, int n_elems, const int* conn, const double* sigma_i,
+                   const double* sigma_e) {
+    const int n = c->n, dim = c->dim, nb = dim + 1;
+    const HostCsr& A = c->csr;
+    c->b_rp.assign(2 * (size_t)n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        const int len = 2 * (A.rowptr[i + 1] - A.rowptr[i]);
+        c->b_rp[2 * i + 1] = c->b_rp[2 * i] + len;
+        c->b_rp[2 * i + 2] = c->b_rp[2 * i + 1] + len;
+    }
+    const size_t nnz = (size_t)c->b_rp[2 * n];
+    c->b_ci.resize(nnz);
+    for (int i = 0; i < n; ++i)
+        for (int r = 0; r < 2; ++r) {
+            int q = c->b_rp[2 * i + r];
+            for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) {
+                c->b_ci[q++] = 2 * A.cols[k];
+                c->b_ci[q++] = 2 * A.cols[k] + 1;
+            }
+        }
+    c->b_val.assign(nnz, 0.0);
+    // position of (node i, node j) in A's row i: B's entries follow as 2 (k - rowptr[i])
+    auto at = [&](int i, int j) { return A.find(i, j) - A.rowptr[i]; };
+    const double ms = c->cfg.surface_area_to_volume_ratio * c->cfg.capacitance / c->cfg.pde_time_step;
+    for (int e = 0; e < n_elems; ++e) {
+        double X[12], Me[16], Ki[16], Me2[16], Ke[16];
+        for (int a = 0; a < nb; ++a)
+            for (int s2 = 0; s2 < 3; ++s2) X[a * 3 + s2] = xyz[(size_t)conn[(size_t)e * nb + a] * 3 + s2];
+        if (!element_matrices(dim, X, sigma_i + (size_t)e * dim, false, Me, Ki) ||
+            !element_matrices(dim, X, sigma_e + (size_t)e * dim, false, Me2, Ke))
+            return CG_ERR_ARG;
+        for (int a = 0; a < nb; ++a)
+            for (int b2 = 0; b2 < nb; ++b2) {
+                const int i = conn[(size_t)e * nb + a], j = conn[(size_t)e * nb + b2];
+                const int off = 2 * at(i, j);
+                const double ki = Ki[a * nb + b2];
+                c->b_val[c->b_rp[2 * i] + off] += ms * Me[a * nb + b2] + ki;
+                c->b_val[c->b_rp[2 * i] + off + 1] += ki;
+                c->b_val[c->b_rp[2 * i + 1] + off] += ki;
+                c->b_val[c->b_rp[2 * i + 1] + off + 1] += ki + Ke[a * nb + b2];
+            }
+    }
+    const size_t n2 = 2 * (size_t)n;
+    CG_TRY(dalloc(c, &c->d_brp, (n2 + 1) * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_bci, nnz * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_bval, nnz * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_bdinv, n2 * sizeof(double)));
+    CG_TRY(dalloc(c, &c->d_u, n2 * sizeof(double)));
+    for (double*& v : c->d_bvec) CG_TRY(dalloc(c, &v, n2 * sizeof(double)));
+    CG_CUDA(cudaMemsetAsync(c->d_u, 0, n2 * sizeof(double), c->stream));
+    CG_CUDA(cudaMemcpyAsync(c->d_brp, c->b_rp.data(), (n2 + 1) * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CG_CUDA(cudaMemcpyAsync(c->d_bci, c->b_ci.data(), nnz * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    // one co-resident grid of 512-thread blocks over the 2n rows
+    int sms = 1, per_sm = 0;
+    CG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_bidomain_kernel, 512, 0));
+    if (per_sm < 1) return CG_ERR_UNSUPPORTED;
+    c->bido_blocks = (int)std::max(1LL, std::min({((long long)n2 + 511) / 512, (long long)per_sm * sms,
+                                                 (long long)kMaxGridBlocks}));
+    CG_TRY(dalloc(c, &c->d_partials, (size_t)2 * kMaxGridBlocks * kPartialStride * sizeof(double)));
+    c->bido = true;
+    c->bido_nullspace = true;
+    return upload_bidomain_values(c);
+}
+
 }  // namespace
 
 extern "C" {
+
+int cg_set_bidomain_mesh(cg_ctx* c, int n_nodes, int dim, const double* xyz, int n_elems, const int* conn,
+                         const double* sigma_i, const double* sigma_e) {
+    if (!c || !sigma_e) return CG_ERR_ARG;
+    if (c->have_mesh) return CG_ERR_ORDER;
+    if (c->mixed() || c->cfg.solver != CG_SOLVER_MONODOMAIN || c->cfg.use_state_variable_interpolation ||
+        c->cfg.use_mass_lumping || c->cfg.ksp_preconditioner == CG_PC_BJACOBI)
+        return CG_ERR_UNSUPPORTED;
+    CG_TRY(cg_set_mesh(c, n_nodes, dim, xyz, n_elems, conn, sigma_i));
+    const int rc = setup_bidomain(c, xyz, n_elems, conn, sigma_i, sigma_e);
+    if (rc != CG_OK) c->have_mesh = false;
+    return rc;
+}
+
+int cg_set_fixed_extracellular_nodes(cg_ctx* c, const int* nodes, int n_fixed) {
+    if (!c || n_fixed < 0 || (n_fixed > 0 && !nodes)) return CG_ERR_ARG;
+    if (!c->bido) return CG_ERR_ORDER;
+    if (c->steps != 0 || !c->bido_nullspace) return CG_ERR_ORDER;
+    for (int k = 0; k < n_fixed; ++k)
+        if (nodes[k] < 0 || nodes[k] >= c->n) return CG_ERR_ARG;
+    if (n_fixed == 0) return CG_OK;
+    CG_CUDA(cudaSetDevice(c->device));
+    // Dirichlet phi_e = 0 on a symmetric matrix: zero the row and the column, 1 on the
+    // diagonal (the column's moved contribution is value x column = 0)
+    std::vector<char> fixed(2 * (size_t)c->n, 0);
+    for (int k = 0; k < n_fixed; ++k) fixed[2 * (size_t)nodes[k] + 1] = 1;
+    for (size_t r = 0; r < fixed.size(); ++r)
+        for (int k = c->b_rp[r]; k < c->b_rp[r + 1]; ++k)
+            if (fixed[r] || fixed[c->b_ci[k]]) c->b_val[k] = c->b_ci[k] == (int)r ? 1.0 : 0.0;
+    c->bido_nullspace = false;
+    return upload_bidomain_values(c);
+}
+
+int cg_get_extracellular_potential(cg_ctx* c, double* phi_e) {
+    if (!c || !phi_e) return CG_ERR_ARG;
+    if (!c->bido || !c->have_cells) return CG_ERR_ORDER;
+    CG_CUDA(cudaSetDevice(c->device));
+    CG_CUDA(cudaMemcpy2D(phi_e, sizeof(double), c->d_u + 1, 2 * sizeof(double), sizeof(double), (size_t)c->n,
+                         cudaMemcpyDeviceToHost));
+    return CG_OK;
+}
 
 int cg_set_mesh(cg_ctx* c, int n_nodes, int dim, const double* xyz, int n_elems, const int* conn,
                 const double* sigma) {
@@ -1076,6 +1219,40 @@ cudaError_t launch_cg(cg_ctx* c) {
     return cudaLaunchKernelEx(&cfg, pick_cg_kernel(c), a);
 }
 
+// The bidomain solve: u's V entries from the voltage, then the persistent CG on B.
+cudaError_t launch_bidomain(cg_ctx* c) {
+    bido_copy_voltage_kernel<<<c->ode_blocks, 256, 0, c->stream>>>(c->n, c->d_V, c->d_u);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    CgArgs a = make_cg_args(c);
+    BidoArgs b;
+    b.n2 = 2 * c->n;
+    b.rp = c->d_brp;
+    b.ci = c->d_bci;
+    b.val = c->d_bval;
+    b.dinv = c->cfg.ksp_preconditioner == CG_PC_JACOBI ? c->d_bdinv : nullptr;
+    b.u = c->d_u;
+    b.r = c->d_bvec[0];
+    b.z = c->d_bvec[1];
+    b.p = c->d_bvec[2];
+    b.q = c->d_bvec[3];
+    b.nullspace = c->bido_nullspace ? 1 : 0;
+    b.inv_sqrt_n = 1.0 / std::sqrt((double)c->n);
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(c->bido_blocks);
+    lc.blockDim = dim3(512);
+    lc.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    return cudaLaunchKernelEx(&lc, cg_bidomain_kernel, a, b);
+}
+
+// The diffusion solve of a step (after the ODE launch).
+cudaError_t launch_solve(cg_ctx* c) { return c->bido ? launch_bidomain(c) : launch_cg(c); }
+
 // The ODE launch of a step: the whole step with V clamped (half 0), or one half of
 // the operator-splitting step including V (half 1, 2); half 0 may cover the nodes
 // [lo, hi) only.
@@ -1177,7 +1354,7 @@ cudaError_t launch_step(cg_ctx* c) {
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    e = launch_cg(c);
+    e = launch_solve(c);
     if (e != cudaSuccess || !split(c)) return e;
     launch_odes(c, 2);
     return cudaGetLastError();
@@ -1308,7 +1485,7 @@ int cg_step_host(cg_ctx* c, const double* v_in, int n_steps, double* v_out, int 
                 CG_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[k], 0));
                 launch_odes(c, 0, lo, hi, keep_history == 0);
             }
-            if (cudaGetLastError() != cudaSuccess || launch_cg(c) != cudaSuccess) {
+            if (cudaGetLastError() != cudaSuccess || launch_solve(c) != cudaSuccess) {
                 cudaGetLastError();
                 return CG_ERR_CUDA;
             }
@@ -1527,6 +1704,7 @@ int cg_get_iteration_history(cg_ctx* c, int n, int* it) {
 }
 
 int cg_snapshot_size(cg_ctx* c, size_t* bytes) {
+    if (c && c->bido) return CG_ERR_UNSUPPORTED;   // the snapshot holds V and the cells, not phi_e
     if (!c || !bytes) return CG_ERR_ARG;
     if (!c->have_cells) return CG_ERR_ORDER;
     const size_t n = (size_t)c->n, w = c->real_size();
@@ -1535,6 +1713,7 @@ int cg_snapshot_size(cg_ctx* c, size_t* bytes) {
 }
 
 int cg_snapshot(cg_ctx* c, void* buf, size_t bytes) {
+    if (c && c->bido) return CG_ERR_UNSUPPORTED;   // the snapshot holds V and the cells, not phi_e
     size_t need = 0;
     CG_TRY(cg_snapshot_size(c, &need));
     if (!buf || bytes < need) return CG_ERR_ARG;
@@ -1565,6 +1744,7 @@ int cg_snapshot(cg_ctx* c, void* buf, size_t bytes) {
 }
 
 int cg_restore(cg_ctx* c, const void* buf, size_t bytes) {
+    if (c && c->bido) return CG_ERR_UNSUPPORTED;   // the snapshot holds V and the cells, not phi_e
     size_t need = 0;
     CG_TRY(cg_snapshot_size(c, &need));
     if (!buf || bytes < need) return CG_ERR_ARG;
@@ -1613,7 +1793,7 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
         launch_odes(c, split(c) ? 1 : 0);
         cudaEventRecord(e[1], c->stream);
         if (c->svi) launch_svi(c);   // part of assembling the RHS (ASSEMBLE_RHS)
-        if (cudaGetLastError() != cudaSuccess || launch_cg(c) != cudaSuccess) rc = CG_ERR_CUDA;
+        if (cudaGetLastError() != cudaSuccess || launch_solve(c) != cudaSuccess) rc = CG_ERR_CUDA;
         cudaEventRecord(e[2], c->stream);
         if (split(c)) launch_odes(c, 2);
         cudaEventRecord(e[3], c->stream);

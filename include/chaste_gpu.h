@@ -145,6 +145,25 @@ int cg_set_mesh(cg_ctx* ctx, int n_nodes, int dim, const double* xyz, int n_elem
 int cg_set_slab_mesh(cg_ctx* ctx, int dim, double h, double width, double height,
                      double depth, const double* sigma, int* n_nodes_out);
 
+/* Bidomain without a bath (BidomainProblem, heart/src/problem/BidomainProblem.cpp;
+ * BidomainSolver, heart/src/solver/electrics/bidomain/BidomainSolver.cpp:63-190;
+ * BidomainAssembler.cpp:41-89): instead of cg_set_mesh, the same mesh with intracellular
+ * and extracellular conductivities (n_elems x dim each).  The unknowns become the
+ * interleaved pairs (V_i, phi_e_i); a step is the cells' ODEs, b = (M z, 0) and CG on
+ * B = [Am Cm/dt M + K_i, K_i; K_i, K_i + K_e].  Without fixed nodes B is singular and
+ * the solve removes the null space of constant phi_e from every preconditioned vector
+ * (AbstractBidomainSolver::GenerateNullBasis, AbstractBidomainSolver.cpp:112-134).
+ * FP64, Jacobi or no preconditioner, CG_SOLVER_MONODOMAIN, no SVI or mass lumping
+ * (CG_ERR_UNSUPPORTED otherwise); snapshots are not available for it. */
+int cg_set_bidomain_mesh(cg_ctx* ctx, int n_nodes, int dim, const double* xyz, int n_elems, const int* conn,
+                         const double* sigma_i, const double* sigma_e);
+/* SetFixedExtracellularPotentialNodes (AbstractBidomainSolver.cpp:262-290): phi_e = 0 at
+ * these nodes (Dirichlet rows and columns), which removes the null space.  Before the
+ * first step, once. */
+int cg_set_fixed_extracellular_nodes(cg_ctx* ctx, const int* nodes, int n_nodes);
+/* phi_e of every node (n_nodes doubles). */
+int cg_get_extracellular_potential(cg_ctx* ctx, double* phi_e);
+
 /* Cells: what AbstractCardiacCellFactory::CreateCardiacCellForTissueNode decides per node
  * (heart/src/problem/cell_factories/AbstractCardiacCellFactory.cpp:42-67).
  * init_states: n_nodes x n_states node-major (AoS as Chaste cells hold them) or NULL
