@@ -110,6 +110,7 @@ SIGNATURES = {
     "cg_apply_inner_preconditioner": (C.c_int, [_vp, _dp, _dp]),
     "cg_num_nodes": (C.c_int, [_vp, _ip]),
     "cg_num_states": (C.c_int, [C.c_int, _ip]),
+    "cg_slab_mesh": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _ip, _ip, _dp, _ip]),
     "cg_num_params": (C.c_int, [C.c_int, _ip]),
     "cg_snapshot_size": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
     "cg_snapshot": (C.c_int, [_vp, _vp, C.c_size_t]),
@@ -212,6 +213,17 @@ def num_params(model):
     n = C.c_int()
     check(lib().cg_num_params(model, C.byref(n)), "cg_num_params")
     return n.value
+
+
+def slab_mesh(dim, h, width, height=0.0, depth=0.0):
+    """(xyz, conn) of the regular slab (cg_slab_mesh; host only, no GPU needed)."""
+    nn, ne = C.c_int(), C.c_int()
+    check(lib().cg_slab_mesh(dim, h, width, height, depth, C.byref(nn), C.byref(ne), None, None), "cg_slab_mesh")
+    xyz = np.zeros((nn.value, 3))
+    conn = np.zeros((ne.value, dim + 1), dtype=np.int32)
+    check(lib().cg_slab_mesh(dim, h, width, height, depth, C.byref(nn), C.byref(ne), dptr(xyz), iptr(conn)),
+          "cg_slab_mesh")
+    return xyz, conn
 
 
 def stimulus(kind, magnitude=0.0, duration=0.0, start=0.0, period=0.0, stop=1.7976931348623157e308):

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstdint>
+#include <climits>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -287,6 +288,24 @@ const char* cg_status_string(int s) {
         case CG_ERR_UNSUPPORTED: return "unsupported configuration";
         default: return "unknown status";
     }
+}
+
+int cg_slab_mesh(int dim, double h, double width, double height, double depth, int* n_nodes, int* n_elems,
+                 double* xyz, int* conn) {
+    if (!n_nodes || !n_elems || dim < 1 || dim > 3) return CG_ERR_ARG;
+    SlabGrid g;
+    if (!slab_grid(dim, h, width, height, depth, g) || g.nodes() > INT_MAX) return CG_ERR_ARG;
+    const long long ne = dim == 1 ? g.nx : (dim == 2 ? 2LL * g.nx * g.ny : 6LL * g.nx * g.ny * g.nz);
+    if (ne > INT_MAX) return CG_ERR_ARG;
+    *n_nodes = (int)g.nodes();
+    *n_elems = (int)ne;
+    if (!xyz && !conn) return CG_OK;
+    std::vector<double> x;
+    std::vector<int> cn;
+    slab_mesh(g, x, cn);
+    if (xyz) std::memcpy(xyz, x.data(), x.size() * sizeof(double));
+    if (conn) std::memcpy(conn, cn.data(), cn.size() * sizeof(int));
+    return CG_OK;
 }
 
 int cg_num_states(int model, int* n) {

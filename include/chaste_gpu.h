@@ -215,6 +215,12 @@ int cg_get_iteration_history(cg_ctx* ctx, int n, int* iterations);
 int cg_apply_inner_preconditioner(cg_ctx* ctx, const double* x, double* y);
 
 int cg_num_nodes(cg_ctx* ctx, int* n);
+/* Host only: the regular slab cg_set_slab_mesh builds (ConstructRegularSlabMesh,
+ * mesh/src/common/AbstractTetrahedralMesh.cpp:569-614), for the calls that take a mesh
+ * (cg_set_mesh, cg_set_bidomain_mesh).  With xyz and conn NULL only the sizes are
+ * returned; xyz: n_nodes x 3, conn: n_elems x (dim + 1). */
+int cg_slab_mesh(int dim, double h, double width, double height, double depth, int* n_nodes, int* n_elems,
+                 double* xyz, int* conn);
 int cg_num_states(int model, int* n);
 int cg_num_params(int model, int* n);
 

@@ -83,3 +83,13 @@ def test_slab_stencil_reproduces_every_row(probe, dim, h, size, sigma, ms):
         for o, off in enumerate(r["offs"]):
             if off not in nz:
                 assert r["at"][c, o] == 0.0 and r["mt"][c, o] == 0.0
+
+
+@pytest.mark.parametrize("dim,size", [(1, (0.1, 0.0, 0.0)), (2, (0.2, 0.1, 0.0)), (3, (0.1, 0.05, 0.03))])
+def test_library_slab_mesh_matches_oracle(oracle, native, dim, size):
+    """cg_slab_mesh (host only, loads the library without a GPU) gives the oracle's
+    ConstructRegularSlabMesh node order and elements bit for bit."""
+    xyz, conn = native.slab_mesh(dim, 0.01, *size)
+    oxyz, oconn, _ = oracle.slab_mesh(dim, 0.01, *size)
+    assert np.array_equal(xyz, oxyz)
+    assert np.array_equal(conn, oconn)
