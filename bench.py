@@ -510,6 +510,83 @@ def run_mixed(args):
     return line
 
 
+def run_bidomain(args):
+    """The bidomain step without a bath on the 2D LR91 sheet of configuration 1 (1 x 1 cm,
+    h = 0.01 cm, 10,201 nodes, 20,402 unknowns), Chaste's default conductivities
+    (intracellular 1.75 / 0.19, extracellular 7.0 / 2.365 mS/cm along x / y), forward Euler dt
+    0.01 ms, PDE dt 0.1 ms, CG + Jacobi rtol 1e-8 with the null space of constant phi_e, FP64.
+    Timed from t = --t-start-ms, L2 flushed before every step.  Metric: node-steps/s."""
+    import torch
+
+    from chaste_b200 import _native as N
+    from chaste_b200.build import build_native
+
+    build_native()
+    dim, h, size = 2, 0.01, (1.0, 1.0, 0.0)
+    xyz, conn = N.slab_mesh(dim, h, *size)
+    si, se = (1.75, 0.19), (7.0, 2.365)
+    cfg = N.default_config()
+    cfg.model, cfg.ode_method = N.MODEL_LR91, N.ODE_FORWARD_EULER
+    cfg.ode_time_step, cfg.pde_time_step = 0.01, 0.1
+    cfg.ksp_preconditioner = N.PC_JACOBI
+    cfg.use_absolute_tolerance, cfg.ksp_tolerance = 0, 1e-8
+    t = N.Tissue(cfg)
+    t.set_bidomain_mesh(xyz, conn, si, se)
+    t.set_cells()
+    sid = np.where(xyz[:, 0] <= 0.0199 + 1e-12, 0, -1).astype(np.int32)
+    t.set_stimulus(sid, [N.stimulus(N.STIM_SIMPLE, -5e5, 0.5, 0.0)])
+    start = int(round(args.t_start_ms / 0.1))
+    t.step(start + args.warmup)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda:0")
+    ms, its = 0.0, 0
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t.step(1)
+        st = t.stats()
+        ms += st.ms_last_call
+        its += st.last_cg_iterations
+    n = xyz.shape[0]
+    vin = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    vout = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    t.voltage(out=vin)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        t.step_host(vin, 1, vout, keep_history=True)
+        vin, vout = vout, vin
+    e2e_s = time.perf_counter() - t0
+    line = {"metric": "bidomain node-steps/s (FP64, null space of constant phi_e)",
+            "value": n * args.steps / (ms / 1e3), "unit": "node-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "2D LR91 forward-Euler sheet 1x1 cm h=0.01 (10,201 nodes), bidomain, "
+                                   "sigma_i (1.75, 0.19), sigma_e (7.0, 2.365)", "dt_ode_ms": 0.01,
+                       "dt_pde_ms": 0.1, "solver": "CG+Jacobi rtol 1e-8, null space of constant phi_e",
+                       "t_start_ms": args.t_start_ms, "l2": "flushed (256 MB write) before every timed step"},
+            "mean_cg_iterations": its / args.steps,
+            "e2e": {"value": n * args.steps / e2e_s, "unit": "node-steps/s", "h2d_bytes_per_step": 8 * n,
+                    "d2h_bytes_per_step": 8 * n}}
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+
+        threads = os.cpu_count() or 1
+        O.lib().orc_set_threads(threads)
+        ocfg = O.Config(O.LR91, O.FE, 0.01, 0.1, 1400.0, 1.0, O.PC_JACOBI, 0, 1e-8, 0, 10000)
+        sig_i = np.tile(np.asarray(si), (conn.shape[0], 1))
+        o = O.Tissue(ocfg, dim, xyz, conn, sig_i, sid, [O.simple(-5e5, 0.5, 0.0)])
+        o.set_bidomain(xyz, conn, sig_i, np.tile(np.asarray(se), (conn.shape[0], 1)))
+        o.step(start)
+        k, c0 = 0, time.perf_counter()
+        while time.perf_counter() - c0 < args.cpu_seconds and k < 50:
+            o.step(1)
+            k += 1
+        dt = time.perf_counter() - c0
+        line["cpu_baseline"] = {"value": n * k / dt, "unit": "node-steps/s", "cores": threads, "kind": "port",
+                                "sample": f"{k} PDE steps of the sheet from t = {args.t_start_ms:g} ms, {dt:.1f} s, "
+                                          f"FP64, {threads} threads"}
+    return line
+
+
 def aggregate(dist, device, ms_step, e2e_s, n, steps, world):
     """Whole-job figures of N replicas: the max over ranks of the device step time and of
     the end-to-end time (a collective on `device`: cuda for NCCL, cpu for gloo), then
@@ -547,7 +624,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tt06_slab_3d",
-                    choices=sorted(WORKLOADS) + ["tt06_population", "lr91_cable_adjoint", "lr91_mixed_population"])
+                    choices=sorted(WORKLOADS) + ["tt06_population", "lr91_cable_adjoint", "lr91_mixed_population",
+                                                  "lr91_bidomain_sheet_2d"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--t-start-ms", type=float, default=10.0,
@@ -600,6 +678,9 @@ def main():
         return
     if args.workload == "lr91_mixed_population":
         print(json.dumps(run_mixed(args)), flush=True)
+        return
+    if args.workload == "lr91_bidomain_sheet_2d":
+        print(json.dumps(run_bidomain(args)), flush=True)
         return
     rank, world, local, dist = dist_setup(args)
     wl = WORKLOADS[args.workload]

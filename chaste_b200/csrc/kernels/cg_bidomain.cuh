@@ -11,8 +11,12 @@
 // Jacobi or no preconditioner.  Without fixed phi_e nodes B is singular and the solve
 // carries the null space of constant phi_e (AbstractBidomainSolver::GenerateNullBasis,
 // AbstractBidomainSolver.cpp:112-134): as PETSc's KSP_PCApply does, every
-// preconditioned vector has its component along e = (0, 1/sqrt(n), 0, 1/sqrt(n), ...)
-// removed, which takes one grid reduction for the coefficient before the norms.
+// preconditioned vector z has its component along e = (0, 1/sqrt(n), 0, 1/sqrt(n), ...)
+// removed, z' = z - c e with c = z.e.  Inside the iteration the kernel keeps z as the
+// preconditioner left it and c beside it: the norms follow from sums taken in the same
+// grid reduction (z'.z' = z.z - c^2, z'.r = z.r - c (e.r), since e.e = 1), and the next
+// operator application and direction update use z' = z - c e entry by entry, so the
+// projection costs no extra reduction.
 // Fixed phi_e nodes are identity rows and columns of B (zero right-hand side), set on
 // the host.  The operator is B's CSR (rows 2i and 2i+1 share node i's pattern).
 #pragma once
@@ -116,18 +120,26 @@ __device__ void cg_bidomain_body(const CgArgs& a, const BidoArgs& b, unsigned& r
     if (dp >= a.dtol * rnorm0) return bido_finish(a, b, step, 0, kStatusCgDiverged);
 
     double betaold = 0.0;
+    double c = 0.0;   // null-space coefficient of the stored z (zero: the z above is projected)
     int it = 0;
     for (; it < a.maxit; ++it) {
         if (beta == 0.0) return bido_finish(a, b, step, it + 1, 0);
         const double bc = it == 0 ? 0.0 : beta / betaold;
         const bool first = it == 0;
-        // ---- p = z + bc p ; B p = B z + bc B p ; p . B p
+        const double ce = c * inv;   // z' = z - ce on the phi_e rows
+        // ---- p = z' + bc p ; B p = B z' + bc B p ; p . B p
         {
             double v[1] = {0};
             for (int i = t0; i < n2; i += stride) {
-                const double bz = csr_row<double, double>(b.rp, b.ci, b.val, i, b.z);
+                double bz = 0.0;
+                const int e = b.rp[i + 1];
+                for (int k = b.rp[i]; k < e; ++k) {
+                    const int j = b.ci[k];
+                    bz += b.val[k] * ((j & 1) ? b.z[j] - ce : b.z[j]);
+                }
+                const double zi = (i & 1) ? b.z[i] - ce : b.z[i];
                 const double qi = first ? bz : bz + bc * b.q[i];
-                const double pi = first ? b.z[i] : b.z[i] + bc * b.p[i];
+                const double pi = first ? zi : zi + bc * b.p[i];
                 b.q[i] = qi;
                 b.p[i] = pi;
                 v[0] += pi * qi;
@@ -137,43 +149,27 @@ __device__ void cg_bidomain_body(const CgArgs& a, const BidoArgs& b, unsigned& r
         const double dpi = res[0];
         if (!(dpi > 0.0)) return bido_finish(a, b, step, it + 1, isfinite(dpi) ? kStatusCgDiverged : kStatusNaN);
         const double alpha = beta / dpi;
-        // ---- u += alpha p ; r -= alpha B p ; z = B r (and its null-space coefficient)
-        double zz = 0.0, zr = 0.0;
+        // ---- u += alpha p ; r -= alpha B p ; z = B r; z.z, z.r and the null-space sums
         {
-            double v[2] = {0, 0};
+            double v[4] = {0, 0, 0, 0};
             for (int i = t0; i < n2; i += stride) {
                 b.u[i] += alpha * b.p[i];
                 const double ri = b.r[i] - alpha * b.q[i];
                 b.r[i] = ri;
                 const double zi = bido_pc(b, i, ri);
                 b.z[i] = zi;
-                if (b.nullspace) {
-                    if (i & 1) v[0] += zi * inv;
-                } else {
-                    v[0] += zi * zi;
-                    v[1] += zi * ri;
-                }
-            }
-            if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
-            zz = res[0];
-            zr = res[1];
-        }
-        if (b.nullspace) {
-            const double c = res[0];
-            double v[2] = {0, 0};
-            for (int i = t0; i < n2; i += stride) {
-                double zi = b.z[i];
-                if (i & 1) {
-                    zi -= c * inv;
-                    b.z[i] = zi;
-                }
                 v[0] += zi * zi;
-                v[1] += zi * b.r[i];
+                v[1] += zi * ri;
+                if (i & 1) {
+                    v[2] += zi * inv;
+                    v[3] += ri * inv;
+                }
             }
-            if (!grid_reduce<2>(v, red, a.gs, a.partials, res, a.status, round)) return;
-            zz = res[0];
-            zr = res[1];
+            if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
         }
+        c = b.nullspace ? res[2] : 0.0;
+        const double zz = fmax(res[0] - c * c, 0.0);
+        const double zr = res[1] - c * (b.nullspace ? res[3] : 0.0);
         dp = sqrt(zz);
         if (!isfinite(dp)) return bido_finish(a, b, step, it + 1, kStatusNaN);
         if (dp <= ttol) return bido_finish(a, b, step, it + 1, 0);
