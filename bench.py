@@ -630,7 +630,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--t-start-ms", type=float, default=10.0,
                     help="simulated time reached, untimed, before the warm-up and timed steps")
-    ap.add_argument("--profile", choices=["fp64", "mixed", "population"],
+    ap.add_argument("--profile", choices=["fp64", "mixed", "population", "runs"],
                     help="only build the workload's tissue in this precision, advance it to --t-start-ms and "
                          "take --steps steps with an L2 flush before each (the program the ncu captures in "
                          "profiles/ run)")
@@ -649,6 +649,22 @@ def main():
         b = N.CellBatch(N.MODEL_TT06, rng.integers(1, 21, size=8192).astype(np.int32), params)
         tpb = b.autotune(steps=args.steps)
         print(json.dumps({"profile": "population", "threads_per_block": tpb, "shape": b.launch_shape()}), flush=True)
+        return
+    if args.profile == "runs":
+        # the mixed population's launch shapes for --steps steps of every run (cg_runs_autotune),
+        # the program the runs-kernel ncu capture runs
+        from chaste_b200 import _native as N
+        from chaste_b200 import fitting as F
+        from chaste_b200.build import build_native
+
+        build_native()
+        stim, cells, cables = mixed_population_runs(N, F, np.random.default_rng(20261204))
+        pop = N.RunPopulation(N.MODEL_LR91)
+        for steps, p in cells:
+            pop.add_cell(N.ODE_RUSH_LARSEN, steps, 0.01, 100, p, stim)
+        for cfg, p, pr in cables:
+            pop.add_cable(cfg, p, pr, 10)
+        print(json.dumps({"profile": "runs", "shape": pop.autotune(steps=args.steps)}), flush=True)
         return
     if args.profile:
         import torch
