@@ -498,6 +498,79 @@ class ModelEmitter:
                 stack.extend(_free(self.live[s_]))
         return out
 
+    def _hoist_voltage_terms(self, outs):
+        """Split the per-substep terms (the expressions `outs` of the states that are not
+        voltage-only gates) for a clamped voltage: every maximal subexpression that
+        depends on V and the parameters alone and holds an exponential, logarithm,
+        power, quotient or piecewise branch becomes a voltage term vt[k], computed once
+        per PDE step.  Returns (terms, live, outs): the hoisted expressions in order, the
+        live definitions with the terms substituted, and the substituted outputs."""
+        V = self.V
+        fixed = set(self.psyms) | {V}
+        if getattr(self, "ueps", None) is not None:
+            fixed.add(self.ueps)
+        needed = self._needed(outs)
+        deps = {s_: self._state_deps([self.live[s_]]) for s_ in needed}
+        vonly = {s_ for s_ in needed if deps[s_] == {V}}
+        fixed |= {s_ for s_ in needed if not deps[s_]}   # constants: no state, no voltage
+
+        def is_vonly(e):
+            # depends on V (directly or through a voltage-only variable) and on nothing
+            # that changes between substeps; constant subexpressions stay for the compiler
+            free = _free(e)
+            return all(x in fixed or x in vonly for x in free) and any(x == V or x in vonly for x in free)
+
+        def costly(e):
+            if e.has(sp.exp) or e.has(sp.log) or e.has(sp.Piecewise):
+                return True
+            return any(not (a.exp.is_Integer and a.exp > 0) for a in e.atoms(sp.Pow))
+
+        terms, memo = [], {}
+
+        def term(e):
+            if e not in memo:
+                memo[e] = sp.Symbol(f"__vt{len(terms)}", real=True)
+                terms.append((memo[e], e))
+            return memo[e]
+
+        def rec(e):
+            if e.is_Atom:
+                if e in vonly and costly(self._fold_expr(self.live[e])):
+                    return term(self._fold_expr(self.live[e]))
+                return e
+            if is_vonly(e) and costly(e):
+                return term(e)
+            args = [rec(a) for a in e.args]
+            if all(a is b for a, b in zip(args, e.args)):
+                return e
+            with sp.evaluate(False):
+                return e.func(*args)
+
+        live = {}
+        for s_ in needed:
+            e = self._fold_expr(self.live[s_])
+            live[s_] = e if (s_ in vonly and costly(e)) else rec(e)
+        new_outs = [rec(self._fold_expr(e)) for e in outs]
+        return terms, live, new_outs
+
+    def _body_from(self, live, outs, pr, indent="        "):
+        """Statements for the symbols of `live` (a substituted definition map) that the
+        expressions `outs` need, in dependency order."""
+        order, seen = [], set()
+
+        def visit(s_):
+            if s_ in seen or s_ not in live:
+                return
+            seen.add(s_)
+            for x in sorted(_free(live[s_]), key=str):
+                visit(x)
+            order.append(s_)
+
+        for e in outs:
+            for x in sorted(_free(e), key=str):
+                visit(x)
+        return [f"{indent}const T {self.cname(s_)} = {pr(live[s_])};" for s_ in order]
+
     # ------------------------------------------------------------------ emit
     def cname(self, s):
         if s == self.stim_arg:
@@ -692,6 +765,43 @@ class ModelEmitter:
                 A(f"        rate[{i}] = {pr(self._fold_expr(h))};")
             else:
                 A(f"        rate[{i}] = {pr(self._fold_expr(self.odes[s_]))};")
+        A("    }")
+        # ---- the same split once more: the voltage-only parts of those terms, once per PDE step
+        r_outs = []
+        for s_ in self.states:
+            if s_ in vonly:
+                continue
+            r_outs += list(self.rl[s_]) if s_ in self.rl else [self.odes[s_]]
+        terms, live_vt, outs_vt = self._hoist_voltage_terms(r_outs)
+        for k, (sym, _) in enumerate(terms):
+            names[sym] = f"vt[{k}]"
+        A("    // The subexpressions of rl_terms_states that depend on the voltage and the")
+        A("    // parameters alone and hold an exponential, logarithm, power, quotient or branch:")
+        A("    // with V clamped over a PDE step they are computed once (rl_vterms) and the")
+        A("    // substeps take them from vt (rl_terms_states_vt, the same terms otherwise).")
+        A(f"    static constexpr int kNumVTerms = {len(terms)};")
+        A("    template <typename T>")
+        A("    CHB_HD static void rl_vterms(const T* __restrict__ y, const T* __restrict__ p, T* __restrict__ vt) {")
+        A("        (void)y; (void)p; (void)vt;")
+        lines.extend(self._body([e for _, e in terms], pr))
+        for k, (_, e) in enumerate(terms):
+            A(f"        vt[{k}] = {pr(e)};")
+        A("    }")
+        A("    template <typename T>")
+        A("    CHB_HD static void rl_terms_states_vt(const T* __restrict__ y, T stim, T cm,")
+        A("                                          const T* __restrict__ p, const T* __restrict__ vt,")
+        A("                                          T* __restrict__ rate, T* __restrict__ inf) {")
+        A("        (void)stim; (void)cm; (void)p; (void)vt; (void)inf;")
+        lines.extend(self._body_from(live_vt, outs_vt, pr))
+        q = iter(outs_vt)
+        for i, s_ in enumerate(self.states):
+            if s_ in vonly:
+                continue
+            if s_ in self.rl:
+                A(f"        inf[{i}] = {pr(next(q))};")
+                A(f"        rate[{i}] = {pr(next(q))};")
+            else:
+                A(f"        rate[{i}] = {pr(next(q))};")
         A("    }")
         A("")
         # ---- iionic

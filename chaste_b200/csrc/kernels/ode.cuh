@@ -157,8 +157,8 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
             }
         } else {
             // Rush-Larsen: the voltage-only gates' terms once per PDE step (V is clamped)
-            T vinf[S], vfac[S];
-            if (METHOD == 1) rl_freeze_voltage_terms<M, T>(y, p, (T)a.dt_ode, vinf, vfac);
+            T vinf[S], vfac[S], vt[M::kNumVTerms > 0 ? M::kNumVTerms : 1];
+            if (METHOD == 1) rl_freeze_voltage_terms<M, T>(y, p, (T)a.dt_ode, vinf, vfac, vt);
             DevTimeStepper ts(t0, t1, a.dt_ode);
             while (!ts.at_end()) {
                 // cell stimulus in uA/cm^2 = tissue stimulus / Am (GetIntracellularAreaStimulus);
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
                 const double sv = stimulus_value(st, ts.time);
                 const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
                 if (METHOD == 1) {
-                    rl_step_except_voltage_frozen<M, T>(y, s, cm, p, (T)a.dt_ode, vinf, vfac);
+                    rl_step_except_voltage_frozen<M, T>(y, s, cm, p, (T)a.dt_ode, vinf, vfac, vt);
                 } else if (METHOD == 3) {
                     grl1_step<M, T, false>(y, s, cm, p, (T)(ts.next - ts.time));
                 } else if (METHOD == 4) {

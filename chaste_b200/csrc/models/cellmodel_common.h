@@ -150,22 +150,25 @@ CHB_UNROLL
 // The same Rush-Larsen step over the substeps of one PDE step, with the terms of the
 // voltage-only states (Model::rl_voltage_only) taken out of the substep loop: V is
 // clamped, so their inf and exp(rate*dt) are the values rl_step_except_voltage would
-// recompute at every substep.  rl_freeze_voltage_terms forms them once; each substep
-// then evaluates only the terms of the other states.
+// recompute at every substep.  rl_freeze_voltage_terms forms them once, together with
+// the voltage-only subexpressions of the other states' terms (Model::rl_vterms); each
+// substep then evaluates only what depends on the other states.
 template <class Model, typename T>
-CHB_HD void rl_freeze_voltage_terms(const T* y, const T* p, T dt, T* vinf, T* vfac) {
+CHB_HD void rl_freeze_voltage_terms(const T* y, const T* p, T dt, T* vinf, T* vfac, T* vt) {
     T rate[Model::kNumStates];
     Model::template rl_terms_voltage<T>(y, p, rate, vinf);
 CHB_UNROLL
     for (int i = 1; i < Model::kNumStates; ++i)
         if (Model::rl_voltage_only(i)) vfac[i] = m_exp(rate[i] * dt);
+    Model::template rl_vterms<T>(y, p, vt);
 }
 
 template <class Model, typename T>
-CHB_HD void rl_step_except_voltage_frozen(T* y, T stim, T cm, const T* p, T dt, const T* vinf, const T* vfac) {
+CHB_HD void rl_step_except_voltage_frozen(T* y, T stim, T cm, const T* p, T dt, const T* vinf, const T* vfac,
+                                          const T* vt) {
     T rate[Model::kNumStates];
     T inf[Model::kNumStates];
-    Model::template rl_terms_states<T>(y, stim, cm, p, rate, inf);
+    Model::template rl_terms_states_vt<T>(y, stim, cm, p, vt, rate, inf);
 CHB_UNROLL
     for (int i = 1; i < Model::kNumStates; ++i) {
         if (Model::rl_voltage_only(i)) {

@@ -174,6 +174,38 @@ struct LuoRudy1991 {
         rate[0] = ((m_divk((-T(1.0)), T(1.0), T(1.0)))*(v_membrane__I_stim + v_fast_sodium_current__i_Na + v_slow_inward_current__i_si + v_time_dependent_potassium_current__i_K + v_time_independent_potassium_current__i_K1 + v_plateau_potassium_current__i_Kp + v_background_current__i_b));
         rate[7] = (((m_divk((-T(0.0001)), T(1.0), T(1.0)))*v_slow_inward_current__i_si) + (T(0.07)*(T(0.0001) - y[7])));
     }
+    // The subexpressions of rl_terms_states that depend on the voltage and the
+    // parameters alone and hold an exponential, logarithm, power, quotient or branch:
+    // with V clamped over a PDE step they are computed once (rl_vterms) and the
+    // substeps take them from vt (rl_terms_states_vt, the same terms otherwise).
+    static constexpr int kNumVTerms = 3;
+    template <typename T>
+    CHB_HD static void rl_vterms(const T* __restrict__ y, const T* __restrict__ p, T* __restrict__ vt) {
+        (void)y; (void)p; (void)vt;
+        const T v_time_independent_potassium_current_K1_gate__alpha_K1 = (m_div(T(1.02), (T(1.0) + m_exp((T(0.2385)*((y[0] - (-T(87.8929017138025))) - T(59.215)))))));
+        const T v_time_independent_potassium_current_K1_gate__beta_K1 = (m_div(((T(0.49124)*m_exp((T(0.08032)*((y[0] + T(5.476)) - (-T(87.8929017138025)))))) + (T(1.0)*m_exp((T(0.06175)*(y[0] - (-T(87.8929017138025) + T(594.31))))))), (T(1.0) + m_exp(((-T(0.5143))*((y[0] - (-T(87.8929017138025))) + T(4.753)))))));
+        vt[0] = (m_div(T(1.0), (T(1.0) + m_exp((m_divk((T(7.488) - y[0]), T(5.98), T(0.16722408026755853)))))));
+        vt[1] = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? ((m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0))))))) + (m_div((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*((m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0))))))) - (m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))), (T(2.0)*(chb::singularity_offset<T>()*T(1.0)))))) : (m_div((T(2.837)*(m_exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0))), ((y[0] + T(77.0))*m_exp((T(0.04)*(y[0] + T(35.0)))))))) : T(1.0));
+        vt[2] = (m_div(v_time_independent_potassium_current_K1_gate__alpha_K1, (v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1)));
+    }
+    template <typename T>
+    CHB_HD static void rl_terms_states_vt(const T* __restrict__ y, T stim, T cm,
+                                          const T* __restrict__ p, const T* __restrict__ vt,
+                                          T* __restrict__ rate, T* __restrict__ inf) {
+        (void)stim; (void)cm; (void)p; (void)vt; (void)inf;
+        const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
+        const T v_fast_sodium_current__i_Na = ((T(23.0)*p[0])*(y[1]*y[1]*y[1])*y[2]*y[3]*(y[0] - T(54.79446393509185)));
+        const T v_membrane__I_stim = stim;
+        const T v_plateau_potassium_current__i_Kp = ((T(0.0183)*p[4])*vt[0]*(y[0] - (-T(87.8929017138025))));
+        const T v_slow_inward_current__E_si = (T(7.7) - (T(13.0287)*m_log((m_divk(y[7], T(1.0), T(1.0))))));
+        const T v_slow_inward_current__i_si = ((T(0.09)*p[1])*y[4]*y[5]*(y[0] - v_slow_inward_current__E_si));
+        const T v_time_dependent_potassium_current__g_K__scaled = (T(0.282)*p[2]);
+        const T v_time_dependent_potassium_current__i_K = (v_time_dependent_potassium_current__g_K__scaled*y[6]*vt[1]*(y[0] - (-T(77.56758438531939))));
+        const T v_time_independent_potassium_current__g_K1__scaled = (T(0.6047)*p[3]);
+        const T v_time_independent_potassium_current__i_K1 = (v_time_independent_potassium_current__g_K1__scaled*vt[2]*(y[0] - (-T(87.8929017138025))));
+        rate[0] = ((m_divk((-T(1.0)), T(1.0), T(1.0)))*(v_membrane__I_stim + v_fast_sodium_current__i_Na + v_slow_inward_current__i_si + v_time_dependent_potassium_current__i_K + v_time_independent_potassium_current__i_K1 + v_plateau_potassium_current__i_Kp + v_background_current__i_b));
+        rate[7] = (((m_divk((-T(0.0001)), T(1.0), T(1.0)))*v_slow_inward_current__i_si) + (T(0.07)*(T(0.0001) - y[7])));
+    }
 
     // Total ionic current in uA/cm^2 (GetIIonic): the dV/dt currents without
     // the stimulus.

@@ -144,3 +144,42 @@ int main() {
                     str(src), "-o", str(exe)], check=True)
     worst = float(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
     assert worst <= 1e-5, worst
+
+
+def test_hoisted_voltage_terms_reproduce_the_substep_terms(tmp_path):
+    """rl_vterms + rl_terms_states_vt (the voltage-only subexpressions evaluated once per
+    PDE step) give rl_terms_states' rates and limits for voltages across the action
+    potential, the GHK singular points included, in double to 1e-12 relative."""
+    src = tmp_path / "h.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <cmath>
+#include "lr91.h"
+#include "tt06.h"
+template <class M> double worst() {
+    double w = 0.0;
+    const double vs[] = {-90.0, -77.0, -47.13, -20.0, 0.0, 15.0, 15.0000001, 40.0};
+    for (double v : vs) {
+        double y[M::kNumStates], p[M::kNumParams], r1[M::kNumStates], i1[M::kNumStates];
+        double r2[M::kNumStates], i2[M::kNumStates], vt[M::kNumVTerms > 0 ? M::kNumVTerms : 1];
+        for (int i = 0; i < M::kNumStates; ++i) { y[i] = M::kInitialStates[i]; r1[i] = r2[i] = i1[i] = i2[i] = 0.0; }
+        for (int i = 0; i < M::kNumParams; ++i) p[i] = 1.0 + 0.05 * i;
+        y[0] = v;
+        M::template rl_terms_states<double>(y, -3.0, 1.0, p, r1, i1);
+        M::template rl_vterms<double>(y, p, vt);
+        M::template rl_terms_states_vt<double>(y, -3.0, 1.0, p, vt, r2, i2);
+        for (int i = 0; i < M::kNumStates; ++i) {
+            w = std::fmax(w, std::fabs(r1[i] - r2[i]) / std::fmax(std::fabs(r1[i]), 1e-30));
+            w = std::fmax(w, std::fabs(i1[i] - i2[i]) / std::fmax(std::fabs(i1[i]), 1e-30));
+        }
+    }
+    return w;
+}
+int main() { std::printf("%.3e %.3e\n", worst<chb::LuoRudy1991>(), worst<chb::TenTusscher2006Epi>()); return 0; }
+''')
+    exe = tmp_path / "h"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "chaste_b200", "csrc", "models"),
+                    str(src), "-o", str(exe)], check=True)
+    lr, tt = (float(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                               text=True).stdout.split())
+    assert lr <= 1e-12 and tt <= 1e-12, (lr, tt)
