@@ -68,6 +68,7 @@ class Stats(C.Structure):
         ("refinement_sweeps", C.c_int), ("operator_kind", C.c_int), ("status_bits", C.c_int),
         ("ms_last_call", C.c_double), ("pipelined_nodes_per_thread", C.c_int), ("cg_blocks", C.c_int),
         ("inner_preconditioner", C.c_int), ("inner_line_segment", C.c_int),
+        ("step_graph", C.c_int), ("host_call_graph", C.c_int), ("capture_error", C.c_int),
     ]
 
 

@@ -29,6 +29,17 @@ namespace {
 constexpr int kRing = 4096;   // iteration-count history per context
 constexpr int kHostChunks = 8;   // cg_step_host: pieces of V copied in while the ODE runs on the earlier ones
 
+constexpr int kHostGraphs = 4;   // cg_step_host calls kept as graphs (distinct buffer pairs)
+
+// One cg_step_host call captured as a graph: its host buffers are part of it.
+struct HostGraph {
+    const double* in;
+    double* out;
+    int n_steps;
+    bool keep;
+    cudaGraphExec_t exec;
+};
+
 // Status word, step counter and iteration ring read back after each call, copied
 // together into page-locked memory so one synchronisation covers them.
 struct HostControl {
@@ -154,7 +165,12 @@ struct cg_ctx {
     // cg_step_host: a copy stream, one event per chunk of V, and page-locked control words
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t chunk_ev[kHostChunks] = {};
+    cudaEvent_t fork_ev = nullptr;
     HostControl* h_ctl = nullptr;
+    HostGraph host_graphs[kHostGraphs] = {};   // replayable calls, by their host buffers
+    int host_graph_next = 0;
+    bool host_call_graph = false;   // the last cg_step_host call was a graph replay
+    int capture_error = 0;          // cudaError_t of the last failed capture
 
     bool mixed() const { return cfg.precision == CG_PRECISION_MIXED; }
     size_t real_size() const { return mixed() ? sizeof(float) : sizeof(double); }
@@ -162,10 +178,17 @@ struct cg_ctx {
 
 namespace {
 
+// The CUDA error behind the calling thread's last CG_ERR_CUDA (for cg_stats).
+inline cudaError_t& last_cuda_error() {
+    static thread_local cudaError_t e = cudaSuccess;
+    return e;
+}
+
 #define CG_CUDA(call)                                 \
     do {                                              \
         cudaError_t e_ = (call);                      \
         if (e_ != cudaSuccess) {                      \
+            last_cuda_error() = e_;                   \
             cudaGetLastError();                       \
             return CG_ERR_CUDA;                       \
         }                                             \
@@ -379,6 +402,9 @@ int cg_destroy(cg_ctx* c) {
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (cudaEvent_t e : c->chunk_ev)
         if (e) cudaEventDestroy(e);
+    for (HostGraph& g : c->host_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1379,10 +1405,123 @@ cudaError_t launch_step(cg_ctx* c) {
     return cudaGetLastError();
 }
 
+// Everything one cg_step_host call puts on the stream after ev0: V in (in pieces the
+// first step's ODE starts on as they arrive), the steps, ev1, V out and the control
+// words.  In a capture (`capture`) the copy stream forks from the captured stream and
+// the steps are plain launches.
+int enqueue_host_call(cg_ctx* c, const double* v_in, int n_steps, double* v_out, int keep_history, bool capture) {
+    const size_t n = (size_t)c->n;
+    int k0 = 0;
+    if (v_in) {
+        if (n_steps > 0 && !split(c) && !c->svi) {
+            CG_CUDA(cudaEventRecord(c->fork_ev, c->stream));
+            CG_CUDA(cudaStreamWaitEvent(c->copy_stream, c->fork_ev, 0));
+            const int per = (int)((n + kHostChunks - 1) / kHostChunks);
+            for (int k = 0; k < kHostChunks; ++k) {
+                const int lo = k * per, hi = (int)std::min(n, (size_t)lo + per);
+                if (lo >= hi) break;
+                CG_CUDA(cudaMemcpyAsync(c->d_V + lo, v_in + lo, (size_t)(hi - lo) * sizeof(double),
+                                        cudaMemcpyHostToDevice, c->copy_stream));
+                CG_CUDA(cudaEventRecord(c->chunk_ev[k], c->copy_stream));
+                CG_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[k], 0));
+                launch_odes(c, 0, lo, hi, keep_history == 0);
+            }
+            if (cudaGetLastError() != cudaSuccess || launch_solve(c) != cudaSuccess) {
+                cudaGetLastError();
+                return CG_ERR_CUDA;
+            }
+            out_after_step(c, c->steps + 1);
+            k0 = 1;
+        } else {
+            CG_CUDA(cudaMemcpyAsync(c->d_V, v_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            if (!keep_history && c->d_Vprev)
+                CG_CUDA(cudaMemcpyAsync(c->d_Vprev, c->d_V, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        }
+    }
+    for (int k = k0; k < n_steps; ++k) {
+        const cudaError_t e = (c->graph && !capture) ? cudaGraphLaunch(c->graph, c->stream) : launch_step(c);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return CG_ERR_CUDA;
+        }
+        out_after_step(c, c->steps + k + 1);
+    }
+    // in a capture the record must be an external one, so that each replay records it
+    CG_CUDA(capture ? cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal)
+                    : cudaEventRecord(c->ev1, c->stream));
+    if (v_out) CG_CUDA(cudaMemcpyAsync(v_out, c->d_V, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HostControl* h = c->h_ctl;
+    CG_CUDA(cudaMemcpyAsync(&h->status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CG_CUDA(cudaMemcpyAsync(&h->step, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    CG_CUDA(cudaMemcpyAsync(h->ring, c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return CG_OK;
+}
+
+// NULL, or page-locked (or mapped) host memory: a copy from it can be captured.
+bool pinned(const void* p) {
+    if (!p) return true;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+HostGraph* add_host_graph(cg_ctx* c, const double* in, double* out, int n_steps, int keep, cudaGraphExec_t exec);
+
+// The call captured as a graph, or null when the capture failed (the error is kept in
+// capture_error and the call runs as plain launches).
+HostGraph* capture_host_call(cg_ctx* c, const double* v_in, int n_steps, double* v_out, int keep_history) {
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    int rc = CG_OK;
+    if (e == cudaSuccess) {
+        rc = enqueue_host_call(c, v_in, n_steps, v_out, keep_history, true);
+        const cudaError_t le = cudaGetLastError();
+        e = cudaStreamEndCapture(c->stream, &graph);
+        if (e == cudaSuccess && le != cudaSuccess) e = le;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess && rc == CG_OK) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess || rc != CG_OK) {
+        c->capture_error = e != cudaSuccess ? (int)e : (int)last_cuda_error();
+        cudaGetLastError();
+        return nullptr;
+    }
+    return add_host_graph(c, v_in, v_out, n_steps, keep_history, exec);
+}
+
+HostGraph* find_host_graph(cg_ctx* c, const double* in, double* out, int n_steps, int keep) {
+    for (HostGraph& g : c->host_graphs)
+        if (g.exec && g.in == in && g.out == out && g.n_steps == n_steps && g.keep == (keep != 0)) return &g;
+    return nullptr;
+}
+
+HostGraph* add_host_graph(cg_ctx* c, const double* in, double* out, int n_steps, int keep, cudaGraphExec_t exec) {
+    HostGraph& g = c->host_graphs[c->host_graph_next];
+    c->host_graph_next = (c->host_graph_next + 1) % kHostGraphs;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = HostGraph{in, out, n_steps, keep != 0, exec};
+    return &g;
+}
+
+void drop_host_graphs(cg_ctx* c) {
+    for (HostGraph& g : c->host_graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = HostGraph{};
+    }
+}
+
 // The copy stream, chunk events and page-locked control words, made on first use.
 int ensure_host_path(cg_ctx* c) {
     if (c->h_ctl) return CG_OK;
     if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return CG_ERR_CUDA;
+    }
+    if (cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         return CG_ERR_CUDA;
     }
@@ -1412,6 +1551,7 @@ int build_graph(cg_ctx* c) {
     cudaError_t le = launch_step(c);
     cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
     if (le != cudaSuccess || ce != cudaSuccess || !g) {
+        c->capture_error = (int)(le != cudaSuccess ? le : ce);
         cudaGetLastError();
         if (g) cudaGraphDestroy(g);
         return CG_ERR_CUDA;
@@ -1419,6 +1559,7 @@ int build_graph(cg_ctx* c) {
     cudaError_t ie = cudaGraphInstantiate(&c->graph, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
+        c->capture_error = (int)ie;
         cudaGetLastError();
         c->graph = nullptr;
         return CG_ERR_CUDA;
@@ -1484,56 +1625,30 @@ int cg_step_host(cg_ctx* c, const double* v_in, int n_steps, double* v_out, int 
     if (c->graph_dirty) {
         if (build_graph(c) != CG_OK) c->graph = nullptr;   // plain launches instead
         c->graph_dirty = false;
+        drop_host_graphs(c);   // their kernel arguments may be out of date too
     }
     if (c->out_max && c->out_count + out_frames_added(c, n_steps) > c->out_max) return CG_ERR_NOMEM;
     CG_TRY(ensure_host_path(c));
-    const size_t n = (size_t)c->n;
     CG_CUDA(cudaEventRecord(c->ev0, c->stream));
-    int k0 = 0;
-    if (v_in) {
-        if (n_steps > 0 && !split(c) && !c->svi) {
-            // the first step's ODE runs on each piece of V as soon as it has arrived
-            CG_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev0, 0));
-            const int per = (int)((n + kHostChunks - 1) / kHostChunks);
-            for (int k = 0; k < kHostChunks; ++k) {
-                const int lo = k * per, hi = (int)std::min(n, (size_t)lo + per);
-                if (lo >= hi) break;
-                CG_CUDA(cudaMemcpyAsync(c->d_V + lo, v_in + lo, (size_t)(hi - lo) * sizeof(double),
-                                        cudaMemcpyHostToDevice, c->copy_stream));
-                CG_CUDA(cudaEventRecord(c->chunk_ev[k], c->copy_stream));
-                CG_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[k], 0));
-                launch_odes(c, 0, lo, hi, keep_history == 0);
-            }
-            if (cudaGetLastError() != cudaSuccess || launch_solve(c) != cudaSuccess) {
-                cudaGetLastError();
-                return CG_ERR_CUDA;
-            }
-            out_after_step(c, c->steps + 1);
-            k0 = 1;
-        } else {
-            CG_CUDA(cudaMemcpyAsync(c->d_V, v_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-            if (!keep_history && c->d_Vprev)
-                CG_CUDA(cudaMemcpyAsync(c->d_Vprev, c->d_V, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-        }
+    // a call with page-locked buffers and no printing-step output is replayed from a
+    // graph of the whole call (copies, launches, read-back), built on its first use
+    const bool replay = (v_in || v_out) && c->out_every == 0 && pinned(v_in) && pinned(v_out);
+    HostGraph* g = replay ? find_host_graph(c, v_in, v_out, n_steps, keep_history) : nullptr;
+    if (replay && !g) g = capture_host_call(c, v_in, n_steps, v_out, keep_history);
+    c->host_call_graph = g != nullptr;
+    if (g) {
+        CG_CUDA(cudaGraphLaunch(g->exec, c->stream));
+    } else {
+        CG_TRY(enqueue_host_call(c, v_in, n_steps, v_out, keep_history, false));
     }
-    for (int k = k0; k < n_steps; ++k) {
-        const cudaError_t e = c->graph ? cudaGraphLaunch(c->graph, c->stream) : launch_step(c);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return CG_ERR_CUDA;
-        }
-        out_after_step(c, c->steps + k + 1);
-    }
-    CG_CUDA(cudaEventRecord(c->ev1, c->stream));
-    if (v_out) CG_CUDA(cudaMemcpyAsync(v_out, c->d_V, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    HostControl* h = c->h_ctl;
-    CG_CUDA(cudaMemcpyAsync(&h->status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CG_CUDA(cudaMemcpyAsync(&h->step, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
-    CG_CUDA(cudaMemcpyAsync(h->ring, c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CG_CUDA(cudaStreamSynchronize(c->stream));
     float ms = 0.0f;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) != cudaSuccess) {
+        cudaGetLastError();   // leave no error behind for the next call's launch checks
+        ms = 0.0f;
+    }
     c->ms_last = ms;
+    HostControl* h = c->h_ctl;
     const long long dstep = h->step;
     const long long from = std::max(c->steps, dstep - kRing);
     for (long long s = from; s < dstep; ++s) {
@@ -1667,6 +1782,9 @@ int cg_get_stats(cg_ctx* c, cg_stats* s) {
     s->cg_blocks = c->cg_blocks;
     s->inner_preconditioner = !c->mixed() ? -1 : (c->line_pc ? CG_INNER_PC_LINE : CG_INNER_PC_JACOBI);
     s->inner_line_segment = c->line_pc ? c->line_segment : 0;
+    s->step_graph = c->graph ? 1 : 0;
+    s->host_call_graph = c->host_call_graph ? 1 : 0;
+    s->capture_error = c->capture_error;
     if (c->have_cells && c->steps > 0) {
         CG_CUDA(cudaSetDevice(c->device));
         CG_CUDA(cudaMemcpy(&s->last_cg_iterations, c->d_ring + ((c->steps - 1) % kRing), sizeof(int),

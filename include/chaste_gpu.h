@@ -122,6 +122,10 @@ typedef struct {
                                       (CG_INNER_PC_JACOBI on CSR meshes); FP64: -1 */
     int inner_line_segment;        /* x-line preconditioner: nodes per segment its x-lines are cut
                                       to (32, a warp's nodes); 0 without it */
+    int step_graph;                /* 1: cg_step replays a CUDA graph of the step, 0: plain launches */
+    int host_call_graph;           /* 1: the last cg_step_host call was replayed from a graph */
+    int capture_error;             /* cudaError_t of the last graph capture that failed (0: none);
+                                      the call then ran as plain launches */
 } cg_stats;
 
 /* Fill cfg with Chaste's defaults (LR91, FE, dt 0.01, Am 1400, Cm 1, Jacobi, atol 2e-4). */
@@ -185,8 +189,11 @@ int cg_step(cg_ctx* ctx, int n_steps);
  * copied to v_out (may be NULL), with one synchronisation for the whole call.
  * keep_history = 1 declares that v_in continues the trajectory (the caller passes
  * back what the previous call returned), so the mixed solve keeps its extrapolated
- * initial guess; 0 treats v_in as new (as cg_set_voltage does).  Page-locked host
- * buffers make the copies DMA transfers. */
+ * initial guess; 0 treats v_in as new (as cg_set_voltage does).  With page-locked host
+ * buffers the copies are DMA transfers and, when no printing-step output is configured,
+ * the whole call is captured as a CUDA graph on its first use and replayed afterwards
+ * (the four most recent (v_in, v_out, n_steps, keep_history) combinations are kept;
+ * cg_stats.host_call_graph says whether the last call was a replay). */
 int cg_step_host(cg_ctx* ctx, const double* v_in, int n_steps, double* v_out, int keep_history);
 
 /* cg_step with device-side event timing per phase, launched kernel by kernel

@@ -467,3 +467,35 @@ def test_host_buffer_steps_match_device_steps(N, precision):
     assert np.array_equal(out, host.voltage())
     host.step_host(out, 0, None)
     assert np.array_equal(out, host.voltage())
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_host_buffer_steps_replayed_from_graphs(N, precision):
+    """With page-locked buffers cg_step_host replays each (v_in, v_out) pair's call from a
+    graph; two alternating buffer pairs reproduce the device-resident steps bit for bit,
+    and a change of the cells (new kernel arguments) drops the cached calls."""
+    import torch
+
+    case = dict(TC.TT06_3D)
+    dev, _ = TC.make_gpu(N, precision=precision, **case)
+    host, _ = TC.make_gpu(N, precision=precision, **case)
+    dev.step(3)
+    host.step(3)
+    a = torch.empty(host.n, dtype=torch.float64, pin_memory=True).numpy()
+    b = torch.empty(host.n, dtype=torch.float64, pin_memory=True).numpy()
+    host.voltage(out=a)
+    for _ in range(12):
+        dev.step(1)
+        host.step_host(a, 1, b, keep_history=True)
+        a, b = b, a
+        assert np.array_equal(a, dev.voltage())
+    assert host.stats().steps == dev.stats().steps
+    # new cells: both tissues restart from the same states, the cached calls are rebuilt
+    dev.set_cells()
+    host.set_cells()
+    dev.set_voltage(a)
+    for k in range(4):
+        dev.step(1)
+        host.step_host(a, 1, b, keep_history=k > 0)   # the first call declares V new, as set_voltage does
+        a, b = b, a
+    assert np.array_equal(a, dev.voltage())
