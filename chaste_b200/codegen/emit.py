@@ -787,9 +787,11 @@ class ModelEmitter:
         for k, (_, e) in enumerate(terms):
             A(f"        vt[{k}] = {pr(e)};")
         A("    }")
-        A("    template <typename T>")
+        A("    // vt is anything indexable: the array rl_vterms wrote, or an accessor that")
+        A("    // reads each term where it is used (a per-thread column of shared memory).")
+        A("    template <typename T, class VT = const T*>")
         A("    CHB_HD static void rl_terms_states_vt(const T* __restrict__ y, T stim, T cm,")
-        A("                                          const T* __restrict__ p, const T* __restrict__ vt,")
+        A("                                          const T* __restrict__ p, const VT& vt,")
         A("                                          T* __restrict__ rate, T* __restrict__ inf) {")
         A("        (void)stim; (void)cm; (void)p; (void)vt; (void)inf;")
         lines.extend(self._body_from(live_vt, outs_vt, pr))
@@ -894,8 +896,6 @@ def _emit_vjp(self, fname, outputs, wdoc, stim_zero=False):
     L.append(f"    CHB_HD static void {fname}(const T* __restrict__ y, T stim, T cm, const T* __restrict__ p,")
     L.append("                                const T* __restrict__ w, T* __restrict__ gy, T* __restrict__ gp) {")
     L.append("        (void)stim; (void)cm; (void)p; (void)w; (void)gy; (void)gp;")
-    if stim_zero:
-        L.append("        stim = T(0.0); (void)stim;")
     body, adj = _vjp_body(self, outputs, pr, stim_zero)
     L.extend(body)
     for i, st in enumerate(self.states):

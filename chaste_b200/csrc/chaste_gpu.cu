@@ -1130,6 +1130,21 @@ int upload_cells_t(cg_ctx* c, const double* init, const int* pset, const double*
     return CG_OK;
 }
 
+// One ode_kernel launch over the nodes [a.lo, a.hi) in the kernel's block shape
+// (c->ode_blocks counts 256-thread blocks, so the grid keeps the same thread budget), or
+// one operator-splitting half step over every node.
+template <class M, typename T, int METHOD>
+void launch_ode_kernel(cg_ctx* c, const OdeArgs<T>& a) {
+    if (a.half) {
+        ode_half_kernel<M, T, METHOD><<<c->ode_blocks, 256, 0, c->stream>>>(a);
+        return;
+    }
+    constexpr int tpb = OdeShape<M, T, METHOD>::kThreads;
+    const long long cap = (long long)c->ode_blocks * 256 / tpb;
+    const int blocks = (int)std::max(1LL, std::min(cap, ((long long)a.hi - a.lo + tpb - 1) / tpb));
+    ode_kernel<M, T, METHOD><<<blocks, tpb, 0, c->stream>>>(a);
+}
+
 template <class M, typename T>
 void launch_ode(cg_ctx* c, int half = 0, int lo = 0, int hi = -1, bool reset_history = false) {
     OdeArgs<T> a;
@@ -1137,7 +1152,6 @@ void launch_ode(cg_ctx* c, int half = 0, int lo = 0, int hi = -1, bool reset_his
     a.lo = lo;
     a.hi = hi < 0 ? c->n : hi;
     a.reset_history = reset_history ? 1 : 0;
-    const int blocks = (int)std::max(1LL, std::min((long long)c->ode_blocks, ((long long)a.hi - a.lo + 255) / 256));
     a.V = c->d_V;
     // the extrapolated guess replaces V^n in place, which splitting and SVI still need
     a.vprev = (c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING || c->svi) ? nullptr : c->d_Vprev;
@@ -1159,15 +1173,15 @@ void launch_ode(cg_ctx* c, int half = 0, int lo = 0, int hi = -1, bool reset_his
     a.act = c->d_act;
     a.act_threshold = c->cfg.activation_threshold;
     if (c->cfg.ode_method == CG_ODE_RUSH_LARSEN)
-        ode_kernel<M, T, 1><<<blocks, 256, 0, c->stream>>>(a);
+        launch_ode_kernel<M, T, 1>(c, a);
     else if (c->cfg.ode_method == CG_ODE_BACKWARD_EULER)
-        ode_kernel<M, T, 2><<<blocks, 256, 0, c->stream>>>(a);
+        launch_ode_kernel<M, T, 2>(c, a);
     else if (c->cfg.ode_method == CG_ODE_GRL1)
-        ode_kernel<M, T, 3><<<blocks, 256, 0, c->stream>>>(a);
+        launch_ode_kernel<M, T, 3>(c, a);
     else if (c->cfg.ode_method == CG_ODE_GRL2)
-        ode_kernel<M, T, 4><<<blocks, 256, 0, c->stream>>>(a);
+        launch_ode_kernel<M, T, 4>(c, a);
     else
-        ode_kernel<M, T, 0><<<blocks, 256, 0, c->stream>>>(a);
+        launch_ode_kernel<M, T, 0>(c, a);
 }
 
 CgArgs make_cg_args(cg_ctx* c) {

@@ -102,19 +102,37 @@ __device__ __forceinline__ void ode_half_step(const OdeArgs<T>& a, double t0, do
     }
 }
 
+// Launch shape of ode_kernel.  The FP64 Rush-Larsen step keeps its frozen terms (the
+// voltage-only gates' inf and exp(rate*dt), the voltage-only subexpressions) in a
+// per-thread column of shared memory instead of registers, and runs 128-thread blocks
+// capped at 128 registers, four blocks per SM: 16 resident warps per SM where 250+
+// registers left 8 (one step of 442,401 TT06 cells 0.455 -> 0.302 ms, bit for bit the
+// same states).  The other steps run 256-thread blocks, two per SM (at most 128
+// registers, which they fit without spilling), except the GRL2 steps and the other
+// FP64 steps of the larger models (more than 10 states), which keep the compiler's
+// register count: capped, they spill hundreds of bytes a thread.
 template <class M, typename T, int METHOD>
-__global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
+struct OdeShape {
+    static constexpr bool kColumn = METHOD == 1 && sizeof(T) == 8;
+    static constexpr int kThreads = kColumn ? 128 : 256;
+    static constexpr int kMinBlocks =
+        kColumn ? 4 : (METHOD == 4 || (sizeof(T) == 8 && M::kNumStates > 10)) ? 1 : 2;
+    static constexpr int kShared = kColumn ? FrozenSlots<M>::kSlots * kThreads : 1;
+};
+
+template <class M, typename T, int METHOD>
+__global__ void __launch_bounds__(OdeShape<M, T, METHOD>::kThreads, OdeShape<M, T, METHOD>::kMinBlocks)
+    ode_kernel(OdeArgs<T> a) {
+    using Shape = OdeShape<M, T, METHOD>;
     constexpr int S = M::kNumStates;
     constexpr int P = M::kNumParams;
+    // frozen-term columns, slot k of thread t at frozen[k * kThreads + t] (blockDim.x is at
+    // most kThreads: the launch bound rejects larger blocks)
+    __shared__ T frozen[Shape::kShared];
     if (*(volatile int*)a.status & ~kStatusStateRange) return;   // a failed step stops the run
-    // the second half step runs after the diffusion solve has advanced the step counter
-    const long long step = *a.step - (a.half == 2 ? 1 : 0);
+    const long long step = *a.step;
     const double t0 = (double)step * a.dt_pde;
     const double t1 = (double)(step + 1) * a.dt_pde;
-    if (a.half) {
-        ode_half_step<M, T, METHOD>(a, t0, t1);
-        return;
-    }
     const double dtinv = 1.0 / a.dt_pde;
     for (int i = a.lo + blockIdx.x * blockDim.x + threadIdx.x; i < a.hi; i += gridDim.x * blockDim.x) {
         T y[S];
@@ -155,6 +173,17 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
                 be_step<M, T>(y, s, cm, p, (T)a.dt_ode, false);
                 y[0] = (T)v;
             }
+        } else if constexpr (Shape::kColumn) {
+            // Rush-Larsen with the frozen terms in this thread's shared-memory column
+            T* column = frozen + threadIdx.x;
+            rl_freeze_voltage_terms_column<M, T, Shape::kThreads>(y, p, (T)a.dt_ode, column);
+            DevTimeStepper ts(t0, t1, a.dt_ode);
+            while (!ts.at_end()) {
+                const double sv = stimulus_value(st, ts.time);
+                const T s = sv == 0.0 ? T(0) : (T)(sv / a.am);
+                rl_step_except_voltage_column<M, T, Shape::kThreads>(y, s, cm, p, (T)a.dt_ode, column);
+                ts.advance();
+            }
         } else {
             // Rush-Larsen: the voltage-only gates' terms once per PDE step (V is clamped)
             T vinf[S], vfac[S], vt[M::kNumVTerms > 0 ? M::kNumVTerms : 1];
@@ -187,6 +216,18 @@ __global__ void __launch_bounds__(256) ode_kernel(OdeArgs<T> a) {
         a.zrhs[i] = (T)(a.am * a.cm * v * dtinv + F);
         if (a.check_range && !states_in_range<M, T>(y)) atomicOr(a.status, kStatusStateRange);
     }
+}
+
+// The operator-splitting half steps (a.half = 1 or 2) in a kernel of their own, so that
+// their register allocation does not weigh on ode_kernel's.
+template <class M, typename T, int METHOD>
+__global__ void __launch_bounds__(256) ode_half_kernel(OdeArgs<T> a) {
+    if (*(volatile int*)a.status & ~kStatusStateRange) return;   // a failed step stops the run
+    // the second half step runs after the diffusion solve has advanced the step counter
+    const long long step = *a.step - (a.half == 2 ? 1 : 0);
+    const double t0 = (double)step * a.dt_pde;
+    const double t1 = (double)(step + 1) * a.dt_pde;
+    ode_half_step<M, T, METHOD>(a, t0, t1);
 }
 
 }  // namespace chb

@@ -168,7 +168,7 @@ CHB_HD void rl_step_except_voltage_frozen(T* y, T stim, T cm, const T* p, T dt, 
                                           const T* vt) {
     T rate[Model::kNumStates];
     T inf[Model::kNumStates];
-    Model::template rl_terms_states_vt<T>(y, stim, cm, p, vt, rate, inf);
+    Model::template rl_terms_states_vt<T, const T*>(y, stim, cm, p, vt, rate, inf);
 CHB_UNROLL
     for (int i = 1; i < Model::kNumStates; ++i) {
         if (Model::rl_voltage_only(i)) {
@@ -180,6 +180,75 @@ CHB_UNROLL
         }
     }
 }
+
+// The frozen terms as slots of a per-thread column: the voltage-only states' inf
+// (slots [0, NV)), their exp(rate*dt) (slots [NV, 2 NV)) and the voltage-only
+// subexpressions (slots [2 NV, 2 NV + kNumVTerms)), NV the number of voltage-only
+// states.  Slot k of a thread lives at column[k * STRIDE].
+template <class Model>
+CHB_HD constexpr int frozen_slot(int i) {
+    int c = 0;
+    for (int j = 1; j < i; ++j) c += Model::rl_voltage_only(j) ? 1 : 0;
+    return c;
+}
+template <class Model>
+struct FrozenSlots {
+    static constexpr int kVoltageOnly = frozen_slot<Model>(Model::kNumStates);
+    static constexpr int kSlots = 2 * kVoltageOnly + Model::kNumVTerms;
+};
+
+#if defined(__CUDACC__)
+// Reads slot k of a shared-memory column where the model code uses it: the loads are
+// volatile, so the compiler neither hoists them out of the substep loop nor keeps
+// the terms in registers across it.
+template <typename T, int STRIDE>
+struct FrozenColumn {
+    const T* base;
+    __device__ __forceinline__ T operator[](int k) const { return *(const volatile T*)(base + k * STRIDE); }
+};
+
+// rl_freeze_voltage_terms with the terms written to a shared-memory column.
+template <class Model, typename T, int STRIDE>
+__device__ __forceinline__ void rl_freeze_voltage_terms_column(const T* y, const T* p, T dt, T* column) {
+    constexpr int NV = FrozenSlots<Model>::kVoltageOnly;
+    T rate[Model::kNumStates], inf[Model::kNumStates];
+    T vt[Model::kNumVTerms > 0 ? Model::kNumVTerms : 1];
+    Model::template rl_terms_voltage<T>(y, p, rate, inf);
+CHB_UNROLL
+    for (int i = 1; i < Model::kNumStates; ++i)
+        if (Model::rl_voltage_only(i)) {
+            column[frozen_slot<Model>(i) * STRIDE] = inf[i];
+            column[(NV + frozen_slot<Model>(i)) * STRIDE] = m_exp(rate[i] * dt);
+        }
+    Model::template rl_vterms<T>(y, p, vt);
+CHB_UNROLL
+    for (int k = 0; k < Model::kNumVTerms; ++k) column[(2 * NV + k) * STRIDE] = vt[k];
+}
+
+// rl_step_except_voltage_frozen reading the frozen terms from the column: the same
+// arithmetic on the same values.
+template <class Model, typename T, int STRIDE>
+__device__ __forceinline__ void rl_step_except_voltage_column(T* y, T stim, T cm, const T* p, T dt,
+                                                              const T* column) {
+    constexpr int NV = FrozenSlots<Model>::kVoltageOnly;
+    T rate[Model::kNumStates];
+    T inf[Model::kNumStates];
+    const FrozenColumn<T, STRIDE> vt{column + 2 * NV * STRIDE};
+    Model::template rl_terms_states_vt<T, FrozenColumn<T, STRIDE>>(y, stim, cm, p, vt, rate, inf);
+    const FrozenColumn<T, STRIDE> fz{column};
+CHB_UNROLL
+    for (int i = 1; i < Model::kNumStates; ++i) {
+        if (Model::rl_voltage_only(i)) {
+            const T vinf = fz[frozen_slot<Model>(i)];
+            y[i] = vinf + (y[i] - vinf) * fz[NV + frozen_slot<Model>(i)];
+        } else if (Model::rush_larsen(i)) {
+            y[i] = inf[i] + (y[i] - inf[i]) * m_exp(rate[i] * dt);
+        } else {
+            y[i] += dt * rate[i];
+        }
+    }
+}
+#endif
 
 // Full single-cell steps including the voltage (Compute / SolveAndUpdateState).
 template <class Model, typename T>

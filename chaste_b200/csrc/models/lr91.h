@@ -188,9 +188,11 @@ struct LuoRudy1991 {
         vt[1] = ((y[0] > (-T(100.0))) ? (((chb::singularity_offset<T>()*T(1.0)) > fabs((y[0] + T(77.0)))) ? ((m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0))))))) + (m_div((y[0] - (-T(77.0) - (chb::singularity_offset<T>()*T(1.0))))*((m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) + (chb::singularity_offset<T>()*T(1.0))) + T(35.0))))))) - (m_div((T(2.837)*(m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0)))) - T(1.0))), (((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(77.0))*m_exp((T(0.04)*((-T(77.0) - (chb::singularity_offset<T>()*T(1.0))) + T(35.0)))))))), (T(2.0)*(chb::singularity_offset<T>()*T(1.0)))))) : (m_div((T(2.837)*(m_exp((T(0.04)*(y[0] + T(77.0)))) - T(1.0))), ((y[0] + T(77.0))*m_exp((T(0.04)*(y[0] + T(35.0)))))))) : T(1.0));
         vt[2] = (m_div(v_time_independent_potassium_current_K1_gate__alpha_K1, (v_time_independent_potassium_current_K1_gate__alpha_K1 + v_time_independent_potassium_current_K1_gate__beta_K1)));
     }
-    template <typename T>
+    // vt is anything indexable: the array rl_vterms wrote, or an accessor that
+    // reads each term where it is used (a per-thread column of shared memory).
+    template <typename T, class VT = const T*>
     CHB_HD static void rl_terms_states_vt(const T* __restrict__ y, T stim, T cm,
-                                          const T* __restrict__ p, const T* __restrict__ vt,
+                                          const T* __restrict__ p, const VT& vt,
                                           T* __restrict__ rate, T* __restrict__ inf) {
         (void)stim; (void)cm; (void)p; (void)vt; (void)inf;
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
@@ -396,7 +398,6 @@ struct LuoRudy1991 {
     CHB_HD static void vjp_iionic(const T* __restrict__ y, T stim, T cm, const T* __restrict__ p,
                                 const T* __restrict__ w, T* __restrict__ gy, T* __restrict__ gp) {
         (void)stim; (void)cm; (void)p; (void)w; (void)gy; (void)gp;
-        stim = T(0.0); (void)stim;
         const T v_background_current__i_b = ((T(0.03921)*p[5])*(y[0] - (-T(59.87))));
         const T v_fast_sodium_current__i_Na = ((T(23.0)*p[0])*(y[1]*y[1]*y[1])*y[2]*y[3]*(y[0] - T(54.79446393509185)));
         const T v_plateau_potassium_current__Kp = (m_div(T(1.0), (T(1.0) + m_exp((m_divk((T(7.488) - y[0]), T(5.98), T(0.16722408026755853)))))));

@@ -445,7 +445,10 @@ int cg_part_ode(cg_part* c) {
     a.act_threshold = c->cfg.activation_threshold;
     const bool tt = c->cfg.model == CG_MODEL_TT06;
     const int m = c->cfg.ode_method;
-#define PART_ODE(M, METHOD) ode_kernel<M, double, METHOD><<<c->ode_blocks, 256, 0, c->stream>>>(a)
+// c->ode_blocks counts 256-thread blocks; the kernel's own block shape keeps that thread budget
+#define PART_ODE(M, METHOD)                                                                    \
+    ode_kernel<M, double, METHOD><<<c->ode_blocks * 256 / OdeShape<M, double, METHOD>::kThreads, \
+                                    OdeShape<M, double, METHOD>::kThreads, 0, c->stream>>>(a)
     if (tt) {
         if (m == CG_ODE_RUSH_LARSEN) PART_ODE(TenTusscher2006Epi, 1);
         else if (m == CG_ODE_BACKWARD_EULER) PART_ODE(TenTusscher2006Epi, 2);
