@@ -246,8 +246,9 @@ def run_ours(args, rank, world, device):
     te.voltage(out=vin)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        # V in from the host, one step, V back to the host (cg_step_host: the copy in
-        # overlaps the step's ODE piece by piece; the caller passes back what it got)
+        # V in from the host, one step, V back to the host (cg_step_host: the step's ODE
+        # reads V from the page-locked buffer as it computes; the caller passes back what
+        # it got)
         te.step_host(vin, 1, vout, keep_history=True)
         vin, vout = vout, vin
     e2e_s = time.perf_counter() - t0

@@ -114,6 +114,9 @@ struct cg_ctx {
     int interior_cls = 0;
     double* d_partials = nullptr;
     GridSync* d_gs = nullptr;
+    // status word, step counter and iteration ring in one device block laid out as
+    // HostControl, so that one copy reads them all; d_status, d_step, d_ring point into it
+    HostControl* d_ctl = nullptr;
     int* d_status = nullptr;
     long long* d_step = nullptr;
     int* d_ring = nullptr;
@@ -532,9 +535,10 @@ int alloc_vectors(cg_ctx* c) {
     }
     CG_TRY(dalloc(c, &c->d_act, n * sizeof(double)));
     CG_TRY(dalloc(c, &c->d_gs, sizeof(GridSync)));
-    CG_TRY(dalloc(c, &c->d_status, sizeof(int)));
-    CG_TRY(dalloc(c, &c->d_step, sizeof(long long)));
-    CG_TRY(dalloc(c, &c->d_ring, kRing * sizeof(int)));
+    CG_TRY(dalloc(c, &c->d_ctl, sizeof(HostControl)));
+    c->d_status = &c->d_ctl->status;
+    c->d_step = &c->d_ctl->step;
+    c->d_ring = c->d_ctl->ring;
     CG_TRY(dalloc(c, &c->d_refine, sizeof(int)));
     cudaStream_t s = c->stream;
     CG_CUDA(cudaMemsetAsync(c->d_gs, 0, sizeof(GridSync), s));
@@ -1130,6 +1134,12 @@ int upload_cells_t(cg_ctx* c, const double* init, const int* pset, const double*
     return CG_OK;
 }
 
+// The ODE methods whose kernel can read V^n from mapped host memory (cg_step_host);
+// the others copy V in first.
+constexpr bool host_input_method(int method) {
+    return method == CG_ODE_FORWARD_EULER || method == CG_ODE_RUSH_LARSEN;
+}
+
 // One ode_kernel launch over the nodes [a.lo, a.hi) in the kernel's block shape
 // (c->ode_blocks counts 256-thread blocks, so the grid keeps the same thread budget), or
 // one operator-splitting half step over every node.
@@ -1142,16 +1152,24 @@ void launch_ode_kernel(cg_ctx* c, const OdeArgs<T>& a) {
     constexpr int tpb = OdeShape<M, T, METHOD>::kThreads;
     const long long cap = (long long)c->ode_blocks * 256 / tpb;
     const int blocks = (int)std::max(1LL, std::min(cap, ((long long)a.hi - a.lo + tpb - 1) / tpb));
+    if constexpr (host_input_method(METHOD)) {
+        if (a.v_in) {
+            ode_kernel<M, T, METHOD, true><<<blocks, tpb, 0, c->stream>>>(a);
+            return;
+        }
+    }
     ode_kernel<M, T, METHOD><<<blocks, tpb, 0, c->stream>>>(a);
 }
 
 template <class M, typename T>
-void launch_ode(cg_ctx* c, int half = 0, int lo = 0, int hi = -1, bool reset_history = false) {
+void launch_ode(cg_ctx* c, int half = 0, int lo = 0, int hi = -1, bool reset_history = false,
+                const double* v_in = nullptr) {
     OdeArgs<T> a;
     a.n = c->n;
     a.lo = lo;
     a.hi = hi < 0 ? c->n : hi;
     a.reset_history = reset_history ? 1 : 0;
+    a.v_in = v_in;
     a.V = c->d_V;
     // the extrapolated guess replaces V^n in place, which splitting and SVI still need
     a.vprev = (c->cfg.solver == CG_SOLVER_OPERATOR_SPLITTING || c->svi) ? nullptr : c->d_Vprev;
@@ -1315,14 +1333,15 @@ cudaError_t launch_solve(cg_ctx* c) { return c->bido ? launch_bidomain(c) : laun
 // The ODE launch of a step: the whole step with V clamped (half 0), or one half of
 // the operator-splitting step including V (half 1, 2); half 0 may cover the nodes
 // [lo, hi) only.
-void launch_odes(cg_ctx* c, int half, int lo = 0, int hi = -1, bool reset_history = false) {
+void launch_odes(cg_ctx* c, int half, int lo = 0, int hi = -1, bool reset_history = false,
+                 const double* v_in = nullptr) {
     const bool tt = c->cfg.model == CG_MODEL_TT06;
     if (c->mixed()) {
-        if (tt) launch_ode<TenTusscher2006Epi, float>(c, half, lo, hi, reset_history);
-        else launch_ode<LuoRudy1991, float>(c, half, lo, hi, reset_history);
+        if (tt) launch_ode<TenTusscher2006Epi, float>(c, half, lo, hi, reset_history, v_in);
+        else launch_ode<LuoRudy1991, float>(c, half, lo, hi, reset_history, v_in);
     } else {
-        if (tt) launch_ode<TenTusscher2006Epi, double>(c, half, lo, hi, reset_history);
-        else launch_ode<LuoRudy1991, double>(c, half, lo, hi, reset_history);
+        if (tt) launch_ode<TenTusscher2006Epi, double>(c, half, lo, hi, reset_history, v_in);
+        else launch_ode<LuoRudy1991, double>(c, half, lo, hi, reset_history, v_in);
     }
 }
 
@@ -1423,10 +1442,32 @@ cudaError_t launch_step(cg_ctx* c) {
 // first step's ODE starts on as they arrive), the steps, ev1, V out and the control
 // words.  In a capture (`capture`) the copy stream forks from the captured stream and
 // the steps are plain launches.
+// The address through which the device reads page-locked host memory p (unified
+// addressing maps it), or null for memory the device cannot read.
+const double* device_view(const double* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return at.type == cudaMemoryTypeHost ? static_cast<const double*>(at.devicePointer) : nullptr;
+}
+
 int enqueue_host_call(cg_ctx* c, const double* v_in, int n_steps, double* v_out, int keep_history, bool capture) {
     const size_t n = (size_t)c->n;
     int k0 = 0;
-    if (v_in) {
+    const double* v_view = v_in ? device_view(v_in) : nullptr;
+    if (v_in && v_view && n_steps > 0 && !split(c) && !c->svi && host_input_method(c->cfg.ode_method)) {
+        // the first step's ODE reads V^n straight from the caller's page-locked buffer
+        // (over the host link, while it computes) and stores it on the device
+        launch_odes(c, 0, 0, -1, keep_history == 0, v_view);
+        if (cudaGetLastError() != cudaSuccess || launch_solve(c) != cudaSuccess) {
+            cudaGetLastError();
+            return CG_ERR_CUDA;
+        }
+        out_after_step(c, c->steps + 1);
+        k0 = 1;
+    } else if (v_in) {
         if (n_steps > 0 && !split(c) && !c->svi) {
             CG_CUDA(cudaEventRecord(c->fork_ev, c->stream));
             CG_CUDA(cudaStreamWaitEvent(c->copy_stream, c->fork_ev, 0));
@@ -1464,10 +1505,7 @@ int enqueue_host_call(cg_ctx* c, const double* v_in, int n_steps, double* v_out,
     CG_CUDA(capture ? cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal)
                     : cudaEventRecord(c->ev1, c->stream));
     if (v_out) CG_CUDA(cudaMemcpyAsync(v_out, c->d_V, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    HostControl* h = c->h_ctl;
-    CG_CUDA(cudaMemcpyAsync(&h->status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CG_CUDA(cudaMemcpyAsync(&h->step, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
-    CG_CUDA(cudaMemcpyAsync(h->ring, c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CG_CUDA(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(HostControl), cudaMemcpyDeviceToHost, c->stream));
     return CG_OK;
 }
 
@@ -1643,13 +1681,14 @@ int cg_step_host(cg_ctx* c, const double* v_in, int n_steps, double* v_out, int 
     }
     if (c->out_max && c->out_count + out_frames_added(c, n_steps) > c->out_max) return CG_ERR_NOMEM;
     CG_TRY(ensure_host_path(c));
-    CG_CUDA(cudaEventRecord(c->ev0, c->stream));
     // a call with page-locked buffers and no printing-step output is replayed from a
-    // graph of the whole call (copies, launches, read-back), built on its first use
+    // graph of the whole call (launches, copies, read-back), built on its first use
     const bool replay = (v_in || v_out) && c->out_every == 0 && pinned(v_in) && pinned(v_out);
     HostGraph* g = replay ? find_host_graph(c, v_in, v_out, n_steps, keep_history) : nullptr;
     if (replay && !g) g = capture_host_call(c, v_in, n_steps, v_out, keep_history);
     c->host_call_graph = g != nullptr;
+    // the timing starts here, after the host-side lookups and any capture
+    CG_CUDA(cudaEventRecord(c->ev0, c->stream));
     if (g) {
         CG_CUDA(cudaGraphLaunch(g->exec, c->stream));
     } else {
@@ -1962,19 +2001,16 @@ extern "C" int cg_step_profiled(cg_ctx* c, int n_steps, double* ms_odes, double*
     if (ms_odes) *ms_odes = t_ode;
     if (ms_linear) *ms_linear = t_cg;
     if (rc != CG_OK) return rc;
-    int bits = 0;
-    long long dstep = 0;
-    CG_CUDA(cudaMemcpy(&bits, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    CG_CUDA(cudaMemcpy(&dstep, c->d_step, sizeof(long long), cudaMemcpyDeviceToHost));
-    std::vector<int> ring(kRing);
-    CG_CUDA(cudaMemcpy(ring.data(), c->d_ring, kRing * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<HostControl> hc(1);
+    CG_CUDA(cudaMemcpy(hc.data(), c->d_ctl, sizeof(HostControl), cudaMemcpyDeviceToHost));
+    const long long dstep = hc[0].step;
     for (long long s = std::max(c->steps, dstep - kRing); s < dstep; ++s) {
-        c->total_iters += ring[s % kRing];
-        c->max_iters = std::max(c->max_iters, ring[s % kRing]);
+        c->total_iters += hc[0].ring[s % kRing];
+        c->max_iters = std::max(c->max_iters, hc[0].ring[s % kRing]);
     }
     c->steps = dstep;
     c->ms_last = t_ode + t_cg;
-    return status_from_bits(bits);
+    return status_from_bits(hc[0].status);
 }
 
 // -------------------------------------------------------------- output --

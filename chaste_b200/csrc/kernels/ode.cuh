@@ -36,6 +36,8 @@ struct OdeArgs {
                                         // half step including V (operator splitting)
     int lo, hi;                         // half 0: the nodes [lo, hi) of this launch
     int reset_history;                  // with vprev: V^n has no predecessor (guess V^n, no extrapolation)
+    const double* v_in;                 // ode_kernel<..., HOSTV = true>: V^n read from here (page-locked
+                                        // host memory, through its device mapping) and stored into V
 };
 
 // First step with V above the threshold (ActivationOutputModifier::ProcessSolutionAtTimeStep,
@@ -120,7 +122,10 @@ struct OdeShape {
     static constexpr int kShared = kColumn ? FrozenSlots<M>::kSlots * kThreads : 1;
 };
 
-template <class M, typename T, int METHOD>
+// HOSTV: V^n is read from a.v_in (a separate instantiation, so that the kernel of the
+// device-resident steps keeps its code; measured with the choice made at run time in
+// one kernel, that kernel took 0.080 instead of 0.063 ms per C2 step).
+template <class M, typename T, int METHOD, bool HOSTV = false>
 __global__ void __launch_bounds__(OdeShape<M, T, METHOD>::kThreads, OdeShape<M, T, METHOD>::kMinBlocks)
     ode_kernel(OdeArgs<T> a) {
     using Shape = OdeShape<M, T, METHOD>;
@@ -136,7 +141,7 @@ __global__ void __launch_bounds__(OdeShape<M, T, METHOD>::kThreads, OdeShape<M, 
     const double dtinv = 1.0 / a.dt_pde;
     for (int i = a.lo + blockIdx.x * blockDim.x + threadIdx.x; i < a.hi; i += gridDim.x * blockDim.x) {
         T y[S];
-        const double v = a.V[i];
+        const double v = HOSTV ? a.v_in[i] : a.V[i];
         // mixed precision: the diffusion solve starts from the linear extrapolation
         // 2 V^n - V^{n-1} (FP64 mode keeps Chaste's guess V^n, LinearSystem.cpp:833-837);
         // the right-hand side below still uses V^n
@@ -144,6 +149,8 @@ __global__ void __launch_bounds__(OdeShape<M, T, METHOD>::kThreads, OdeShape<M, 
             const double vp = a.reset_history ? v : a.vprev[i];
             a.vprev[i] = v;
             a.V[i] = 2.0 * v - vp;
+        } else if (HOSTV) {
+            a.V[i] = v;
         }
         // activation bookkeeping of the previous step's solution (time t0)
         if (v > a.act_threshold && a.act[i] < 0.0) a.act[i] = t0;

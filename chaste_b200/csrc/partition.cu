@@ -427,6 +427,7 @@ int cg_part_ode(cg_part* c) {
     a.V = c->x + c->halo;
     a.vprev = nullptr;
     a.half = 0;
+    a.v_in = nullptr;
     a.states = (double*)c->states;
     a.iion = c->iion;
     a.zrhs = c->z + c->halo;

@@ -184,13 +184,16 @@ int cg_step(cg_ctx* ctx, int n_steps);
 /* The same with the voltage in host memory, for a caller that keeps V on the host
  * between steps (AbstractDynamicLinearPdeSolver::Solve hands the solution Vec back
  * every step, pde/src/solver/AbstractDynamicLinearPdeSolver.hpp:233-272): v_in
- * (n_nodes, may be NULL) is copied in before the first step -- in pieces, the first
- * step's ODE starting on each piece as it arrives -- and V after the last step is
- * copied to v_out (may be NULL), with one synchronisation for the whole call.
+ * (n_nodes, may be NULL) is V before the first step -- page-locked memory is read by
+ * the first step's ODE kernel through its device mapping, over the host link while
+ * it computes; pageable memory is copied in, in pieces, the first step's ODE starting
+ * on each piece as it arrives -- and V after the last step is copied to v_out (may be
+ * NULL), with one synchronisation for the whole call.  v_in must not change during
+ * the call.
  * keep_history = 1 declares that v_in continues the trajectory (the caller passes
  * back what the previous call returned), so the mixed solve keeps its extrapolated
  * initial guess; 0 treats v_in as new (as cg_set_voltage does).  With page-locked host
- * buffers the copies are DMA transfers and, when no printing-step output is configured,
+ * buffers the copy out is a DMA transfer and, when no printing-step output is configured,
  * the whole call is captured as a CUDA graph on its first use and replayed afterwards
  * (the four most recent (v_in, v_out, n_steps, keep_history) combinations are kept;
  * cg_stats.host_call_graph says whether the last call was a replay). */

@@ -490,6 +490,15 @@ def test_host_buffer_steps_replayed_from_graphs(N, precision):
         a, b = b, a
         assert np.array_equal(a, dev.voltage())
     assert host.stats().steps == dev.stats().steps
+    # several steps per call: the first call of a (buffers, steps) pair is captured, the
+    # next ones replay it
+    for _ in range(3):
+        dev.step(4)
+        host.step_host(a, 4, b, keep_history=True)
+        a, b = b, a
+        assert np.array_equal(a, dev.voltage())
+        assert host.stats().steps == dev.stats().steps
+    assert host.stats().host_call_graph == 1
     # new cells: both tissues restart from the same states, the cached calls are rebuilt
     dev.set_cells()
     host.set_cells()
