@@ -470,13 +470,16 @@ def test_host_buffer_steps_match_device_steps(N, precision):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_host_buffer_steps_replayed_from_graphs(N, precision):
-    """With page-locked buffers cg_step_host replays each (v_in, v_out) pair's call from a
-    graph; two alternating buffer pairs reproduce the device-resident steps bit for bit,
-    and a change of the cells (new kernel arguments) drops the cached calls."""
+@pytest.mark.parametrize("case_name", ["TT06_3D", "LR91_2D"])
+def test_host_buffer_steps_replayed_from_graphs(N, precision, case_name):
+    """With page-locked buffers the first step's ODE reads V from the caller's buffer
+    through its device mapping and cg_step_host replays each (v_in, v_out) pair's call
+    from a graph; two alternating buffer pairs reproduce the device-resident steps bit
+    for bit (Rush-Larsen and forward Euler), and a change of the cells (new kernel
+    arguments) drops the cached calls."""
     import torch
 
-    case = dict(TC.TT06_3D)
+    case = dict(getattr(TC, case_name))
     dev, _ = TC.make_gpu(N, precision=precision, **case)
     host, _ = TC.make_gpu(N, precision=precision, **case)
     dev.step(3)
