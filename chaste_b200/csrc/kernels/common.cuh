@@ -130,10 +130,42 @@ __device__ __forceinline__ bool wait_count(unsigned* counter, unsigned target, i
 // Needs blockDim >= 32 * kReduceWarps; red holds 32 * NV doubles.
 constexpr int kReduceWarps = 4;
 
+// The same reduction when the grid is one block: the block's sums are the totals, with
+// no global partials, atomics or polling.
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], double* red, double* out, unsigned& round) {
+    __shared__ double s_tot[2][kPartialStride];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp * NV + k] = v[k];
+    __syncthreads();
+    // two buffers by round parity: round r + 1 writes the other one, so a thread still
+    // reading round r's totals is never overwritten
+    const unsigned par = round & 1u;
+    round++;
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const double b = warp_sum(lane < nw ? red[lane * NV + k] : 0.0);
+            if (lane == 0) s_tot[par][k] = b;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = s_tot[par][k];
+}
+
 template <int NV>
 __device__ bool grid_reduce(double (&v)[NV], double* red, GridSync* gs, double* partials, double* out, int* status,
                             unsigned& round) {
     static_assert(NV >= 1 && NV <= kPartialStride, "at most four sums per reduction");
+    if (gridDim.x == 1) {
+        block_reduce<NV>(v, red, out, round);
+        return true;
+    }
     constexpr int kLoads = kMaxGridBlocks / (32 * kReduceWarps);
     __shared__ int s_ok;
     __shared__ double s_part[kReduceWarps][kPartialStride];
