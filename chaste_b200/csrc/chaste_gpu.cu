@@ -146,6 +146,7 @@ struct cg_ctx {
     // bjacobi (ILU(0) of the whole matrix): factors, level schedules, b and B b
     bool ilu = false;
     IluArgs ilu_args{};
+    size_t ilu_smem = 0;   // > 0: cg_ilu_smem_kernel with this much dynamic shared memory
     // bidomain (cg_set_bidomain_mesh): the interleaved (V, phi_e) operator B, on the host
     // for fixing phi_e nodes and on the device, and the solve's vectors
     bool bido = false;
@@ -622,6 +623,10 @@ int alloc_vectors(cg_ctx* c) {
         const long long want_ilu = (long long)n <= kIluOneBlockNodes ? 1 : ((long long)n + 1023) / 1024;
         c->cg_blocks = (int)std::max(1LL, std::min({want_ilu, (long long)per_sm_ilu * sms, (long long)kMaxGridBlocks}));
         c->cg_threads = 1024;
+        if (c->ilu_smem > 0) {
+            c->cg_blocks = 1;
+            c->cg_threads = kIluSmemThreads;
+        }
     }
     CG_TRY(dalloc(c, &c->d_partials,
                   (size_t)2 * std::max(blocks_512, c->cg_blocks) * kPartialStride * sizeof(double)));
@@ -736,6 +741,78 @@ int setup_ilu(cg_ctx* c) {
     c->ilu_args.b_ptr = d_bp;
     c->ilu_args.b_levels = bl;
     c->ilu = true;
+    // small meshes: the one-block solve with its vectors in shared memory, when the packed
+    // rows fit (at most kIluPackE entries either side of the diagonal, levels of at most
+    // kIluSmemThreads rows, at most kIluSmemLevels levels a sweep)
+    c->ilu_smem = 0;
+    auto widest = [](const std::vector<int>& ptr) {
+        int w = 0;
+        for (size_t l = 0; l + 1 < ptr.size(); ++l) w = std::max(w, ptr[l + 1] - ptr[l]);
+        return w;
+    };
+    int most_l = 0, most_u = 0;
+    for (int i = 0; i < n; ++i) {
+        most_l = std::max(most_l, diag[i] - A.rowptr[i]);
+        most_u = std::max(most_u, A.rowptr[i + 1] - diag[i] - 1);
+    }
+    if (n <= kIluSmemNodes && fl <= kIluSmemLevels && bl <= kIluSmemLevels && most_l <= kIluPackE &&
+        most_u <= kIluPackE && widest(fptr) <= kIluSmemThreads && widest(bptr) <= kIluSmemThreads) {
+        const int pe = std::max(most_l, most_u) <= 4 ? 4 : kIluPackE;
+        const size_t slots = (size_t)n * pe;
+        std::vector<int> fcnt(n), fcol(slots, 0), bcnt(n), bcol(slots, 0);
+        std::vector<double> fval(slots, 0.0), bval(slots, 0.0), bdg(n);
+        for (int k = 0; k < n; ++k) {
+            const int i = frows[k];
+            fcnt[k] = diag[i] - A.rowptr[i];
+            for (int e = 0; e < fcnt[k]; ++e) {
+                fcol[(size_t)k * pe + e] = A.cols[A.rowptr[i] + e];
+                fval[(size_t)k * pe + e] = lu[A.rowptr[i] + e];
+            }
+            const int j = brows[k];
+            bcnt[k] = A.rowptr[j + 1] - diag[j] - 1;
+            for (int e = 0; e < bcnt[k]; ++e) {
+                bcol[(size_t)k * pe + e] = A.cols[diag[j] + 1 + e];
+                bval[(size_t)k * pe + e] = lu[diag[j] + 1 + e];
+            }
+            bdg[k] = lu[diag[j]];
+        }
+        int *d_fcnt = nullptr, *d_fcol = nullptr, *d_bcnt = nullptr, *d_bcol = nullptr;
+        double *d_fval = nullptr, *d_bval = nullptr, *d_bdg = nullptr;
+        CG_TRY(dalloc(c, &d_fcnt, n * sizeof(int)));
+        CG_TRY(dalloc(c, &d_fcol, slots * sizeof(int)));
+        CG_TRY(dalloc(c, &d_fval, slots * sizeof(double)));
+        CG_TRY(dalloc(c, &d_bcnt, n * sizeof(int)));
+        CG_TRY(dalloc(c, &d_bcol, slots * sizeof(int)));
+        CG_TRY(dalloc(c, &d_bval, slots * sizeof(double)));
+        CG_TRY(dalloc(c, &d_bdg, n * sizeof(double)));
+        CG_CUDA(cudaMemcpyAsync(d_fcnt, fcnt.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(d_fcol, fcol.data(), slots * sizeof(int), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(d_fval, fval.data(), slots * sizeof(double), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(d_bcnt, bcnt.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(d_bcol, bcol.data(), slots * sizeof(int), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(d_bval, bval.data(), slots * sizeof(double), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaMemcpyAsync(d_bdg, bdg.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+        CG_CUDA(cudaStreamSynchronize(s));
+        c->ilu_args.fk_cnt = d_fcnt;
+        c->ilu_args.fk_col = d_fcol;
+        c->ilu_args.fk_val = d_fval;
+        c->ilu_args.bk_cnt = d_bcnt;
+        c->ilu_args.bk_col = d_bcol;
+        c->ilu_args.bk_val = d_bval;
+        c->ilu_args.bk_dg = d_bdg;
+        c->ilu_args.pack_e = pe;
+        auto kern = pe == 4 ? cg_ilu_smem_kernel<4> : cg_ilu_smem_kernel<kIluPackE>;
+        const size_t bytes = 2 * (size_t)n * sizeof(double) + (size_t)(fl + 1 + bl + 1) * sizeof(int);
+        int optin = 0;
+        CG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+        cudaFuncAttributes fa;
+        CG_CUDA(cudaFuncGetAttributes(&fa, kern));
+        if (bytes + fa.sharedSizeBytes <= (size_t)optin) {
+            CG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         optin - (int)fa.sharedSizeBytes));
+            c->ilu_smem = bytes;
+        }
+    }
     return CG_OK;
 }
 
@@ -1281,6 +1358,11 @@ cudaError_t launch_cg(cg_ctx* c) {
         at[0].val.cooperative = 1;
         lc.attrs = at;
         lc.numAttrs = 1;
+        if (c->ilu_smem > 0) {
+            lc.dynamicSmemBytes = c->ilu_smem;
+            return cudaLaunchKernelEx(&lc, c->ilu_args.pack_e == 4 ? cg_ilu_smem_kernel<4> : cg_ilu_smem_kernel<kIluPackE>,
+                                      a, c->ilu_args);
+        }
         return cudaLaunchKernelEx(&lc, cg_ilu_kernel, a, c->ilu_args);
     }
     cudaLaunchConfig_t cfg = {};

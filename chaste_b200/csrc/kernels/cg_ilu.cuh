@@ -37,7 +37,24 @@ struct IluArgs {
     int b_levels;
     double* bvec;            // b = M z (+ correction), n
     double* wvec;            // B b, n
+    // Packed rows for the one-block solve with its vectors in shared memory (cg_ilu_smem_kernel):
+    // position k of the forward (backward) level order holds row fk_row[k] (bk_row[k]), its
+    // count of entries left (right) of the diagonal and those entries' columns and factors in
+    // ascending column order, pack_e slots per position (4 or kIluPackE); bk_dg: the row's
+    // diagonal factor.
+    const int* fk_cnt;
+    const int* fk_col;
+    const double* fk_val;
+    const int* bk_cnt;
+    const int* bk_col;
+    const double* bk_val;
+    const double* bk_dg;
+    int pack_e;
 };
+
+// Entries per row of the packed triangular factors (2D meshes of triangles have 3 on either
+// side of the diagonal, the Kuhn tetrahedra 7).
+constexpr int kIluPackE = 8;
 
 // Every thread of every block arrives; returns false when a bounded wait gave up.
 // One block: a block barrier.  Several: the arrival counter of grid_reduce (the
@@ -217,6 +234,223 @@ __device__ void cg_ilu_kernel_body(const CgArgs& a, const IluArgs& f, unsigned& 
 static __global__ void __launch_bounds__(1024, 1) cg_ilu_kernel(CgArgs a, IluArgs f) {
     unsigned round = 0;
     cg_ilu_kernel_body(a, f, round);
+    grid_exit(a.gs);
+}
+
+// ---------------------------------------------------------------------------
+// Small meshes (at most kIluSmemNodes nodes): one block of kIluSmemThreads threads whose
+// triangular solves run in place on vectors held in shared memory.  Per level a thread
+// takes position ptr[l] + t (levels of at most kIluSmemThreads rows); the packed rows of
+// the next levels (row, columns, factors, diagonal) are loaded while this level computes,
+// so after each block barrier only shared-memory reads remain on the critical path.
+// The rows, their entry order and the arithmetic of each row are those of
+// cg_ilu_kernel; the inner products are summed over the nodes in natural order after the
+// sweeps instead of in level order.
+constexpr int kIluSmemThreads = 512;
+constexpr int kIluSmemNodes = 12800;
+constexpr int kIluSmemLevels = 2048;
+
+// E: entries per packed row (the slot stride of the packed arrays, 4 or kIluPackE).
+template <int E>
+struct PackedRow {
+    int i;   // -1: no row
+    int cnt;
+    int col[E];
+    double val[E];
+    double dg;
+};
+
+template <int E>
+__device__ __forceinline__ void load_packed_row(PackedRow<E>& r, int k, int end, const int* rows, const int* cnt,
+                                                const int* col, const double* val, const double* dg) {
+    if (k >= end) {
+        r.i = -1;
+        r.cnt = 0;
+        r.dg = 1.0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            r.col[e] = 0;
+            r.val[e] = 0.0;
+        }
+        return;
+    }
+    r.i = rows[k];
+    r.cnt = cnt[k];
+    r.dg = dg ? dg[k] : 1.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        r.col[e] = col[(size_t)k * E + e];
+        r.val[e] = val[(size_t)k * E + e];
+    }
+}
+
+// In-place triangular solve of NV shared-memory vectors (z1 ignored when NV == 1).
+template <int NV, bool BACK, int E>
+__device__ __forceinline__ void packed_sweep(const int* lptr, int levels, const int* rows, const int* cnt,
+                                             const int* col, const double* val, const double* dg, double* z0,
+                                             double* z1) {
+    // rows loaded AHEAD levels ahead (two for the narrow rows of 2D meshes; one for the
+    // 3D rows, whose registers would otherwise spill)
+    constexpr int AHEAD = E <= 4 ? 2 : 1;
+    const int t = threadIdx.x;
+    PackedRow<E> cur, nx1, nx2;
+    nx1.i = nx2.i = -1;
+    nx1.cnt = nx2.cnt = 0;
+    load_packed_row(cur, lptr[0] + t, lptr[1], rows, cnt, col, val, dg);
+    if (AHEAD == 2 && levels > 1) load_packed_row(nx1, lptr[1] + t, lptr[2], rows, cnt, col, val, dg);
+    for (int l = 0; l < levels; ++l) {
+        if (l + AHEAD < levels)
+            load_packed_row(AHEAD == 2 ? nx2 : nx1, lptr[l + AHEAD] + t, lptr[l + AHEAD + 1], rows, cnt, col, val,
+                            dg);
+        if (cur.i >= 0) {
+            double s0 = z0[cur.i], s1 = NV > 1 ? z1[cur.i] : 0.0;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                if (e < cur.cnt) {
+                    s0 -= cur.val[e] * z0[cur.col[e]];
+                    if (NV > 1) s1 -= cur.val[e] * z1[cur.col[e]];
+                }
+            }
+            if (BACK) {
+                s0 = s0 / cur.dg;
+                if (NV > 1) s1 = s1 / cur.dg;
+            }
+            z0[cur.i] = s0;
+            if (NV > 1) z1[cur.i] = s1;
+        }
+        __syncthreads();
+        cur = nx1;
+        if (AHEAD == 2) nx1 = nx2;
+    }
+}
+
+
+
+// The solve of cg_ilu_kernel_body on one block with B r in shared memory (z0) and, in
+// phase 0, B b beside it (z1); the level pointers are copied to shared memory first.
+template <int E>
+__device__ void cg_ilu_smem_body(const CgArgs& a, const IluArgs& f, unsigned& round) {
+    __shared__ double red[32 * 4];
+    extern __shared__ double dyn[];
+    const int n = a.n;
+    double* z0 = dyn;
+    double* z1 = dyn + n;
+    int* fptr = reinterpret_cast<int*>(dyn + 2 * (size_t)n);
+    int* bptr = fptr + (f.f_levels + 1);
+    for (int l = threadIdx.x; l <= f.f_levels; l += blockDim.x) fptr[l] = f.f_ptr[l];
+    for (int l = threadIdx.x; l <= f.b_levels; l += blockDim.x) bptr[l] = f.b_ptr[l];
+    if (*(volatile int*)a.status & ~kStatusStateRange) return;
+    const long long step = *a.step;
+    const int t0 = threadIdx.x, stride = blockDim.x;
+    double* __restrict__ x = a.x;
+    double* __restrict__ r = a.r;
+    double* __restrict__ q = a.q;
+    double* __restrict__ p = a.p0;
+    double res[4];
+
+    // ---- b = M z (+ correction), r = b - A x; the sweeps' right-hand sides r and b
+    double babs = 0.0;
+    for (int i = t0; i < n; i += stride) {
+        const double b = csr_row<double, double>(a.csr.rowptr, a.csr.cols, a.csr.m, i, a.zrhs) +
+                         (a.corr ? a.corr[i] : 0.0);
+        const double av = csr_row<double, double>(a.csr.rowptr, a.csr.cols, a.csr.a, i, x);
+        const double rr = b - av;
+        f.bvec[i] = b;
+        r[i] = rr;
+        z0[i] = rr;
+        z1[i] = b;
+        babs += fabs(b);
+    }
+    __syncthreads();
+    packed_sweep<2, false, E>(fptr, f.f_levels, f.f_rows, f.fk_cnt, f.fk_col, f.fk_val, nullptr, z0, z1);
+    packed_sweep<2, true, E>(bptr, f.b_levels, f.b_rows, f.bk_cnt, f.bk_col, f.bk_val, f.bk_dg, z0, z1);
+    double v[4] = {babs, 0.0, 0.0, 0.0};
+    for (int i = t0; i < n; i += stride) {
+        const double zz = z0[i], ww = z1[i];
+        v[1] += ww * ww;
+        v[2] += zz * zz;
+        v[3] += r[i] * zz;
+    }
+    if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
+    double rnorm0 = sqrt(res[1]);
+    double dp = sqrt(res[2]);
+    double beta = res[3];
+    if (res[0] < 1e-15 && res[0] > 0.0) {
+        // LinearSystem.cpp:984-994: tiny RHS -> zero initial guess, r = b, B r = B b
+        double v2[2] = {0, 0};
+        for (int i = t0; i < n; i += stride) {
+            const double b = f.bvec[i], zz = z1[i];
+            x[i] = 0.0;
+            r[i] = b;
+            z0[i] = zz;
+            v2[0] += zz * zz;
+            v2[1] += b * zz;
+        }
+        double o2[2];
+        if (!grid_reduce<2>(v2, red, a.gs, a.partials, o2, a.status, round)) return;
+        dp = sqrt(o2[0]);
+        beta = o2[1];
+        rnorm0 = dp;
+    }
+    if (rnorm0 == 0.0) rnorm0 = dp;
+    const double ttol = fmax(a.rtol * rnorm0, a.abstol);
+    if (!isfinite(dp)) return cg_finish(a, step, 0, kStatusNaN);
+    if (dp <= ttol) return cg_finish(a, step, 0, 0);
+    if (dp >= a.dtol * rnorm0) return cg_finish(a, step, 0, kStatusCgDiverged);
+
+    double betaold = 0.0;
+    int it = 0;
+    for (; it < a.maxit; ++it) {
+        if (beta == 0.0) return cg_finish(a, step, it + 1, 0);
+        const double bc = it == 0 ? 0.0 : beta / betaold;
+        const bool first = it == 0;
+        // ---- p = z + bc p ; A p = A z + bc A p ; p . A p
+        {
+            double v1[1] = {0};
+            for (int i = t0; i < n; i += stride) {
+                const double az = csr_row<double, double>(a.csr.rowptr, a.csr.cols, a.csr.a, i, z0);
+                const double qi = first ? az : az + bc * q[i];
+                const double pi = first ? z0[i] : z0[i] + bc * p[i];
+                q[i] = qi;
+                p[i] = pi;
+                v1[0] += pi * qi;
+            }
+            if (!grid_reduce<1>(v1, red, a.gs, a.partials, res, a.status, round)) return;
+        }
+        const double dpi = res[0];
+        if (!(dpi > 0.0)) return cg_finish(a, step, it + 1, isfinite(dpi) ? kStatusCgDiverged : kStatusNaN);
+        const double alpha = beta / dpi;
+        // ---- x += alpha p, r -= alpha A p; then z = B r in place
+        for (int i = t0; i < n; i += stride) {
+            x[i] += alpha * p[i];
+            const double rr = r[i] - alpha * q[i];
+            r[i] = rr;
+            z0[i] = rr;
+        }
+        __syncthreads();
+        packed_sweep<1, false, E>(fptr, f.f_levels, f.f_rows, f.fk_cnt, f.fk_col, f.fk_val, nullptr, z0, nullptr);
+        packed_sweep<1, true, E>(bptr, f.b_levels, f.b_rows, f.bk_cnt, f.bk_col, f.bk_val, f.bk_dg, z0, nullptr);
+        double v2[2] = {0, 0};
+        for (int i = t0; i < n; i += stride) {
+            const double zz = z0[i];
+            v2[0] += zz * zz;
+            v2[1] += zz * r[i];
+        }
+        if (!grid_reduce<2>(v2, red, a.gs, a.partials, res, a.status, round)) return;
+        dp = sqrt(res[0]);
+        if (!isfinite(dp)) return cg_finish(a, step, it + 1, kStatusNaN);
+        if (dp <= ttol) return cg_finish(a, step, it + 1, 0);
+        if (dp >= a.dtol * rnorm0) return cg_finish(a, step, it + 1, kStatusCgDiverged);
+        betaold = beta;
+        beta = res[1];
+    }
+    cg_finish(a, step, it, kStatusCgMaxIt);
+}
+
+template <int E>
+__global__ void __launch_bounds__(kIluSmemThreads, 1) cg_ilu_smem_kernel(CgArgs a, IluArgs f) {
+    unsigned round = 0;
+    cg_ilu_smem_body<E>(a, f, round);
     grid_exit(a.gs);
 }
 
