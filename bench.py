@@ -160,13 +160,13 @@ def stimulated(wl, xyz):
     return np.where(inside, 0, -1).astype(np.int32)
 
 
-def build_tissue(N, wl, precision, device):
+def build_tissue(N, wl, precision, device, pc=None):
     from chaste_b200.heart import slab_coordinates
 
     cfg = N.default_config()
     cfg.model, cfg.ode_method = wl["model"], wl["method"]
     cfg.ode_time_step, cfg.pde_time_step = wl["dt_ode"], wl["dt_pde"]
-    cfg.ksp_preconditioner = N.PC_JACOBI
+    cfg.ksp_preconditioner = N.PC_JACOBI if pc is None else pc
     cfg.use_absolute_tolerance, cfg.ksp_tolerance = 0, wl["rel_tol"]
     cfg.precision = precision
     cfg.device = device
@@ -641,10 +641,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--t-start-ms", type=float, default=10.0,
                     help="simulated time reached, untimed, before the warm-up and timed steps")
-    ap.add_argument("--profile", choices=["fp64", "mixed", "population", "runs"],
-                    help="only build the workload's tissue in this precision, advance it to --t-start-ms and "
-                         "take --steps steps with an L2 flush before each (the program the ncu captures in "
-                         "profiles/ run)")
+    ap.add_argument("--profile", choices=["fp64", "mixed", "fp64-bjacobi", "population", "runs"],
+                    help="only build the workload's tissue in this precision (fp64-bjacobi: FP64 with Chaste's "
+                         "default bjacobi preconditioner), advance it to --t-start-ms and take --steps steps "
+                         "with an L2 flush before each (the program the ncu captures in profiles/ run)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.profile == "population":
@@ -685,17 +685,21 @@ def main():
 
         build_native()
         wl = WORKLOADS[args.workload]
-        t = build_tissue(N, wl, 0 if args.profile == "fp64" else 1, 0)
+        t = build_tissue(N, wl, 1 if args.profile == "mixed" else 0, 0,
+                         pc=N.PC_BJACOBI if args.profile == "fp64-bjacobi" else None)
         t.step(start_steps(args, wl))
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda:0")
+        ms = 0.0
         for _ in range(args.steps):
             flush_l2(flush)
             torch.cuda.synchronize()
             t.step(1)
+            ms += t.stats().ms_last_call
         torch.cuda.synchronize()
         st = t.stats()
         print(json.dumps({"profile": args.profile, "workload": args.workload, "steps": int(st.steps),
-                          "last_cg_iterations": st.last_cg_iterations}), flush=True)
+                          "last_cg_iterations": st.last_cg_iterations,
+                          "ms_per_step": ms / max(1, args.steps)}), flush=True)
         return
     if args.workload == "tt06_population":
         print(json.dumps(run_population(args)), flush=True)
