@@ -801,6 +801,8 @@ int setup_ilu(cg_ctx* c) {
         c->ilu_args.bk_val = d_bval;
         c->ilu_args.bk_dg = d_bdg;
         c->ilu_args.pack_e = pe;
+        c->ilu_args.f_warps = (widest(fptr) + 31) / 32;
+        c->ilu_args.b_warps = (widest(bptr) + 31) / 32;
         auto kern = pe == 4 ? cg_ilu_smem_kernel<4> : cg_ilu_smem_kernel<kIluPackE>;
         const size_t bytes = 2 * (size_t)n * sizeof(double) + (size_t)(fl + 1 + bl + 1) * sizeof(int);
         int optin = 0;

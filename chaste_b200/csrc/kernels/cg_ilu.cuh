@@ -50,6 +50,7 @@ struct IluArgs {
     const double* bk_val;
     const double* bk_dg;
     int pack_e;
+    int f_warps, b_warps;    // warps covering the widest forward / backward level
 };
 
 // Entries per row of the packed triangular factors (2D meshes of triangles have 3 on either
@@ -284,11 +285,10 @@ __device__ __forceinline__ void load_packed_row(PackedRow<E>& r, int k, int end,
     }
 }
 
-// In-place triangular solve of NV shared-memory vectors (z1 ignored when NV == 1).
 template <int NV, bool BACK, int E>
-__device__ __forceinline__ void packed_sweep(const int* lptr, int levels, const int* rows, const int* cnt,
-                                             const int* col, const double* val, const double* dg, double* z0,
-                                             double* z1) {
+__device__ __forceinline__ void packed_levels(const int* lptr, int levels, const int* rows, const int* cnt,
+                                              const int* col, const double* val, const double* dg, double* z0,
+                                              double* z1, int nthreads) {
     // rows loaded AHEAD levels ahead (two for the narrow rows of 2D meshes; one for the
     // 3D rows, whose registers would otherwise spill)
     constexpr int AHEAD = E <= 4 ? 2 : 1;
@@ -318,13 +318,23 @@ __device__ __forceinline__ void packed_sweep(const int* lptr, int levels, const 
             z0[cur.i] = s0;
             if (NV > 1) z1[cur.i] = s1;
         }
-        __syncthreads();
+        asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
         cur = nx1;
         if (AHEAD == 2) nx1 = nx2;
     }
 }
 
-
+// In-place triangular solve of NV shared-memory vectors (z1 ignored when NV == 1).  Only
+// the first `warps` warps (those the widest level needs) take part, synchronising the
+// levels on named barrier 1 among themselves; the block meets again at the end.
+template <int NV, bool BACK, int E>
+__device__ __forceinline__ void packed_sweep(const int* lptr, int levels, const int* rows, const int* cnt,
+                                             const int* col, const double* val, const double* dg, double* z0,
+                                             double* z1, int warps) {
+    if ((int)(threadIdx.x >> 5) < warps) packed_levels<NV, BACK, E>(lptr, levels, rows, cnt, col, val, dg, z0, z1,
+                                                                     warps * 32);
+    __syncthreads();
+}
 
 // The solve of cg_ilu_kernel_body on one block with B r in shared memory (z0) and, in
 // phase 0, B b beside it (z1); the level pointers are copied to shared memory first.
@@ -362,8 +372,8 @@ __device__ void cg_ilu_smem_body(const CgArgs& a, const IluArgs& f, unsigned& ro
         babs += fabs(b);
     }
     __syncthreads();
-    packed_sweep<2, false, E>(fptr, f.f_levels, f.f_rows, f.fk_cnt, f.fk_col, f.fk_val, nullptr, z0, z1);
-    packed_sweep<2, true, E>(bptr, f.b_levels, f.b_rows, f.bk_cnt, f.bk_col, f.bk_val, f.bk_dg, z0, z1);
+    packed_sweep<2, false, E>(fptr, f.f_levels, f.f_rows, f.fk_cnt, f.fk_col, f.fk_val, nullptr, z0, z1, f.f_warps);
+    packed_sweep<2, true, E>(bptr, f.b_levels, f.b_rows, f.bk_cnt, f.bk_col, f.bk_val, f.bk_dg, z0, z1, f.b_warps);
     double v[4] = {babs, 0.0, 0.0, 0.0};
     for (int i = t0; i < n; i += stride) {
         const double zz = z0[i], ww = z1[i];
@@ -428,8 +438,8 @@ __device__ void cg_ilu_smem_body(const CgArgs& a, const IluArgs& f, unsigned& ro
             z0[i] = rr;
         }
         __syncthreads();
-        packed_sweep<1, false, E>(fptr, f.f_levels, f.f_rows, f.fk_cnt, f.fk_col, f.fk_val, nullptr, z0, nullptr);
-        packed_sweep<1, true, E>(bptr, f.b_levels, f.b_rows, f.bk_cnt, f.bk_col, f.bk_val, f.bk_dg, z0, nullptr);
+        packed_sweep<1, false, E>(fptr, f.f_levels, f.f_rows, f.fk_cnt, f.fk_col, f.fk_val, nullptr, z0, nullptr, f.f_warps);
+        packed_sweep<1, true, E>(bptr, f.b_levels, f.b_rows, f.bk_cnt, f.bk_col, f.bk_val, f.bk_dg, z0, nullptr, f.b_warps);
         double v2[2] = {0, 0};
         for (int i = t0; i < n; i += stride) {
             const double zz = z0[i];
