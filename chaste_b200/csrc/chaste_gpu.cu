@@ -131,6 +131,7 @@ struct cg_ctx {
     std::vector<cg_stimulus> stims_host;
     // launch shapes
     int ode_blocks = 0;
+    int sms = 0;            // multiprocessors of the device
     int cg_blocks = 0;
     int cg_threads = 512;   // threads per block of the persistent CG kernel
     int pipe_nodes = 0;   // > 0: mixed slab solve by cg_mixed_pipe_kernel with this many nodes per thread
@@ -553,6 +554,7 @@ int alloc_vectors(cg_ctx* c) {
     // launch shapes: the CG kernel is cooperative, so its grid must be co-resident
     int sms = 0;
     CG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    c->sms = sms;
     int per_sm = 0;
     CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_cg_kernel(c), 512, 0));
     if (per_sm < 1) return CG_ERR_UNSUPPORTED;
@@ -1228,9 +1230,13 @@ void launch_ode_kernel(cg_ctx* c, const OdeArgs<T>& a) {
         ode_half_kernel<M, T, METHOD><<<c->ode_blocks, 256, 0, c->stream>>>(a);
         return;
     }
-    constexpr int tpb = OdeShape<M, T, METHOD>::kThreads;
+    // small meshes: smaller blocks, so that the cells spread over every SM (each thread's
+    // step is a long chain of dependent FP64 or SFU operations: SMs, not warps, set the pace)
+    const long long nodes = (long long)a.hi - a.lo;
+    int tpb = OdeShape<M, T, METHOD>::kThreads;
+    while (tpb > 32 && (nodes + tpb - 1) / tpb < c->sms) tpb /= 2;
     const long long cap = (long long)c->ode_blocks * 256 / tpb;
-    const int blocks = (int)std::max(1LL, std::min(cap, ((long long)a.hi - a.lo + tpb - 1) / tpb));
+    const int blocks = (int)std::max(1LL, std::min(cap, (nodes + tpb - 1) / tpb));
     if constexpr (host_input_method(METHOD)) {
         if (a.v_in) {
             ode_kernel<M, T, METHOD, true><<<blocks, tpb, 0, c->stream>>>(a);
