@@ -33,18 +33,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # BASELINE config 2 (3D TT06 slab) -- the metric's configuration
+    # the headline workload: the 3D TT06 slab of 442,401 nodes
     "tt06_slab_3d": dict(model=1, method=1, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01,
                          size=(2.0, 0.7, 0.3), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
                          box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8,
                          name="3D TT06-epi Rush-Larsen slab 2x0.7x0.3 cm h=0.01 (201x71x31 = 442,401 nodes)"),
-    # BASELINE config 5 (2.1M nodes): endo / mid / epi layers by thirds of z
+    # the 2.1M-node TT06 slab: endo / mid / epi layers by thirds of z
     "tt06_slab_3d_large": dict(model=1, method=1, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.0125,
                                size=(2.0, 2.0, 1.0), sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0),
                                box_hi=(0.1, 0.1, 0.1), rel_tol=1e-8, transmural=True,
                                name="3D TT06 Rush-Larsen slab 2x2x1 cm h=0.0125 (2,099,601 nodes), "
                                     "endo/mid/epi layers by z-thirds"),
-    # BASELINE config 1 (2D LR91 forward Euler)
+    # the 2D LR91 forward-Euler sheet of 10,201 nodes
     "lr91_sheet_2d": dict(model=0, method=0, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, size=(1.0, 1.0, 0.0),
                           sigma=(1.75, 1.75, 1.75), stim=(-5e5, 0.5, 0.0), box_hi=(0.0199, 1e9),
                           rel_tol=1e-8, name="2D LR91 forward-Euler sheet 1x1 cm h=0.01 (10,201 nodes)"),
@@ -334,7 +334,7 @@ def cpu_baseline(wl, start_steps, seconds=15.0, threads=None):
 
 
 def run_population(args):
-    """8192 TT06 cells, six conductances scaled by lognormal(0, 0.2), 1-20 beats
+    """Batched single cells: 8192 TT06 cells, six conductances scaled by lognormal(0, 0.2), 1-20 beats
     (uniform) at BCL 1000 ms, stimulus -52 uA/uF for 1 ms, Rush-Larsen dt 0.01 ms, FP64 and FP32 side by
     side, the engine the autotuner picks (one persistent launch in a CUDA graph, or one launch per beat).
     Metric: cell-steps/s over both precisions."""
@@ -374,7 +374,7 @@ def run_population(args):
 
 
 def run_cable(args):
-    """LR91 cable of 1000 nodes, h 0.01 cm, dt 0.01 ms, 400 ms, stimulus at x = 0,
+    """Adjoint conductance fitting: LR91 cable of 1000 nodes, h 0.01 cm, dt 0.01 ms, 400 ms, stimulus at x = 0,
     20 evenly spaced probes, targets from scale factors drawn from lognormal(0, 0.3) over 4 regions x 7
     (six LR91 conductances + the region's tissue conductivity), loss = MSE of the probe traces, gradient by
     the adjoint with checkpoints every 200 steps; central differences (eps 1e-6) of all 28 parameters run
@@ -515,7 +515,7 @@ def run_mixed(args):
 
 
 def run_bidomain(args):
-    """The bidomain step without a bath on the 2D LR91 sheet of configuration 1 (1 x 1 cm,
+    """The bidomain step without a bath on the 2D LR91 sheet of 10,201 nodes (1 x 1 cm,
     h = 0.01 cm, 10,201 nodes, 20,402 unknowns), Chaste's default conductivities
     (intracellular 1.75 / 0.19, extracellular 7.0 / 2.365 mS/cm along x / y), forward Euler dt
     0.01 ms, PDE dt 0.1 ms, CG + Jacobi rtol 1e-8 with the null space of constant phi_e, FP64.

@@ -94,11 +94,11 @@ def _fp64_and_mixed(N, orc, case, t_end, oracle_until, expect_pipe, every=1.0):
 
 def test_c1_sheet_full_size_against_oracle(N, orc):
     """LR91 2D sheet, 10,201 nodes, 100 ms: FP64 against the oracle all the way, mixed against FP64."""
-    r = _fp64_and_mixed(N, orc, TC.C1_SHEET_2D, t_end=100.0, oracle_until=100.0, expect_pipe=None)
-    print("C1", r)
+    r = _fp64_and_mixed(N, orc, TC.LR91_SHEET_10201, t_end=100.0, oracle_until=100.0, expect_pipe=None)
+    print("lr91_sheet_10201", r)
     assert r["fp64_vs_oracle_rel"] <= FP64_RTOL
     assert r["fp64_vs_oracle_its"] <= 1
-    assert r["fp64_vs_oracle_activation_ms"] <= TC.C1_SHEET_2D["dt_pde"] + 1e-12
+    assert r["fp64_vs_oracle_activation_ms"] <= TC.LR91_SHEET_10201["dt_pde"] + 1e-12
     assert r["mixed_vs_fp64_mv"] <= 0.5
     assert r["mixed_vs_fp64_activation_ms"] <= 1.0
     assert r["activated"] == r["n"]
@@ -108,11 +108,11 @@ def test_c2_slab_full_size_against_oracle(N, orc):
     """TT06 3D slab, 442,401 nodes, 50 ms (the benchmark's configuration): FP64 against
     the oracle over the whole run; mixed (cg_mixed_pipe_kernel with 3 nodes per thread
     and the x-line inner preconditioner) against FP64."""
-    r = _fp64_and_mixed(N, orc, TC.C2_SLAB_3D, t_end=50.0, oracle_until=50.0, expect_pipe=3)
-    print("C2", r)
+    r = _fp64_and_mixed(N, orc, TC.TT06_SLAB_442401, t_end=50.0, oracle_until=50.0, expect_pipe=3)
+    print("tt06_slab_442401", r)
     assert r["fp64_vs_oracle_rel"] <= FP64_RTOL
     assert r["fp64_vs_oracle_its"] <= 1
-    assert r["fp64_vs_oracle_activation_ms"] <= TC.C2_SLAB_3D["dt_pde"] + 1e-12
+    assert r["fp64_vs_oracle_activation_ms"] <= TC.TT06_SLAB_442401["dt_pde"] + 1e-12
     assert r["mixed_vs_fp64_mv"] <= 0.5
     assert r["mixed_vs_fp64_activation_ms"] <= 1.0
     assert r["activated"] > r["n"] // 2
@@ -123,8 +123,8 @@ def test_c5_transmural_slab_full_size(N, orc):
     layers, 100 ms: mixed (the HBM-resident two-reduction solve with the x-line inner
     preconditioner, no pipelining) against FP64 over the whole run, FP64 against the
     oracle over the first 5 ms."""
-    r = _fp64_and_mixed(N, orc, TC.transmural(TC.C5_SLAB_3D), t_end=100.0, oracle_until=5.0, expect_pipe=0)
-    print("C5", r)
+    r = _fp64_and_mixed(N, orc, TC.transmural(TC.TT06_SLAB_2099601), t_end=100.0, oracle_until=5.0, expect_pipe=0)
+    print("tt06_slab_2099601", r)
     assert r["fp64_vs_oracle_rel"] <= FP64_RTOL
     assert r["fp64_vs_oracle_its"] <= 1
     assert r["mixed_vs_fp64_mv"] <= 0.5

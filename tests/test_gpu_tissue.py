@@ -79,10 +79,10 @@ def test_lr91_2d_forward_euler_parity(N, oracle):
     assert np.max(np.abs(ig - io)) <= 1e-6 * max(1.0, np.abs(io).max())
 
 
-@pytest.mark.parametrize("case_name", ["LR91_2D", "TT06_3D", "C1_SHEET_2D"])
+@pytest.mark.parametrize("case_name", ["LR91_2D", "TT06_3D", "LR91_SHEET_10201"])
 def test_bjacobi_ilu0_parity(N, oracle, case_name):
     """bjacobi (ILU(0) of the whole matrix, level-scheduled on the device) against the
-    oracle's ILU(0) on the reduced benchmark slabs and the full 10,201-node C1 sheet (all
+    oracle's ILU(0) on the reduced benchmark slabs and the full 10,201-node LR91 sheet (all
     three take the one-block solve with its vectors in shared memory): Vm every 1 ms
     within 1e-6, CG iteration counts within one, and fewer iterations than Jacobi."""
     case = dict(getattr(TC, case_name), pc=2)

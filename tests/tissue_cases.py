@@ -88,12 +88,12 @@ def niederer_activation(t, n, printing_steps=10, n_prints=400, printing_dt=0.1):
     return act
 
 
-# The benchmark configurations at full size (2 and 5)
-C1_SHEET_2D = dict(model=LR91, method=FE, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, size=(1.0, 1.0, 0.0),
+# The benchmark workloads at full size: the 2D LR91 sheet, the 3D TT06 slab and the 2.1M-node slab
+LR91_SHEET_10201 = dict(model=LR91, method=FE, dt_ode=0.01, dt_pde=0.1, dim=2, h=0.01, size=(1.0, 1.0, 0.0),
                    sigma=(1.75, 1.75, 1.75), stim=(-5e5, 0.5, 0.0), box_hi=(0.0199, 1e9))
-C2_SLAB_3D = dict(model=TT06, method=RL, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01, size=(2.0, 0.7, 0.3),
+TT06_SLAB_442401 = dict(model=TT06, method=RL, dt_ode=0.02, dt_pde=0.1, dim=3, h=0.01, size=(2.0, 0.7, 0.3),
                   sigma=(1.75, 0.19, 0.19), stim=(-5e5, 1.0, 0.0), box_hi=(0.1, 0.1, 0.1))
-C5_SLAB_3D = dict(C2_SLAB_3D, h=0.0125, size=(2.0, 2.0, 1.0))
+TT06_SLAB_2099601 = dict(TT06_SLAB_442401, h=0.0125, size=(2.0, 2.0, 1.0))
 
 
 def transmural(case):
