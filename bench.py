@@ -267,10 +267,11 @@ def run_ours(args, rank, world, device):
 
 # DRAM bytes (read + write) per launch of the dominant kernels from one ncu capture of
 # the timed region's conditions (L2 flushed before the step, the window starting at
-# --t-start-ms), `bench.py --profile <precision> --steps 5`, summarised in
-# profiles/cg_kernels_tt06_slab_3d.md.  None where no such capture exists.
+# --t-start-ms: `bench.py --profile mixed [--workload ...] --steps 1 --t-start-ms 0.5`,
+# the 6th solve).  None where no such capture exists.
 NCU_TRAFFIC = {
     ("tt06_slab_3d", "mixed", "cg_kernel"): 11.07e6,   # 10.21 MB read + 0.86 MB written, 163 us
+    ("tt06_slab_3d_large", "mixed", "cg_kernel"): 124.7e6,   # 75.9 MB read + 48.8 MB written, 364 us
 }
 
 
@@ -644,7 +645,7 @@ def main():
     ap.add_argument("--profile", choices=["fp64", "mixed", "fp64-bjacobi", "population", "runs"],
                     help="only build the workload's tissue in this precision (fp64-bjacobi: FP64 with Chaste's "
                          "default bjacobi preconditioner), advance it to --t-start-ms and take --steps steps "
-                         "with an L2 flush before each (the program the ncu captures in profiles/ run)")
+                         "with an L2 flush before each (the program the ncu captures run)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.profile == "population":
