@@ -381,7 +381,7 @@ __device__ void cg_ilu_smem_body(const CgArgs& a, const IluArgs& f, unsigned& ro
         v[2] += zz * zz;
         v[3] += r[i] * zz;
     }
-    if (!grid_reduce<4>(v, red, a.gs, a.partials, res, a.status, round)) return;
+    block_reduce<4>(v, red, res, round);
     double rnorm0 = sqrt(res[1]);
     double dp = sqrt(res[2]);
     double beta = res[3];
@@ -397,7 +397,7 @@ __device__ void cg_ilu_smem_body(const CgArgs& a, const IluArgs& f, unsigned& ro
             v2[1] += b * zz;
         }
         double o2[2];
-        if (!grid_reduce<2>(v2, red, a.gs, a.partials, o2, a.status, round)) return;
+        block_reduce<2>(v2, red, o2, round);
         dp = sqrt(o2[0]);
         beta = o2[1];
         rnorm0 = dp;
@@ -425,7 +425,7 @@ __device__ void cg_ilu_smem_body(const CgArgs& a, const IluArgs& f, unsigned& ro
                 p[i] = pi;
                 v1[0] += pi * qi;
             }
-            if (!grid_reduce<1>(v1, red, a.gs, a.partials, res, a.status, round)) return;
+            block_reduce<1>(v1, red, res, round);
         }
         const double dpi = res[0];
         if (!(dpi > 0.0)) return cg_finish(a, step, it + 1, isfinite(dpi) ? kStatusCgDiverged : kStatusNaN);
@@ -446,7 +446,7 @@ __device__ void cg_ilu_smem_body(const CgArgs& a, const IluArgs& f, unsigned& ro
             v2[0] += zz * zz;
             v2[1] += zz * r[i];
         }
-        if (!grid_reduce<2>(v2, red, a.gs, a.partials, res, a.status, round)) return;
+        block_reduce<2>(v2, red, res, round);
         dp = sqrt(res[0]);
         if (!isfinite(dp)) return cg_finish(a, step, it + 1, kStatusNaN);
         if (dp <= ttol) return cg_finish(a, step, it + 1, 0);

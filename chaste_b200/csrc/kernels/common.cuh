@@ -130,8 +130,11 @@ __device__ __forceinline__ bool wait_count(unsigned* counter, unsigned target, i
 // Needs blockDim >= 32 * kReduceWarps; red holds 32 * NV doubles.
 constexpr int kReduceWarps = 4;
 
-// The same reduction when the grid is one block: the block's sums are the totals, with
-// no global partials, atomics or polling.
+// The same reduction for a kernel that always runs as one block (the shared-memory
+// bjacobi solve): the block's sums are the totals, with no global partials, atomics or
+// polling.  (Taken inside grid_reduce whenever gridDim is 1, the branch pushed the
+// HBM-resident mixed solve from 16 to 156 bytes of spills a thread and 0.49 to 0.61 ms
+// per solve on the 2.1M-node slab.)
 template <int NV>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], double* red, double* out, unsigned& round) {
     __shared__ double s_tot[2][kPartialStride];
@@ -162,10 +165,7 @@ template <int NV>
 __device__ bool grid_reduce(double (&v)[NV], double* red, GridSync* gs, double* partials, double* out, int* status,
                             unsigned& round) {
     static_assert(NV >= 1 && NV <= kPartialStride, "at most four sums per reduction");
-    if (gridDim.x == 1) {
-        block_reduce<NV>(v, red, out, round);
-        return true;
-    }
+
     constexpr int kLoads = kMaxGridBlocks / (32 * kReduceWarps);
     __shared__ int s_ok;
     __shared__ double s_part[kReduceWarps][kPartialStride];
