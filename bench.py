@@ -272,6 +272,7 @@ def run_ours(args, rank, world, device):
 NCU_TRAFFIC = {
     ("tt06_slab_3d", "mixed", "cg_kernel"): 11.07e6,   # 10.21 MB read + 0.86 MB written, 163 us
     ("tt06_slab_3d_large", "mixed", "cg_kernel"): 124.7e6,   # 75.9 MB read + 48.8 MB written, 364 us
+    ("lr91_sheet_2d", "mixed", "cg_kernel"): 0.296e6,   # 296 kB read + 256 B written, 99 us: all in L2
 }
 
 
